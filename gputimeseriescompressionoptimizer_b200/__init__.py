@@ -1,0 +1,146 @@
+"""gputimeseriescompressionoptimizer_b200 -- B200-native lightweight column compression.
+
+Python host side over the C ABI of libgtsc.so (declared in include/gtsc.h).  The CUDA library is
+the only implementation: importing this package loads it, and every call fails loudly when it is
+missing or when no GPU is present -- there is no CPU fallback.
+
+Low-level API (device buffers in, device buffers out)::
+
+    import gputimeseriescompressionoptimizer_b200 as g
+    col = g.to_device(np.arange(1000, dtype=np.int32))
+    parts = g.encode(g.AFL, g.INT, col)          # [metadata, data] on the GPU
+    back = g.decode(g.AFL, g.INT, parts)
+    assert (g.to_host(back, np.int32) == np.arange(1000)).all()
+
+The reference-shaped classes (EncodingType, DataType, Encoding factories, CompressionTree,
+CompressionOptimizer, ...) live in `gputimeseriescompressionoptimizer_b200.api`.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgtsc.so")
+
+# DataType codes (this library's; the reference's live in an unavailable submodule)
+CHAR, SHORT, INT, TIME, FLOAT, DOUBLE = range(6)
+# EncodingType codes (compression/encoding_type.hpp:17-30)
+DELTA, AFL, SCALE, RLE, DICT, UNIQUE, PATCH, NONE, FLOAT_TO_INT, CONST, GFC = range(11)
+ENCODING_NAMES = ["delta", "afl", "scale", "rle", "dict", "unique", "patch", "none", "floatToInt",
+                  "constData", "gfc"]
+NP_TYPES = {CHAR: np.int8, SHORT: np.int16, INT: np.int32, TIME: np.int64, FLOAT: np.float32,
+            DOUBLE: np.float64}
+
+STATUS_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_TYPE", -3: "ERR_CAPACITY", -4: "ERR_FORMAT",
+                -5: "ERR_UNSUPPORTED", -6: "ERR_CUDA", -7: "ERR_TIMEOUT", -8: "ERR_NO_DEVICE"}
+
+
+class GtscError(RuntimeError):
+    """A libgtsc call returned a non-zero status."""
+
+    def __init__(self, status, what, message):
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Buffer(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("bytes", ctypes.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libgtsc.so.  Raises when the extension was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libgtsc.so not built ({LIB_PATH}); run __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32
+        L.gtsc_last_error.restype = ctypes.c_char_p
+        L.gtsc_version.restype = ctypes.c_char_p
+        L.gtsc_dtype_size.argtypes = [i32]
+        L.gtsc_malloc.argtypes = [ctypes.POINTER(vp), u64, vp]
+        L.gtsc_free.argtypes = [vp, vp]
+        L.gtsc_memcpy.argtypes = [vp, vp, u64, i32, vp]
+        L.gtsc_stream_synchronize.argtypes = [vp]
+        L.gtsc_encode.argtypes = [i32, i32, vp, u64, ctypes.POINTER(Buffer), ctypes.POINTER(ctypes.c_uint32), vp]
+        L.gtsc_decode.argtypes = [i32, i32, ctypes.POINTER(Buffer), ctypes.c_uint32, ctypes.POINTER(Buffer), vp]
+        _lib = L
+    return _lib
+
+
+def check(status, what):
+    if status != 0:
+        msg = lib().gtsc_last_error().decode(errors="replace")
+        raise GtscError(status, what, msg)
+
+
+class DeviceBuffer:
+    """Owned device allocation (freed with gtsc_free when collected)."""
+
+    __slots__ = ("ptr", "nbytes", "_owned")
+
+    def __init__(self, ptr, nbytes, owned=True):
+        self.ptr = ptr or None
+        self.nbytes = int(nbytes)
+        self._owned = owned and bool(ptr)
+
+    def __del__(self):
+        if getattr(self, "_owned", False) and _lib is not None:
+            _lib.gtsc_free(self.ptr, None)
+            self._owned = False
+
+    def __len__(self):
+        return self.nbytes
+
+    def __repr__(self):
+        return f"DeviceBuffer(0x{self.ptr or 0:x}, {self.nbytes} B)"
+
+
+def alloc(nbytes, stream=None):
+    p = ctypes.c_void_p()
+    check(lib().gtsc_malloc(ctypes.byref(p), nbytes, stream), "gtsc_malloc")
+    return DeviceBuffer(p.value, nbytes)
+
+
+def to_device(array, stream=None):
+    a = np.ascontiguousarray(array)
+    buf = alloc(a.nbytes, stream)
+    if a.nbytes:
+        check(lib().gtsc_memcpy(buf.ptr, a.ctypes.data, a.nbytes, 1, stream), "gtsc_memcpy h2d")
+        check(lib().gtsc_stream_synchronize(stream), "sync")
+    return buf
+
+
+def to_host(buf, dtype=np.uint8, stream=None):
+    out = np.empty(buf.nbytes, np.uint8)
+    if buf.nbytes:
+        check(lib().gtsc_memcpy(out.ctypes.data, buf.ptr, buf.nbytes, 2, stream), "gtsc_memcpy d2h")
+    return out.view(dtype) if np.dtype(dtype).itemsize and buf.nbytes % np.dtype(dtype).itemsize == 0 else out
+
+
+def dtype_size(dtype):
+    return lib().gtsc_dtype_size(dtype)
+
+
+def encode(encoding, dtype, data, stream=None):
+    """Encoding::Encode -> [metadata, out1, (out2)] as DeviceBuffers."""
+    outs = (Buffer * 3)()
+    n_out = ctypes.c_uint32(0)
+    check(lib().gtsc_encode(encoding, dtype, data.ptr, data.nbytes, outs, ctypes.byref(n_out), stream),
+          f"encode {ENCODING_NAMES[encoding]}")
+    return [DeviceBuffer(outs[i].ptr, outs[i].bytes) for i in range(n_out.value)]
+
+
+def decode(encoding, dtype, parts, stream=None):
+    """Encoding::Decode of [metadata, in1, (in2)] -> DeviceBuffer."""
+    ins = (Buffer * 3)()
+    for i, p in enumerate(parts):
+        ins[i] = Buffer(p.ptr, p.nbytes)
+    out = Buffer()
+    check(lib().gtsc_decode(encoding, dtype, ins, len(parts), ctypes.byref(out), stream),
+          f"decode {ENCODING_NAMES[encoding]}")
+    return DeviceBuffer(out.ptr, out.bytes)

@@ -1,0 +1,137 @@
+// capi.cpp -- the extern "C" boundary of libgtsc.  Every entry point converts C++ exceptions into
+// gtsc_status codes and records the message for gtsc_last_error().
+#include "common.cuh"
+#include "encodings.hpp"
+#include "kernels.hpp"
+
+#include <cstring>
+#include <exception>
+
+namespace gtsc {
+const std::string &last_error();
+}
+
+using namespace gtsc;
+
+namespace {
+
+template <class F>
+gtsc_status guard(F &&f)
+{
+    try {
+        set_last_error("");
+        f();
+        return GTSC_OK;
+    } catch (const Error &e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return GTSC_ERR_CAPACITY;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return GTSC_ERR_ARG;
+    }
+}
+
+inline cudaStream_t S(void *p) { return reinterpret_cast<cudaStream_t>(p); }
+
+// hands a library-owned buffer to the caller, who releases it with gtsc_free
+gtsc_buffer release(DevBuf &b)
+{
+    gtsc_buffer r{b.disown(), b.bytes};
+    b.m.reset();
+    return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gtsc_last_error(void) { return last_error().c_str(); }
+
+const char *gtsc_version(void) { return "gtsc 0.1 sm_100a"; }
+
+int32_t gtsc_dtype_size(int32_t dtype) { return dtype_size(dtype); }
+
+gtsc_status gtsc_malloc(void **d_ptr, uint64_t bytes, void *stream)
+{
+    return guard([&] {
+        if (!d_ptr) fail(GTSC_ERR_ARG, "null d_ptr");
+        *d_ptr = nullptr;
+        if (bytes) GTSC_CUDA(cudaMallocAsync(d_ptr, bytes, S(stream)));
+    });
+}
+
+gtsc_status gtsc_free(void *d_ptr, void *stream)
+{
+    return guard([&] {
+        if (d_ptr) GTSC_CUDA(cudaFreeAsync(d_ptr, S(stream)));
+    });
+}
+
+gtsc_status gtsc_memcpy(void *dst, const void *src, uint64_t bytes, int32_t kind, void *stream)
+{
+    return guard([&] {
+        if (kind < 1 || kind > 3) fail(GTSC_ERR_ARG, "bad copy kind");
+        if (bytes) GTSC_CUDA(cudaMemcpyAsync(dst, src, bytes, (cudaMemcpyKind)kind, S(stream)));
+        if (kind == 2) GTSC_CUDA(cudaStreamSynchronize(S(stream)));
+    });
+}
+
+gtsc_status gtsc_stream_synchronize(void *stream)
+{
+    return guard([&] { GTSC_CUDA(cudaStreamSynchronize(S(stream))); });
+}
+
+gtsc_status gtsc_encode(int32_t encoding, int32_t dtype, const void *d_in, uint64_t in_bytes,
+                        gtsc_buffer out[3], uint32_t *n_out, void *stream)
+{
+    return guard([&] {
+        if (!out || !n_out) fail(GTSC_ERR_ARG, "null output");
+        Parts p = encode(encoding, dtype, View(d_in, in_bytes), S(stream));
+        GTSC_CUDA(cudaStreamSynchronize(S(stream)));
+        for (int i = 0; i < 3; i++) out[i] = gtsc_buffer{nullptr, 0};
+        *n_out = (uint32_t)p.size();
+        for (size_t i = 0; i < p.size(); i++) out[i] = release(p[i]);
+    });
+}
+
+gtsc_status gtsc_decode(int32_t encoding, int32_t dtype, const gtsc_buffer in[3], uint32_t n_in,
+                        gtsc_buffer *out, void *stream)
+{
+    return guard([&] {
+        if (!out || (!in && n_in)) fail(GTSC_ERR_ARG, "null argument");
+        if (n_in > 3) fail(GTSC_ERR_ARG, "at most 3 inputs");
+        std::vector<View> v;
+        for (uint32_t i = 0; i < n_in; i++) v.push_back(View(in[i].ptr, in[i].bytes));
+        DevBuf r = decode(encoding, dtype, v, S(stream));
+        GTSC_CUDA(cudaStreamSynchronize(S(stream)));
+        *out = release(r);
+    });
+}
+
+gtsc_status gtsc_afl_compress_gpu(int32_t dtype, uint32_t bit_length, const void *d_data, uint64_t n,
+                                  void *d_out, uint64_t out_bytes, void *stream)
+{
+    return guard([&] {
+        const int es = dtype_size(dtype);
+        if (!es || is_fp(dtype)) fail(GTSC_ERR_TYPE, "afl: integer data types only");
+        const uint64_t W = 8ull * es;
+        if (out_bytes < (bit_length * n + W - 1) / W * es) fail(GTSC_ERR_CAPACITY, "afl: output too small");
+        launch_afl_pack((const uint8_t *)d_data, n, es, (int)bit_length, (uint8_t *)d_out, out_bytes, S(stream));
+    });
+}
+
+gtsc_status gtsc_afl_decompress_gpu(int32_t dtype, uint32_t bit_length, const void *d_comp,
+                                    uint64_t comp_bytes, void *d_out, uint64_t n, void *stream)
+{
+    return guard([&] {
+        const int es = dtype_size(dtype);
+        if (!es || is_fp(dtype)) fail(GTSC_ERR_TYPE, "afl: integer data types only");
+        if (comp_bytes * 8 < n * (uint64_t)bit_length) fail(GTSC_ERR_FORMAT, "afl: stream too short");
+        launch_afl_unpack((const uint8_t *)d_comp, comp_bytes, n, es, (int)bit_length, (uint8_t *)d_out, S(stream));
+    });
+}
+
+}  // extern "C"

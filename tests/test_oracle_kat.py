@@ -1,0 +1,116 @@
+"""Pins the CPU oracle against the reference's own known-answer tests (restated) and against the
+reference's AFL host implementation compiled from its sources (oracle/_ref).  CPU only."""
+import numpy as np
+import pytest
+
+import oracle as OR
+
+
+# ---- BITLEN / ALT_BITLEN (src/test/macros_unittest.cu:5-139) --------------------------------
+@pytest.mark.parametrize("dt,mn,mx,expected", [
+    (OR.INT, 0, 0, 1), (OR.INT, 0, 1, 1), (OR.INT, 0, 12345, 14), (OR.INT, 0, 2147268225, 31),
+    (OR.INT, -12345, -12345, 32), (OR.INT, -2147268227, 147268227, 32), (OR.SHORT, 0, 12345, 14),
+    (OR.CHAR, 0, 45, 6), (OR.TIME, 0, 22147268225, 35)])
+def test_bitlen_kat(O, dt, mn, mx, expected):
+    assert O.lib().or_bitlen(dt, mn, mx) == expected
+
+
+@pytest.mark.parametrize("v,expected", [(12345, 14), (2147268225, 31), (-12345, 32),
+                                        (-2147268227, 32), (0, 1), (1, 1)])
+def test_alt_bitlen_kat(O, v, expected):
+    assert O.lib().or_alt_bitlen(v) == expected
+
+
+# ---- _getFloatPrecision (util/statistics/cuda_array_statistics_unittest.cpp:21-83) ----------
+@pytest.mark.parametrize("x,expected", [(123.0, 0), (123123123123.0, 0), (-123123123.0, 0), (123.1, 1),
+                                        (123.34, 2), (13.3412312, 6), (1231201.2312, 1),
+                                        (12312311.33412312, 0)])
+def test_float_precision_kat(O, x, expected):
+    assert O.lib().or_float_precision(np.float32(x)) == expected
+
+
+# ---- Sorted / RlMetric / Mean (cuda_array_statistics_unittest.cpp:103-187), size 10000 -------
+N = 10000
+
+
+def test_sorted_kat(O):
+    h = np.array([i // 100 if i % 50 == 0 else N for i in range(N)], np.int32)
+    assert O.stats(OR.INT, h).sorted == 0
+    h = np.array([i // 100 + 39 for i in range(N)], np.int32)
+    assert O.stats(OR.INT, h).sorted == 1
+
+
+def test_rlmetric_kat(O):
+    const = np.full(N, 100, np.int32)
+    assert O.lib().or_rl_metric(OR.INT, const.ctypes.data, const.nbytes, 4) == 4.0
+    consec = np.arange(N, dtype=np.int32)
+    assert O.lib().or_rl_metric(OR.INT, consec.ctypes.data, consec.nbytes, 4) == 1.0
+    pairs = (np.arange(N) // 2).astype(np.int32)
+    assert O.stats(OR.INT, pairs).rl_metric == 1.5
+
+
+def test_mean_kat(O):
+    assert O.stats(OR.INT, np.arange(N, dtype=np.int32)).mean == float((N - 1) // 2)
+
+
+# ---- stencil pack / unpack (util/stencil/stencil_unittest.cpp:10-34) -------------------------
+@pytest.mark.parametrize("n", [1, 7, 8, 9, 1000, 1001])
+def test_stencil_pack_unpack(O, rng, n):
+    st = rng.integers(0, 2, n).astype(np.int32)
+    packed = np.zeros(n // 8 + 2, np.uint8)
+    nb = O.lib().or_stencil_pack(st.ctypes.data, n, packed.ctypes.data)
+    assert nb == (n + 7) // 8 + 1 and nb < 4 * n
+    assert packed[0] == n % 8
+    # tail bits repeat the last element (stencil.cu:27)
+    if n % 8:
+        tail = (packed[nb - 1] >> (n % 8)) & 1
+        assert tail == st[-1]
+    out = np.zeros(n + 8, np.int32)
+    m = O.lib().or_stencil_unpack(packed.ctypes.data, nb, out.ctypes.data, n + 8)
+    assert m == n and np.array_equal(out[:n], st)
+
+
+# ---- split / merge ordering (util/splitter/splitter_unittest.cpp:63-170) ----------------------
+def test_split_manual_complex(O, rng):
+    # a patch split is Splitter::Split on the stencil x < threshold: check stable ordering
+    n = 1000
+    x = rng.integers(0, 100, n).astype(np.int32)
+    x[: n // 4] = 95
+    x[n // 2: 3 * n // 4] = 99
+    x[0] = 0
+    parts = O.encode(OR.PATCH, OR.INT, x)
+    st = np.unpackbits(parts[0][1:], bitorder="little")[:n].astype(bool)
+    t = int(99 - 0.1 * 99)
+    assert np.array_equal(st, x < t)
+    assert np.array_equal(parts[1].view(np.int32), x[st])
+    assert np.array_equal(parts[2].view(np.int32), x[~st])
+
+
+# ---- AFL against the reference's own host implementation (afl_gpu.cu:6-65) ------------------
+@pytest.mark.parametrize("dt,npt", [(OR.CHAR, np.int8), (OR.SHORT, np.int16), (OR.INT, np.int32),
+                                    (OR.TIME, np.int64)])
+def test_afl_oracle_matches_reference(O, rng, dt, npt):
+    if not OR.build_ref():
+        pytest.skip("reference AFL sources not available")
+    W = 8 * np.dtype(npt).itemsize
+    for n in [1, 31, 32, 33, 1000, 4097]:
+        for b in sorted({1, 3, 5, 7, 11, W - 1}):
+            if b >= W:
+                continue
+            x = rng.integers(0, 2 ** b, n).astype(npt)
+            x[0] = 2 ** b - 1
+            meta, data = O.encode(OR.AFL, dt, x)
+            assert meta[0] == b and meta[2] == 0 and meta[3] == 0
+            assert np.array_equal(O.ref_afl_compress(dt, x, b), data)
+            assert np.array_equal(O.ref_afl_decompress(dt, data, b, n), x)
+
+
+def test_afl_config1_sizes(O, rng):
+    """2^20 int32 uniform in [0, 2^11): b = 11, 1 441 792 data bytes + 4 metadata bytes."""
+    x = rng.integers(0, 2 ** 11, 1 << 20).astype(np.int32)
+    x[0] = 2 ** 11 - 1
+    meta, data = O.encode(OR.AFL, OR.INT, x)
+    assert meta.size == 4 and meta[0] == 11 and meta[1] == 0
+    assert data.size == 1441792
+    if OR.build_ref():
+        assert np.array_equal(O.ref_afl_compress(OR.INT, x, 11), data)
