@@ -48,6 +48,14 @@ class Buffer(ctypes.Structure):
     _fields_ = [("ptr", ctypes.c_void_p), ("bytes", ctypes.c_uint64)]
 
 
+class DataStatistics(ctypes.Structure):
+    """DataStatistics (util/statistics/cuda_array_statistics.hpp:24-34)."""
+    _fields_ = [("min", ctypes.c_double), ("max", ctypes.c_double),
+                ("min_bit_cnt", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("sorted", ctypes.c_int32), ("rl_metric", ctypes.c_float),
+                ("mean", ctypes.c_double), ("size", ctypes.c_uint64)]
+
+
 _lib = None
 
 
@@ -68,6 +76,19 @@ def lib():
         L.gtsc_stream_synchronize.argtypes = [vp]
         L.gtsc_encode.argtypes = [i32, i32, vp, u64, ctypes.POINTER(Buffer), ctypes.POINTER(ctypes.c_uint32), vp]
         L.gtsc_decode.argtypes = [i32, i32, ctypes.POINTER(Buffer), ctypes.c_uint32, ctypes.POINTER(Buffer), vp]
+        u32 = ctypes.c_uint32
+        L.gtsc_stats.argtypes = [i32, vp, u64, ctypes.POINTER(DataStatistics), vp]
+        L.gtsc_afl_compress_gpu.argtypes = [i32, u32, vp, u64, vp, u64, vp]
+        L.gtsc_afl_decompress_gpu.argtypes = [i32, u32, vp, u64, vp, u64, vp]
+        i16p, i32p, u64p = ctypes.POINTER(ctypes.c_int16), ctypes.POINTER(i32), ctypes.POINTER(u64)
+        L.gtsc_tree_from_path.argtypes = [i16p, i32, i32, i16p, i32, i32p]
+        L.gtsc_tree_compress.argtypes = [i16p, i32, vp, u64, ctypes.POINTER(Buffer), vp]
+        L.gtsc_tree_decompress.argtypes = [vp, u64, ctypes.POINTER(Buffer), i32p, vp]
+        L.gtsc_tree_predict_size.argtypes = [i16p, i32, vp, u64, u64p, vp]
+        L.gtsc_plan_exhaustive.argtypes = [i32, vp, u64, i16p, i32, i32p, u64p, vp]
+        L.gtsc_optimize_tree.argtypes = [i32, vp, u64, i16p, i32, i32p, u64p, vp]
+        L.gtsc_sample_bytes.argtypes = [i32, u64]
+        L.gtsc_sample_bytes.restype = u64
         _lib = L
     return _lib
 
@@ -144,3 +165,80 @@ def decode(encoding, dtype, parts, stream=None):
     check(lib().gtsc_decode(encoding, dtype, ins, len(parts), ctypes.byref(out), stream),
           f"decode {ENCODING_NAMES[encoding]}")
     return DeviceBuffer(out.ptr, out.bytes)
+
+
+def stats(dtype, data, stream=None):
+    """CudaArrayStatistics::GenerateStatistics of a device column -> DataStatistics."""
+    s = DataStatistics()
+    check(lib().gtsc_stats(dtype, data.ptr, data.nbytes, ctypes.byref(s), stream), "stats")
+    return s
+
+
+# ------------------------------------------------------------------------ compression trees
+def _i16(a):
+    a = np.ascontiguousarray(a, np.int16)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int16))
+
+
+def tree_from_path(encodings, dtype):
+    """PathGenerator::GenerateTree -> node list [(enc, dtype), ...] as an int16 array of pairs."""
+    p, pp = _i16(encodings)
+    out = np.zeros(2 * 256, np.int16)
+    n = ctypes.c_int32(0)
+    check(lib().gtsc_tree_from_path(pp, p.size, dtype,
+                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)), 256,
+                                    ctypes.byref(n)), "tree_from_path")
+    return out[:2 * n.value].copy()
+
+
+def tree_compress(nodes, data, stream=None):
+    """CompressionTree::Compress -> serialized blob (DeviceBuffer)."""
+    nd, ndp = _i16(nodes)
+    out = Buffer()
+    check(lib().gtsc_tree_compress(ndp, nd.size // 2, data.ptr, data.nbytes, ctypes.byref(out), stream),
+          "tree_compress")
+    return DeviceBuffer(out.ptr, out.bytes)
+
+
+def tree_decompress(blob, stream=None):
+    """CompressionTree::Decompress -> (DeviceBuffer, root data type)."""
+    out = Buffer()
+    dt = ctypes.c_int32(-1)
+    check(lib().gtsc_tree_decompress(blob.ptr, blob.nbytes, ctypes.byref(out), ctypes.byref(dt), stream),
+          "tree_decompress")
+    return DeviceBuffer(out.ptr, out.bytes), dt.value
+
+
+def tree_predict_size(nodes, data, stream=None):
+    nd, ndp = _i16(nodes)
+    sz = ctypes.c_uint64(0)
+    check(lib().gtsc_tree_predict_size(ndp, nd.size // 2, data.ptr, data.nbytes, ctypes.byref(sz), stream),
+          "tree_predict_size")
+    return sz.value
+
+
+def _plan(fn, what, dtype, data, stream):
+    out = np.zeros(2 * 1024, np.int16)
+    n = ctypes.c_int32(0)
+    sz = ctypes.c_uint64(0)
+    check(fn(dtype, data.ptr, data.nbytes, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)), 1024,
+             ctypes.byref(n), ctypes.byref(sz), stream), what)
+    return out[:2 * n.value].copy(), sz.value
+
+
+def plan_exhaustive(dtype, sample, stream=None):
+    """FullStatisticsUpdate + max-ratio pick on a device sample -> (nodes, candidate size)."""
+    return _plan(lib().gtsc_plan_exhaustive, "plan_exhaustive", dtype, sample, stream)
+
+
+def optimize_tree(dtype, data, stream=None):
+    """CompressionOptimizer::OptimizeTree -> (nodes, predicted size)."""
+    return _plan(lib().gtsc_optimize_tree, "optimize_tree", dtype, data, stream)
+
+
+def sample_bytes(dtype, nbytes):
+    return lib().gtsc_sample_bytes(dtype, nbytes)
+
+
+def tree_names(nodes):
+    return [ENCODING_NAMES[e] for e in np.asarray(nodes)[::2]]

@@ -3,6 +3,8 @@
 #include "common.cuh"
 #include "encodings.hpp"
 #include "kernels.hpp"
+#include "planner.hpp"
+#include "tree.hpp"
 
 #include <cstring>
 #include <exception>
@@ -110,6 +112,89 @@ gtsc_status gtsc_decode(int32_t encoding, int32_t dtype, const gtsc_buffer in[3]
         *out = release(r);
     });
 }
+
+gtsc_status gtsc_stats(int32_t dtype, const void *d_in, uint64_t in_bytes, gtsc_data_statistics *out,
+                       void *stream)
+{
+    return guard([&] {
+        if (!out) fail(GTSC_ERR_ARG, "null output");
+        Stats st = column_stats(dtype, View(d_in, in_bytes), S(stream));
+        static_assert(sizeof(Stats) == sizeof(gtsc_data_statistics), "layout");
+        std::memcpy(out, &st, sizeof(st));
+    });
+}
+
+static void write_tree(const Tree &t, int16_t *nodes_out, int32_t cap, int32_t *n_nodes)
+{
+    if (!nodes_out || !n_nodes) fail(GTSC_ERR_ARG, "null output");
+    if (t.size() > cap) fail(GTSC_ERR_CAPACITY, "node list longer than cap");
+    tree_to_nodes(t, nodes_out);
+    *n_nodes = t.size();
+}
+
+gtsc_status gtsc_tree_from_path(const int16_t *encodings, int32_t n_encodings, int32_t dtype,
+                                int16_t *nodes_out, int32_t cap, int32_t *n_nodes)
+{
+    return guard([&] {
+        if (!encodings || n_encodings <= 0) fail(GTSC_ERR_ARG, "empty path");
+        write_tree(tree_from_path(encodings, n_encodings, dtype), nodes_out, cap, n_nodes);
+    });
+}
+
+gtsc_status gtsc_tree_compress(const int16_t *nodes, int32_t n_nodes, const void *d_in, uint64_t in_bytes,
+                               gtsc_buffer *blob, void *stream)
+{
+    return guard([&] {
+        if (!blob) fail(GTSC_ERR_ARG, "null output");
+        DevBuf b = tree_compress(tree_from_nodes(nodes, n_nodes), View(d_in, in_bytes), S(stream));
+        *blob = release(b);
+    });
+}
+
+gtsc_status gtsc_tree_decompress(const void *d_blob, uint64_t blob_bytes, gtsc_buffer *out, int32_t *dtype,
+                                 void *stream)
+{
+    return guard([&] {
+        if (!out) fail(GTSC_ERR_ARG, "null output");
+        int dt = 0;
+        DevBuf b = tree_decompress(View(d_blob, blob_bytes), &dt, S(stream));
+        if (dtype) *dtype = dt;
+        *out = release(b);
+    });
+}
+
+gtsc_status gtsc_tree_predict_size(const int16_t *nodes, int32_t n_nodes, const void *d_in, uint64_t in_bytes,
+                                   uint64_t *size, void *stream)
+{
+    return guard([&] {
+        if (!size) fail(GTSC_ERR_ARG, "null output");
+        *size = tree_predict_size(tree_from_nodes(nodes, n_nodes), View(d_in, in_bytes), S(stream));
+    });
+}
+
+gtsc_status gtsc_plan_exhaustive(int32_t dtype, const void *d_sample, uint64_t sample_bytes_, int16_t *nodes_out,
+                                 int32_t cap, int32_t *n_nodes, uint64_t *candidate_size, void *stream)
+{
+    return guard([&] {
+        uint64_t sz = 0;
+        Tree t = plan_exhaustive(dtype, View(d_sample, sample_bytes_), &sz, nullptr, S(stream));
+        write_tree(t, nodes_out, cap, n_nodes);
+        if (candidate_size) *candidate_size = sz;
+    });
+}
+
+gtsc_status gtsc_optimize_tree(int32_t dtype, const void *d_in, uint64_t in_bytes, int16_t *nodes_out,
+                               int32_t cap, int32_t *n_nodes, uint64_t *predicted_size, void *stream)
+{
+    return guard([&] {
+        uint64_t sz = 0;
+        Tree t = optimize_tree(dtype, View(d_in, in_bytes), &sz, S(stream));
+        write_tree(t, nodes_out, cap, n_nodes);
+        if (predicted_size) *predicted_size = sz;
+    });
+}
+
+uint64_t gtsc_sample_bytes(int32_t dtype, uint64_t in_bytes) { return sample_bytes(dtype, in_bytes); }
 
 gtsc_status gtsc_afl_compress_gpu(int32_t dtype, uint32_t bit_length, const void *d_data, uint64_t n,
                                   void *d_out, uint64_t out_bytes, void *stream)

@@ -21,11 +21,32 @@ void cuda_check(cudaError_t e, const char *what)
     }
 }
 
+// The default memory pool returns freed memory to the driver at every synchronisation unless its
+// release threshold is raised; the encodings allocate and free column-sized buffers on every call,
+// so keep what the pool has reserved (once per device).
+static void keep_pool_memory()
+{
+    static std::mutex mu;
+    static std::vector<int> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    std::lock_guard<std::mutex> lock(mu);
+    for (int d : done)
+        if (d == dev) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done.push_back(dev);
+}
+
 DevBuf dev_alloc(uint64_t bytes, cudaStream_t s)
 {
     DevBuf b;
     b.bytes = bytes;
     if (bytes == 0) return b;
+    keep_pool_memory();
     void *p = nullptr;
     // round up so that vector loads of a final partial chunk stay inside the allocation
     GTSC_CUDA(cudaMallocAsync(&p, (bytes + 63) & ~63ull, s));

@@ -131,6 +131,16 @@ GTSC_HD int64_t sext(uint64_t u, int es)
     return (int64_t)(u << sh) >> sh;
 }
 
+#ifdef __CUDACC__
+// `a < b` in the element's own arithmetic (IEEE compare for floats: -0 < +0 is false, NaN false)
+__device__ __forceinline__ bool lt_native(uint64_t a, uint64_t b, int es, Order o)
+{
+    if (o == ORD_F32) return __uint_as_float((uint32_t)a) < __uint_as_float((uint32_t)b);
+    if (o == ORD_F64) return __longlong_as_double((long long)a) < __longlong_as_double((long long)b);
+    return sext(a, es) < sext(b, es);
+}
+#endif
+
 // BITLEN<T>(min, max) for signed integer T (core/cuda_macros.cuh:168-175)
 GTSC_HD int bitlen_signed(int64_t mn, int64_t mx, int es)
 {

@@ -14,4 +14,18 @@ DevBuf decode(int enc, int dt, const std::vector<View> &in, cudaStream_t s);
 int n_results(int enc);
 int return_type(int enc, int dt, int j);
 
+// DataStatistics (util/statistics/cuda_array_statistics.hpp:24-34)
+struct Stats {
+    double min;
+    double max;
+    int32_t min_bit_cnt;
+    int32_t precision;
+    int32_t sorted;
+    float rl_metric;
+    double mean;
+    uint64_t size;
+};
+// CudaArrayStatistics::GenerateStatistics (cuda_array_statistics.cu:141-179), one pass
+Stats column_stats(int dt, View in, cudaStream_t s);
+
 }  // namespace gtsc

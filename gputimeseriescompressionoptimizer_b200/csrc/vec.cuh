@@ -33,6 +33,16 @@ __device__ __forceinline__ uint64_t ld_elem(const uint8_t *p, uint64_t i)
     return __ldg((const unsigned long long *)p + i);
 }
 
+// Little-endian load of an ES-byte value at any address (metadata fields inside a blob).
+template <int ES>
+__device__ __forceinline__ uint64_t ld_unaligned(const uint8_t *p)
+{
+    uint64_t v = 0;
+#pragma unroll
+    for (int k = 0; k < ES; k++) v |= (uint64_t)__ldg(p + k) << (8 * k);
+    return v;
+}
+
 template <int ES>
 __device__ __forceinline__ void st_elem(uint8_t *p, uint64_t i, uint64_t v)
 {
@@ -54,12 +64,14 @@ __device__ __forceinline__ uint4 make_chunk(const uint64_t *v)
     uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int j = 0; j < 16 / ES; j++) {
-        if (ES == 8) {
+        if constexpr (ES == 8) {
             w[2 * j] = (uint32_t)v[j];
             w[2 * j + 1] = (uint32_t)(v[j] >> 32);
+        } else if constexpr (ES == 4) {
+            w[j] = (uint32_t)v[j];
         } else {
-            int word = (j * ES) >> 2, sh = ((j * ES) & 3) * 8;
-            uint32_t m = ES == 4 ? 0xffffffffu : ((1u << (8 * ES)) - 1);
+            const int word = (j * ES) >> 2, sh = ((j * ES) & 3) * 8;
+            constexpr uint32_t m = (1u << (8 * ES)) - 1;
             w[word] |= ((uint32_t)v[j] & m) << sh;
         }
     }

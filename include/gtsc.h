@@ -78,6 +78,68 @@ gtsc_status gtsc_encode(int32_t encoding, int32_t dtype, const void *d_in, uint6
 gtsc_status gtsc_decode(int32_t encoding, int32_t dtype, const gtsc_buffer in[3], uint32_t n_in,
                         gtsc_buffer *out, void *stream);
 
+/* DataStatistics (util/statistics/cuda_array_statistics.hpp:24-34) */
+typedef struct {
+    double min;
+    double max;
+    int32_t min_bit_cnt;
+    int32_t precision;
+    int32_t sorted;
+    float rl_metric;
+    double mean;
+    uint64_t size;
+} gtsc_data_statistics;
+
+/*
+ * CudaArrayStatistics::GenerateStatistics (util/statistics/cuda_array_statistics.cu:141-179):
+ * min, max, precision, sorted, RlMetric<T,2> and mean of a column in one pass over the data.
+ */
+gtsc_status gtsc_stats(int32_t dtype, const void *d_in, uint64_t in_bytes, gtsc_data_statistics *out,
+                       void *stream);
+
+/* ------------------------------------------------------------------ compression trees */
+
+/*
+ * Trees are pre-order node lists: node k = (nodes[2k] = EncodingType, nodes[2k+1] = DataType), each
+ * node followed by its GetNumberOfResults() child subtrees, every leaf `none` (a Fix()ed tree,
+ * tree/compression_node.cpp:209-223).
+ *
+ * PathGenerator::GenerateTree (optimizer/path_generator.cpp:70-91): builds the node list of a path
+ * of encoding types, children typed by GetReturnTypes.  Returns GTSC_ERR_CAPACITY when more than
+ * `cap` nodes would be written.
+ */
+gtsc_status gtsc_tree_from_path(const int16_t *encodings, int32_t n_encodings, int32_t dtype,
+                                int16_t *nodes_out, int32_t cap, int32_t *n_nodes);
+
+/* CompressionTree::Compress (tree/compression_tree.cpp:98-103): serialized blob of the column. */
+gtsc_status gtsc_tree_compress(const int16_t *nodes, int32_t n_nodes, const void *d_in, uint64_t in_bytes,
+                               gtsc_buffer *blob, void *stream);
+
+/* CompressionTree::Decompress (tree/compression_tree.cpp:105-155); *dtype = the root's data type. */
+gtsc_status gtsc_tree_decompress(const void *d_blob, uint64_t blob_bytes, gtsc_buffer *out, int32_t *dtype,
+                                 void *stream);
+
+/* CompressionTree::GetPredictedSizeAfterCompression (tree/compression_tree.cpp:157-160). */
+gtsc_status gtsc_tree_predict_size(const int16_t *nodes, int32_t n_nodes, const void *d_in, uint64_t in_bytes,
+                                   uint64_t *size, void *stream);
+
+/* ------------------------------------------------------------------ planners */
+
+/*
+ * The plain exhaustive planner: CompressionOptimizer::FullStatisticsUpdate on `d_sample` and the
+ * max-compression-ratio pick of CompressData (optimizer/compression_optimizer.cpp:88-182).  Writes the
+ * chosen Fix()ed tree and its candidate size (as the reference counts it).
+ */
+gtsc_status gtsc_plan_exhaustive(int32_t dtype, const void *d_sample, uint64_t sample_bytes, int16_t *nodes_out,
+                                 int32_t cap, int32_t *n_nodes, uint64_t *candidate_size, void *stream);
+
+/* CompressionOptimizer::OptimizeTree (optimizer/compression_optimizer.cpp:16-36): best of 30 paths. */
+gtsc_status gtsc_optimize_tree(int32_t dtype, const void *d_in, uint64_t in_bytes, int16_t *nodes_out,
+                               int32_t cap, int32_t *n_nodes, uint64_t *predicted_size, void *stream);
+
+/* GetSampleDataForFullUpdateSize (optimizer/compression_optimizer.cpp:148-154). */
+uint64_t gtsc_sample_bytes(int32_t dtype, uint64_t in_bytes);
+
 /* ------------------------------------------------------------------ kernel-level entry points */
 
 /*

@@ -31,12 +31,14 @@ static inline int32_t dev_f2i(double d)
     return (int32_t)d;
 }
 
-/* `int value = data[idx]` of _rlMetricKernel, then `value == data[idx+i]` in T arithmetic */
+/* `int value = data[idx]` of _rlMetricKernel, then `value == data[idx+i]` in T arithmetic.  The
+ * kernel runs on the device, so the conversion is the device's cvt.rzi.s32: measured on the B200,
+ * a float NaN converts to 0 and a double NaN to INT_MIN (tests/test_encodings_gpu.py pins both). */
 static inline int32_t rl_to_int(uint64_t u, int dt)
 {
     switch (dt) {
     case OR_FLOAT: return dev_f2i((double)bits_f32((uint32_t)u));
-    case OR_DOUBLE: return dev_f2i(bits_f64(u));
+    case OR_DOUBLE: { double d = bits_f64(u); return d != d ? INT32_MIN : dev_f2i(d); }
     case OR_TIME: return (int32_t)(uint32_t)u;
     default: return (int32_t)sext(u, es_of(dt));
     }

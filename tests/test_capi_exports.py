@@ -31,6 +31,14 @@ def test_library_exports_every_declared_symbol(G):
     assert not missing, f"not exported: {missing}"
 
 
+def test_python_binding_declares_every_signature(G):
+    """ctypes would silently truncate 64-bit arguments of an undeclared function."""
+    L = G.lib()
+    undeclared = [n for n in declared_symbols()
+                  if getattr(L, n).argtypes is None and n not in ("gtsc_last_error", "gtsc_version")]
+    assert not undeclared, f"no argtypes for {undeclared}"
+
+
 def test_version_and_sizes(G):
     assert G.lib().gtsc_version().startswith(b"gtsc")
     assert [G.dtype_size(d) for d in range(6)] == [1, 2, 4, 8, 4, 8]

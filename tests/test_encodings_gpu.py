@@ -1,0 +1,177 @@
+"""Every encoding on the GPU against the oracle: byte-identical streams, bit-exact decode (NaN
+payloads, +-0, +-inf included), and decode of the oracle's stream.  Mirrors the reference's
+per-encoding round-trip tests (compression/*/`*_unittest.cpp`) with byte-level checks added."""
+import numpy as np
+import pytest
+
+import oracle as OR
+
+pytestmark = pytest.mark.gpu
+
+INT_TYPES = [(OR.CHAR, np.int8), (OR.SHORT, np.int16), (OR.INT, np.int32), (OR.TIME, np.int64)]
+FP_TYPES = [(OR.FLOAT, np.float32), (OR.DOUBLE, np.float64)]
+ALL_TYPES = INT_TYPES + FP_TYPES
+SIZES = [0, 1, 2, 7, 33, 1000, 2049, 65537]
+
+
+def gen(kind, npt, n, rng):
+    """Seeded column generators covering the encodings' interesting cases."""
+    fp = np.issubdtype(npt, np.floating)
+    if kind == "uniform":
+        x = rng.normal(0, 1000, n) if fp else rng.integers(-100, 100, n)
+    elif kind == "walk":
+        x = np.cumsum(rng.integers(-8, 9, n)) + 1000
+        x = x / 100.0 if fp else x
+    elif kind == "runs":
+        x = np.repeat(rng.integers(0, 16, n + 1), rng.integers(1, 16, n + 1))[:n]
+        x = x / 4.0 if fp else x
+    elif kind == "const":
+        x = np.full(n, 7)
+    elif kind == "zipf":
+        x = np.minimum(rng.zipf(1.3, n), 5000) - 1
+    elif kind == "outliers":
+        x = rng.integers(0, 256, n)
+        k = max(n // 100, 0)
+        if k:
+            idx = rng.choice(n, k, replace=False)
+            x[idx] = rng.integers(0, 2 ** 14, k)
+    else:
+        raise ValueError(kind)
+    x = np.asarray(x)
+    if not fp:
+        info = np.iinfo(npt)
+        x = np.clip(x, info.min, info.max)
+    x = x.astype(npt)
+    if fp and n > 20:
+        # special values: NaN with payloads and both signs, infinities, signed zeros
+        bits = x.view(np.uint32 if npt == np.float32 else np.uint64)
+        if npt == np.float32:
+            bits[3], bits[9] = 0x7fc00001, 0xffa00005
+        else:
+            bits[3], bits[9] = 0x7ff8000000000123, 0xfff4000000000007
+        x[4], x[5], x[6], x[7] = np.inf, -np.inf, -0.0, 0.0
+    return x
+
+
+KINDS = ["uniform", "walk", "runs", "const", "zipf", "outliers"]
+
+
+def check_encoding(G, O, enc, dt, x):
+    dev = G.to_device(x)
+    parts = G.encode(enc, dt, dev)
+    host = [G.to_host(p) for p in parts]
+    expect = O.encode(enc, dt, x)
+    assert len(host) == len(expect), (OR.ENC_NAMES[enc], len(host), len(expect))
+    for k, (h, e) in enumerate(zip(host, expect)):
+        assert h.size == e.size and np.array_equal(h, e), \
+            f"{OR.ENC_NAMES[enc]} dt={dt} n={x.size} part {k}: sizes {h.size} vs {e.size}"
+    back = G.to_host(G.decode(enc, dt, parts))
+    assert back.tobytes() == x.tobytes(), f"{OR.ENC_NAMES[enc]} dt={dt} n={x.size} round trip"
+    # the GPU decodes the oracle's stream too
+    back2 = G.to_host(G.decode(enc, dt, [G.to_device(e) for e in expect]))
+    assert back2.tobytes() == x.tobytes()
+
+
+@pytest.mark.parametrize("dt,npt", ALL_TYPES)
+@pytest.mark.parametrize("enc", [OR.DELTA, OR.SCALE, OR.NONE])
+@pytest.mark.parametrize("n", SIZES)
+def test_elementwise_encodings(G, O, rng, enc, dt, npt, n):
+    for kind in ["uniform", "walk"]:
+        check_encoding(G, O, enc, dt, gen(kind, npt, n, rng))
+
+
+@pytest.mark.parametrize("dt,npt", ALL_TYPES)
+@pytest.mark.parametrize("enc", [OR.RLE, OR.DICT, OR.CONST, OR.PATCH])
+@pytest.mark.parametrize("n", SIZES)
+def test_split_and_run_encodings(G, O, rng, enc, dt, npt, n):
+    for kind in KINDS:
+        check_encoding(G, O, enc, dt, gen(kind, npt, n, rng))
+
+
+@pytest.mark.parametrize("dt,npt", ALL_TYPES)
+@pytest.mark.parametrize("n", SIZES + [32768, 32769, 100000])
+def test_gfc(G, O, rng, dt, npt, n):
+    for kind in ["uniform", "walk", "runs"]:
+        check_encoding(G, O, OR.GFC, dt, gen(kind, npt, n, rng))
+
+
+@pytest.mark.parametrize("dt,npt", ALL_TYPES)
+@pytest.mark.parametrize("n", SIZES)
+def test_float_to_int(G, O, rng, dt, npt, n):
+    for kind in ["uniform", "walk", "const"]:
+        x = gen(kind, npt, n, rng)
+        if np.issubdtype(npt, np.floating) and kind == "walk":
+            x = np.round(x.astype(np.float64), 2).astype(npt)
+        check_encoding(G, O, OR.FLOAT2INT, dt, x)
+
+
+def test_gfc_price_series(G, O, rng):
+    """GFC on the price-like series of the GFC workload (scaled down), float64 and float32."""
+    t = np.arange(1 << 18)
+    x = np.round(100 * np.sin(2 * np.pi * t / 1000) + rng.normal(0, 0.01, t.size), 2)
+    bits = x.view(np.uint64)
+    idx = rng.choice(x.size, x.size // 1000, replace=False)
+    bits[idx] = 0x7ff0000000000000 | rng.integers(1, 1 << 52, idx.size, dtype=np.uint64) | \
+        (rng.integers(0, 2, idx.size, dtype=np.uint64) << 63)
+    x[5], x[6], x[7] = np.inf, -np.inf, -0.0
+    check_encoding(G, O, OR.GFC, OR.DOUBLE, x)
+    check_encoding(G, O, OR.GFC, OR.FLOAT, x.astype(np.float32))
+
+
+@pytest.mark.parametrize("dt,npt", ALL_TYPES)
+@pytest.mark.parametrize("n", [1, 2, 3, 100, 10000, 70001])
+def test_statistics(G, O, rng, dt, npt, n):
+    for kind in KINDS:
+        x = gen(kind, npt, n, rng)
+        if np.issubdtype(npt, np.floating) and kind in ("walk", "uniform"):
+            x = np.round(x.astype(np.float64), 3).astype(npt)
+        got = G.stats(dt, G.to_device(x))
+        exp = O.stats(dt, x)
+        for f in ("min_bit_cnt", "precision", "sorted", "size"):
+            assert getattr(got, f) == getattr(exp, f), (f, kind, getattr(got, f), getattr(exp, f))
+        for f in ("min", "max"):
+            a, b = getattr(got, f), getattr(exp, f)
+            assert (np.isnan(a) and np.isnan(b)) or a == b, (f, kind, a, b)
+        assert got.rl_metric == exp.rl_metric, (kind, got.rl_metric, exp.rl_metric)
+        if np.issubdtype(npt, np.floating):
+            # floating sums are order dependent in the reference (thrust::reduce): the two
+            # summation orders may differ by the rounding bound 2*n*eps*mean(|x|)
+            if np.isfinite(exp.mean):
+                eps = np.finfo(npt).eps
+                tol = 2 * n * eps * float(np.mean(np.abs(x.astype(np.float64)))) + 1e-12
+                assert abs(got.mean - exp.mean) <= tol, (got.mean, exp.mean, tol)
+        else:
+            assert got.mean == exp.mean
+
+
+def test_precision_table_matches_glibc(G, O):
+    """The device logf table used for _getFloatPrecision equals the host KAT values."""
+    for k, v in enumerate([1.0, 0.1, 0.01, 0.001, 1e-4, 1e-5, 1e-6, 1e-7]):
+        x = np.full(64, 3 + v, np.float32)
+        assert G.stats(OR.FLOAT, G.to_device(x)).precision == O.stats(OR.FLOAT, x).precision
+
+
+def test_corrupt_streams_fail_cleanly(G, O, rng):
+    x = rng.integers(0, 100, 5000).astype(np.int32)
+    for enc in (OR.RLE, OR.DICT, OR.PATCH, OR.CONST, OR.GFC):
+        for dt, src in ((OR.INT, x), (OR.DOUBLE, x.astype(np.float64))):
+            parts = [G.to_host(p) for p in G.encode(enc, dt, G.to_device(src))]
+            for k in range(1, len(parts)):
+                if parts[k].size < 8:
+                    continue
+                cut = [G.to_device(p if j != k else p[: p.size // 2]) for j, p in enumerate(parts)]
+                try:
+                    G.decode(enc, dt, cut)
+                except G.GtscError as e:
+                    assert e.status in (-4, -3)
+
+
+@pytest.mark.parametrize("dt,npt,bits,expected", [
+    (OR.DOUBLE, np.float64, 0x7ff8000000000123, -2 ** 31), (OR.DOUBLE, np.float64, 0xfff4000000000007, -2 ** 31),
+    (OR.FLOAT, np.float32, 0x7fc00001, 0), (OR.FLOAT, np.float32, 0xffa00005, 0)])
+def test_device_nan_to_int_conversion(G, O, dt, npt, bits, expected):
+    """RlMetric converts `int value = data[idx]` on the device (cuda_array_statistics.cu:103): the
+    B200's conversion of NaN (INT_MIN for double, 0 for float) is what the oracle restates."""
+    x = np.array([0, expected, expected], npt)
+    x.view(np.uint64 if npt == np.float64 else np.uint32)[0] = bits
+    assert G.stats(dt, G.to_device(x)).rl_metric == 2.0 == O.stats(dt, x).rl_metric
