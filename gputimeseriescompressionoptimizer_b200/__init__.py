@@ -89,6 +89,7 @@ def lib():
         L.gtsc_optimize_tree.argtypes = [i32, vp, u64, i16p, i32, i32p, u64p, vp]
         L.gtsc_sample_bytes.argtypes = [i32, u64]
         L.gtsc_sample_bytes.restype = u64
+        L.gtsc_delta_decode_noalloc.argtypes = [i32, vp, vp, u64, vp, vp]
         _lib = L
     return _lib
 
