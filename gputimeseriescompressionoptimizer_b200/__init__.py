@@ -48,6 +48,11 @@ class Buffer(ctypes.Structure):
     _fields_ = [("ptr", ctypes.c_void_p), ("bytes", ctypes.c_uint64)]
 
 
+class Column(ctypes.Structure):
+    _fields_ = [("d_data", ctypes.c_void_p), ("bytes", ctypes.c_uint64), ("dtype", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
 class DataStatistics(ctypes.Structure):
     """DataStatistics (util/statistics/cuda_array_statistics.hpp:24-34)."""
     _fields_ = [("min", ctypes.c_double), ("max", ctypes.c_double),
@@ -90,6 +95,18 @@ def lib():
         L.gtsc_sample_bytes.argtypes = [i32, u64]
         L.gtsc_sample_bytes.restype = u64
         L.gtsc_delta_decode_noalloc.argtypes = [i32, vp, vp, u64, vp, vp]
+        L.gtsc_stream_create.argtypes = [ctypes.POINTER(vp)]
+        L.gtsc_stream_destroy.argtypes = [vp]
+        L.gtsc_batch_create.argtypes = [ctypes.POINTER(Column), ctypes.c_uint32, i16p, i32p,
+                                        ctypes.POINTER(vp), vp]
+        L.gtsc_batch_set_inputs.argtypes = [vp, ctypes.POINTER(vp), vp]
+        L.gtsc_batch_compress.argtypes = [vp, vp]
+        L.gtsc_batch_output.argtypes = [vp, ctypes.POINTER(vp), u64p, vp]
+        L.gtsc_batch_blob_sizes.argtypes = [vp, u64p, vp]
+        L.gtsc_batch_decompress.argtypes = [vp, vp, u64, ctypes.POINTER(vp), vp]
+        L.gtsc_batch_status.argtypes = [vp, vp]
+        L.gtsc_batch_launches.argtypes = [vp, i32]
+        L.gtsc_batch_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -243,3 +260,93 @@ def sample_bytes(dtype, nbytes):
 
 def tree_names(nodes):
     return [ENCODING_NAMES[e] for e in np.asarray(nodes)[::2]]
+
+
+# ------------------------------------------------------------------------ streams and batches
+class Stream:
+    """A non-blocking CUDA stream owned by the library (batched steps are captured on it)."""
+
+    def __init__(self):
+        p = ctypes.c_void_p()
+        check(lib().gtsc_stream_create(ctypes.byref(p)), "stream_create")
+        self.handle = p.value
+
+    def synchronize(self):
+        check(lib().gtsc_stream_synchronize(self.handle), "sync")
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.gtsc_stream_destroy(self.handle)
+            self.handle = None
+
+
+class Batch:
+    """Many columns with their trees, compressed / decompressed by the batched engine.
+
+    columns: DeviceBuffers (or objects with .ptr and .nbytes); dtypes: data type codes;
+    trees: node lists (int16 pairs) per column."""
+
+    def __init__(self, columns, dtypes, trees, stream):
+        self.stream = stream
+        self.n = len(columns)
+        cols = (Column * self.n)()
+        for i, (c, dt) in enumerate(zip(columns, dtypes)):
+            cols[i] = Column(c.ptr, c.nbytes, dt, 0)
+        counts = np.array([len(t) // 2 for t in trees], np.int32)
+        nodes = np.ascontiguousarray(np.concatenate([np.asarray(t, np.int16) for t in trees]))
+        h = ctypes.c_void_p()
+        check(lib().gtsc_batch_create(cols, self.n, nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
+                                      counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(h),
+                                      stream.handle), "batch_create")
+        self.handle = h.value
+        self.sizes = [c.nbytes for c in columns]
+
+    def set_inputs(self, columns):
+        arr = (ctypes.c_void_p * self.n)(*[c.ptr for c in columns])
+        check(lib().gtsc_batch_set_inputs(self.handle, arr, self.stream.handle), "batch_set_inputs")
+
+    def compress(self):
+        check(lib().gtsc_batch_compress(self.handle, self.stream.handle), "batch_compress")
+
+    def output(self):
+        """(device pointer, bytes) of the framed output of the last compress (synchronises)."""
+        p = ctypes.c_void_p()
+        b = ctypes.c_uint64(0)
+        check(lib().gtsc_batch_output(self.handle, ctypes.byref(p), ctypes.byref(b), self.stream.handle),
+              "batch_output")
+        return p.value, b.value
+
+    def blob_sizes(self):
+        out = np.zeros(self.n, np.uint64)
+        check(lib().gtsc_batch_blob_sizes(self.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                          self.stream.handle), "batch_blob_sizes")
+        return out
+
+    def decompress(self, framed_ptr, framed_bytes, outputs):
+        arr = (ctypes.c_void_p * self.n)(*[o.ptr for o in outputs])
+        check(lib().gtsc_batch_decompress(self.handle, framed_ptr, framed_bytes, arr, self.stream.handle),
+              "batch_decompress")
+
+    def status(self):
+        check(lib().gtsc_batch_status(self.handle, self.stream.handle), "batch step")
+
+    def launches(self, compress=True):
+        return lib().gtsc_batch_launches(self.handle, 1 if compress else 0)
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.gtsc_batch_destroy(self.handle)
+            self.handle = None
+
+
+def split_framed(framed):
+    """Split a framed host buffer (uint64 column count, uint64 blob bytes per column, blobs)."""
+    framed = np.ascontiguousarray(framed, np.uint8)
+    nc = int(framed[:8].view(np.uint64)[0])
+    lens = framed[8:8 + 8 * nc].view(np.uint64).astype(np.int64)
+    pos = 8 + 8 * nc
+    blobs = []
+    for n in lens:
+        blobs.append(framed[pos:pos + n])
+        pos += n
+    return blobs

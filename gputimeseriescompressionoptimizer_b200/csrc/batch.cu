@@ -1,0 +1,791 @@
+// batch.cu -- compiles many columns' compression trees into stages of batched passes, owns their
+// device memory, and records each step (compress / decompress) once as a CUDA graph.
+//
+// Compile: every node of every tree gets its output streams with worst-case capacities (computed
+// from the column length), a scratch area (accumulators, look-back state, hash table, GFC layout)
+// and a list of passes.  A pass's level is one more than the pass it waits for (the previous pass of
+// its node, or the pass that produced its input); passes with the same (level, kind) form one
+// launch over all columns.  Capacities only bound memory and grids: the real lengths are written
+// by the passes into the device stream table, so a step never waits for the host.
+#include "batch.hpp"
+#include "encodings.hpp"
+#include "kernels.hpp"
+#include "scan.cuh"
+
+#include <algorithm>
+#include <map>
+#include <tuple>
+
+namespace gtsc {
+
+namespace {
+
+__global__ void k_set_streams(const unsigned long long *vals, const int *sids, int n, StreamDesc *S)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    S[sids[i]].ptr = (uint8_t *)vals[2 * i];
+    S[sids[i]].len = vals[2 * i + 1];
+}
+
+uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+uint64_t cdiv(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
+
+struct HNode {
+    int col = 0, enc = 0, dt = 0, es = 0;
+    int parent = -1;
+    std::vector<int> kids;
+    int in_sid = -1;                  // compress input
+    int out_sid[3] = {-1, -1, -1};    // compress outputs: meta, out1, out2
+    int dec_meta_sid = -1;            // decode: the node's metadata inside the blob
+    int dec_data_sid = -1;            // decode (none leaves): the data inside the blob
+    int dec_out_sid = -1;             // decode: this node's decoded stream
+    uint64_t in_cap = 0;              // bytes
+    uint64_t scratch = 0;             // offset in the arena
+    uint64_t c_bytes = 0, d_bytes = 0;
+    // compress scratch layout
+    uint64_t lb_off = 64, tab_off = 0, starts_off = 0, g_sizes = 0, g_incl = 0, g_layout = 0, tab_cap = 0;
+    uint64_t hist_tiles = 0, split_tiles = 0, gfc_warps = 0;
+    // decode scratch layout (relative to scratch)
+    uint64_t dlb_off = 0, dends_off = 0, druns_off = 0, dsizes_off = 0, dincl_off = 0;
+    int last_c_level = 0, last_d_level = 0;
+};
+
+struct Pass {
+    int level;
+    int op;
+    int node;
+    BItem item;
+};
+
+struct Launch {
+    int op;
+    int first, count;
+    uint64_t tiles;
+};
+
+uint64_t gfc_warps_for(bool dbl, uint64_t n)
+{
+    const uint64_t wpb = dbl ? 16 : 32;
+    const uint64_t bs = wpb * (dbl ? 64 : 32) * 32;
+    return cdiv(n, bs) * wpb;
+}
+
+}  // namespace
+
+class BatchEngine {
+public:
+    std::vector<HNode> nodes;
+    std::vector<StreamDesc> streams;        // host image of the table
+    std::vector<int> col_root;              // root node of each column
+    std::vector<int> col_in_sid, col_out_sid;
+    std::vector<uint64_t> col_bytes;
+    std::vector<BColumnDev> cols_dev;
+    std::vector<BNodeDev> nodes_c, nodes_d;  // framing (compress) / parse (decode) node tables
+    std::vector<Pass> pass_c, pass_d;
+    std::vector<BItem> items_c, items_d, items_copy;
+    std::vector<Launch> launch_c, launch_d;
+    uint64_t copy_tiles = 0, framed_cap = 0;
+    std::vector<unsigned long long> zero_c, zero_d;  // (ptr, bytes) pairs
+    std::vector<std::pair<uint64_t, uint64_t>> hist_tables;  // (offset, cap) to initialise
+
+    DevBuf arena, tables;
+    StreamDesc *d_streams = nullptr;
+    BItem *d_items_c = nullptr, *d_items_d = nullptr, *d_items_copy = nullptr;
+    BColumnDev *d_cols = nullptr;
+    BNodeDev *d_nodes_c = nullptr, *d_nodes_d = nullptr;
+    unsigned long long *d_col_off = nullptr, *d_col_off_d = nullptr, *d_total = nullptr;
+    unsigned long long *d_zero_c = nullptr, *d_zero_d = nullptr;
+    unsigned long long *d_set_vals = nullptr, *d_frame_len = nullptr;
+    int *d_set_sids = nullptr;
+    uint8_t **d_frame_ptr = nullptr;
+    uint32_t *d_status = nullptr, *d_counters = nullptr;
+    uint8_t *d_framed = nullptr;
+    int n_counters = 0;
+    cudaGraphExec_t graph_c = nullptr, graph_d = nullptr;
+
+    int new_stream(uint64_t cap)
+    {
+        streams.push_back(StreamDesc{nullptr, 0, cap, 0});
+        return (int)streams.size() - 1;
+    }
+
+    void build_node(const Tree &t, int &k, int col, int parent, int in_sid, uint64_t in_cap, int depth);
+    void plan_passes();
+    void layout(cudaStream_t s);
+    void capture(cudaStream_t s);
+    void record_compress(cudaStream_t s);
+    void record_decompress(cudaStream_t s);
+};
+
+// ---------------------------------------------------------------------------------- compile
+
+void BatchEngine::build_node(const Tree &t, int &k, int col, int parent, int in_sid, uint64_t in_cap, int depth)
+{
+    if (k >= t.size() || depth > 64) fail(GTSC_ERR_ARG, "batch: incomplete tree");
+    HNode nd;
+    nd.col = col;
+    nd.enc = t.enc[k];
+    nd.dt = t.dt[k];
+    nd.es = dtype_size(nd.dt);
+    nd.parent = parent;
+    nd.in_sid = in_sid;
+    nd.in_cap = in_cap;
+    ++k;
+    const int id = (int)nodes.size();
+    nodes.push_back(nd);
+    if (parent >= 0) nodes[parent].kids.push_back(id);
+    HNode &me = nodes[id];
+    const uint64_t es = me.es, n = in_cap / es;
+    uint64_t cap[3] = {0, 0, 0};
+    switch (me.enc) {
+    case GTSC_NONE: break;
+    case GTSC_DELTA: case GTSC_SCALE: cap[0] = es; cap[1] = in_cap; break;
+    case GTSC_AFL: cap[0] = 4; cap[1] = in_cap + es; break;
+    case GTSC_RLE: cap[0] = 4; cap[1] = 4 * n; cap[2] = in_cap; break;
+    case GTSC_DICT: cap[0] = 2 + cdiv(n, 8); cap[1] = 20 + 4 * es + 4 * cdiv(n, 16); cap[2] = in_cap; break;
+    case GTSC_CONST: cap[0] = es + 2 + cdiv(n, 8); cap[1] = in_cap; break;
+    case GTSC_PATCH: cap[0] = 2 + cdiv(n, 8); cap[1] = in_cap; cap[2] = in_cap; break;
+    case GTSC_FLOAT_TO_INT: cap[0] = 4; cap[1] = std::max<uint64_t>(4 * n, in_cap); break;
+    case GTSC_GFC:
+        if (is_fp(me.dt)) {
+            cap[0] = 12;
+            cap[1] = 4 * gfc_warps_for(me.dt == GTSC_DOUBLE, n);
+            cap[2] = cdiv((n + 31) & ~31ull, 32) * (16 + 32 * es);
+        } else {
+            cap[0] = 4;
+            cap[1] = in_cap + es;
+        }
+        break;
+    default: fail(GTSC_ERR_ARG, "batch: unsupported encoding in tree");
+    }
+    const int r = n_results(me.enc);
+    if (me.enc != GTSC_NONE)
+        for (int j = 0; j <= r; j++) nodes[id].out_sid[j] = new_stream(cap[j]);
+    // decode-side streams
+    if (nodes[id].enc == GTSC_NONE) nodes[id].dec_data_sid = new_stream(0);
+    else nodes[id].dec_meta_sid = new_stream(0);
+    if (parent >= 0) nodes[id].dec_out_sid = new_stream(in_cap);
+    for (int j = 0; j < r; j++) build_node(t, k, col, id, nodes[id].out_sid[j + 1], cap[j + 1], depth + 1);
+}
+
+void BatchEngine::plan_passes()
+{
+    // scratch sizes
+    for (auto &nd : nodes) {
+        const uint64_t n = nd.in_cap / nd.es;
+        uint64_t c = 64;
+        switch (nd.enc) {
+        case GTSC_PATCH:
+            nd.split_tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
+            c = 64 + align_up(lookback_bytes(nd.split_tiles), 256);
+            break;
+        case GTSC_DICT: case GTSC_CONST: {
+            nd.split_tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
+            nd.hist_tiles = std::max<uint64_t>(1, cdiv(n, kBHistTile));
+            uint64_t cap = 1024;
+            while (cap < 2 * n + 64) cap <<= 1;
+            nd.tab_cap = cap;
+            nd.tab_off = 64 + align_up(lookback_bytes(nd.split_tiles), 256);
+            c = nd.tab_off + align_up(bhist_bytes(cap, nd.hist_tiles), 256);
+            break;
+        }
+        case GTSC_RLE:
+            nd.split_tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
+            nd.starts_off = 64 + align_up(lookback_bytes(nd.split_tiles), 256);
+            c = nd.starts_off + align_up(4 * n + 16, 256);
+            break;
+        case GTSC_FLOAT_TO_INT: c = 128; break;
+        case GTSC_GFC:
+            if (is_fp(nd.dt)) {
+                const bool dbl = nd.dt == GTSC_DOUBLE;
+                nd.gfc_warps = gfc_warps_for(dbl, n);
+                const uint64_t scan_tiles = std::max<uint64_t>(1, cdiv(nd.gfc_warps, kBTile));
+                nd.g_sizes = 64 + align_up(lookback_bytes(scan_tiles), 256);
+                nd.g_incl = nd.g_sizes + align_up(4 * nd.gfc_warps + 16, 256);
+                nd.g_layout = nd.g_incl + align_up(8 * nd.gfc_warps + 16, 256);
+                c = nd.g_layout + align_up(((n + 31) & ~31ull) / 2 * (dbl ? 17 : 9) + 64, 256);
+            }
+            break;
+        default: break;
+        }
+        nd.c_bytes = align_up(c, 256);
+        // decode scratch (after the compress scratch, which keeps the hash tables clean)
+        uint64_t d = 0;
+        const uint64_t tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
+        switch (nd.enc) {
+        case GTSC_DELTA: case GTSC_PATCH: case GTSC_DICT: case GTSC_CONST:
+            nd.dlb_off = nd.c_bytes;
+            d = align_up(lookback_bytes(tiles), 256);
+            break;
+        case GTSC_RLE:
+            nd.dlb_off = nd.c_bytes;
+            nd.dends_off = nd.dlb_off + align_up(lookback_bytes(tiles), 256);
+            nd.druns_off = nd.dends_off + align_up(8 * n + 16, 256);
+            d = nd.druns_off + 256 - nd.c_bytes;
+            break;
+        case GTSC_GFC:
+            if (is_fp(nd.dt)) {
+                const uint64_t scan_tiles = std::max<uint64_t>(1, cdiv(nd.gfc_warps, kBTile));
+                nd.dlb_off = nd.c_bytes;
+                nd.dsizes_off = nd.dlb_off + align_up(lookback_bytes(scan_tiles), 256);
+                nd.dincl_off = nd.dsizes_off + align_up(4 * nd.gfc_warps + 16, 256);
+                d = nd.dincl_off + align_up(8 * nd.gfc_warps + 16, 256) - nd.c_bytes;
+            }
+            break;
+        default: break;
+        }
+        nd.d_bytes = align_up(d, 256);
+    }
+
+    auto base_item = [](const HNode &nd, int op, uint64_t tiles) {
+        BItem it{};
+        it.op = (int16_t)op;
+        it.es = (int16_t)nd.es;
+        it.order = (int16_t)ORD_INT;
+        it.dt = nd.dt;
+        it.tiles = (uint32_t)std::max<uint64_t>(1, tiles);
+        for (int j = 0; j < 3; j++) {
+            it.in[j] = -1;
+            it.out[j] = nd.out_sid[j];
+        }
+        it.in[0] = nd.in_sid;
+        return it;
+    };
+
+    // ---------------- compress passes (parents before children)
+    for (size_t id = 0; id < nodes.size(); id++) {
+        HNode &nd = nodes[id];
+        const int start = nd.parent >= 0 ? nodes[nd.parent].last_c_level + 1 : 0;
+        const uint64_t n = nd.in_cap / nd.es;
+        const uint64_t t2k = cdiv(n, kBTile);
+        std::vector<BItem> ps;
+        auto add = [&](BItem it) { ps.push_back(it); };
+        switch (nd.enc) {
+        case GTSC_NONE: break;
+        case GTSC_DELTA: add(base_item(nd, B_DELTA_ENC, t2k)); break;
+        case GTSC_SCALE:
+            add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+            add(base_item(nd, B_SCALE_SUB, t2k));
+            break;
+        case GTSC_AFL:
+            add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+            add(base_item(nd, B_AFL_PACK, t2k));
+            break;
+        case GTSC_PATCH: {
+            BItem mm = base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile));
+            mm.order = (int16_t)native_order(nd.dt);
+            add(mm);
+            BItem sp = base_item(nd, B_SPLIT, nd.split_tiles);
+            sp.order = (int16_t)native_order(nd.dt);
+            sp.mode = SPLIT_LOWER;
+            sp.p[0] = 64;
+            add(sp);
+            break;
+        }
+        case GTSC_DICT: case GTSC_CONST: {
+            const int k = nd.enc == GTSC_DICT ? 4 : 1;
+            BItem h = base_item(nd, B_HIST, nd.hist_tiles);
+            h.order = (int16_t)native_order(nd.dt);
+            h.mode = (int16_t)k;
+            h.p[0] = nd.tab_cap;
+            h.p[1] = nd.hist_tiles;
+            h.p[2] = nd.tab_off;
+            add(h);
+            BItem tk = h;
+            tk.op = B_TOPK;
+            tk.tiles = 1;
+            add(tk);
+            BItem sp = base_item(nd, B_SPLIT, nd.split_tiles);
+            sp.order = (int16_t)native_order(nd.dt);
+            sp.mode = (int16_t)(nd.enc == GTSC_DICT ? SPLIT_DICT : SPLIT_NOT_CONST);
+            sp.p[0] = 64;
+            add(sp);
+            break;
+        }
+        case GTSC_RLE: {
+            BItem h = base_item(nd, B_RLE_HEADS, nd.split_tiles);
+            h.order = (int16_t)native_order(nd.dt);
+            h.p[0] = 64;
+            h.p[1] = nd.starts_off;
+            add(h);
+            BItem l = h;
+            l.op = B_RLE_LENGTHS;
+            add(l);
+            break;
+        }
+        case GTSC_FLOAT_TO_INT: {
+            BItem s1 = base_item(nd, B_F2I_STATS, t2k);
+            s1.order = (int16_t)native_order(nd.dt);
+            add(s1);
+            BItem s2 = s1;
+            s2.op = B_F2I_ENC;
+            add(s2);
+            BItem s3 = s1;
+            s3.op = B_F2I_RAW;
+            add(s3);
+            break;
+        }
+        case GTSC_GFC:
+            if (is_fp(nd.dt)) {
+                BItem g = base_item(nd, B_GFC_COMPRESS, cdiv(nd.gfc_warps, kBGfcChunks));
+                g.p[0] = 64;
+                g.p[1] = nd.g_sizes;
+                g.p[2] = nd.g_incl;
+                g.p[3] = nd.g_layout;
+                add(g);
+                BItem sc = g;
+                sc.op = B_GFC_SCAN;
+                sc.mode = 0;
+                sc.tiles = (uint32_t)std::max<uint64_t>(1, cdiv(nd.gfc_warps, kBTile));
+                add(sc);
+                BItem cp = g;
+                cp.op = B_GFC_COMPACT;
+                add(cp);
+            } else {
+                add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+                add(base_item(nd, B_AFL_PACK, t2k));
+            }
+            break;
+        default: break;
+        }
+        int lvl = start;
+        for (auto &it : ps) pass_c.push_back(Pass{lvl++, it.op, (int)id, it});
+        nd.last_c_level = ps.empty() ? start - 1 : lvl - 1;
+    }
+
+    // ---------------- decode passes (children before parents)
+    std::vector<int> order(nodes.size());
+    for (size_t i = 0; i < nodes.size(); i++) order[i] = (int)i;
+    // post-order by depth: process nodes with larger ids first works for pre-order trees
+    std::reverse(order.begin(), order.end());
+    for (int id : order) {
+        HNode &nd = nodes[id];
+        int start = 0;
+        for (int kid : nd.kids)
+            if (nodes[kid].enc != GTSC_NONE) start = std::max(start, nodes[kid].last_d_level + 1);
+        const uint64_t n = nd.in_cap / nd.es;
+        const uint64_t t2k = std::max<uint64_t>(1, cdiv(n, kBTile));
+        auto child_out = [&](int j) {
+            const int kid = nd.kids[j];
+            return nodes[kid].enc == GTSC_NONE ? nodes[kid].dec_data_sid : nodes[kid].dec_out_sid;
+        };
+        auto ditem = [&](int op, uint64_t tiles) {
+            BItem it{};
+            it.op = (int16_t)op;
+            it.es = (int16_t)nd.es;
+            it.order = (int16_t)native_order(nd.dt);
+            it.dt = nd.dt;
+            it.tiles = (uint32_t)std::max<uint64_t>(1, tiles);
+            for (int j = 0; j < 3; j++) it.in[j] = it.out[j] = -1;
+            it.in[0] = nd.dec_meta_sid;
+            for (size_t j = 0; j < nd.kids.size() && j < 2; j++) it.in[j + 1] = child_out((int)j);
+            it.out[0] = nd.dec_out_sid;
+            return it;
+        };
+        std::vector<BItem> ps;
+        switch (nd.enc) {
+        case GTSC_NONE:
+            if (nd.parent < 0) {  // a lone none root: copy the data out
+                BItem it = ditem(B_NONE_COPY, cdiv(nd.in_cap, batch_copy_piece()));
+                it.in[0] = nd.dec_data_sid;
+                ps.push_back(it);
+            }
+            break;
+        case GTSC_AFL: ps.push_back(ditem(B_AFL_UNPACK, t2k)); break;
+        case GTSC_DELTA: { BItem it = ditem(B_DELTA_DEC, t2k); it.p[0] = nd.dlb_off; ps.push_back(it); break; }
+        case GTSC_SCALE: ps.push_back(ditem(B_SCALE_ADD, t2k)); break;
+        case GTSC_PATCH: case GTSC_DICT: case GTSC_CONST: {
+            BItem it = ditem(B_MERGE, t2k);
+            it.mode = (int16_t)(nd.enc == GTSC_PATCH ? SPLIT_LOWER : nd.enc == GTSC_DICT ? SPLIT_DICT : SPLIT_NOT_CONST);
+            it.p[0] = nd.dlb_off;
+            ps.push_back(it);
+            break;
+        }
+        case GTSC_RLE: {
+            BItem it = ditem(B_RLE_SCAN, t2k);
+            it.p[0] = nd.dlb_off;
+            it.p[1] = nd.dends_off;
+            it.p[2] = nd.druns_off;
+            ps.push_back(it);
+            BItem ex = it;
+            ex.op = B_RLE_EXPAND;
+            ps.push_back(ex);
+            break;
+        }
+        case GTSC_FLOAT_TO_INT: ps.push_back(ditem(B_F2I_DEC, t2k)); break;
+        case GTSC_GFC:
+            if (is_fp(nd.dt)) {
+                const uint64_t st = std::max<uint64_t>(1, cdiv(nd.gfc_warps, kBTile));
+                BItem a = ditem(B_GFC_SIZES, st);
+                a.p[0] = nd.dlb_off;
+                a.p[1] = nd.dsizes_off;
+                a.p[2] = nd.dincl_off;
+                a.p[3] = nd.gfc_warps;
+                ps.push_back(a);
+                BItem b = a;
+                b.op = B_GFC_SCAN;
+                b.mode = 1;
+                ps.push_back(b);
+                BItem c = a;
+                c.op = B_GFC_DEC;
+                c.tiles = (uint32_t)std::max<uint64_t>(1, cdiv(nd.gfc_warps, kBGfcChunks));
+                ps.push_back(c);
+            } else {
+                ps.push_back(ditem(B_AFL_UNPACK, t2k));
+            }
+            break;
+        default: break;
+        }
+        int lvl = start;
+        for (auto &it : ps) pass_d.push_back(Pass{lvl++, it.op, id, it});
+        nd.last_d_level = ps.empty() ? start - 1 : lvl - 1;
+    }
+}
+
+void BatchEngine::layout(cudaStream_t s)
+{
+    // arena: node scratch, then streams
+    uint64_t off = 0;
+    for (auto &nd : nodes) {
+        nd.scratch = off;
+        off += nd.c_bytes + nd.d_bytes;
+    }
+    std::vector<uint64_t> sid_off(streams.size(), UINT64_MAX);
+    for (size_t i = 0; i < streams.size(); i++) {
+        if (streams[i].cap == 0) continue;
+        sid_off[i] = off;
+        off += align_up(streams[i].cap + 64, 256);
+    }
+    framed_cap = 8 + 8 * (uint64_t)col_root.size();  // column count and directory
+    for (auto &nd : nodes) {
+        framed_cap += 16;
+        if (nd.enc != GTSC_NONE) framed_cap += streams[nd.out_sid[0]].cap;
+        else framed_cap += nd.in_cap;
+    }
+    const uint64_t framed_off = off;
+    off += align_up(framed_cap + 64, 256);
+    arena = dev_alloc(off, s);
+    GTSC_CUDA(cudaMemsetAsync(arena.get(), 0, off, s));
+    uint8_t *A = arena.get();
+    d_framed = A + framed_off;
+    for (size_t i = 0; i < streams.size(); i++)
+        if (sid_off[i] != UINT64_MAX) streams[i].ptr = A + sid_off[i];
+    for (size_t c = 0; c < col_root.size(); c++) {
+        streams[col_in_sid[c]].len = col_bytes[c];
+        streams[col_out_sid[c]].cap = col_bytes[c];
+    }
+    // hash tables start empty: keys all ones
+    for (auto &nd : nodes)
+        if (nd.tab_cap) {
+            GTSC_CUDA(cudaMemsetAsync(A + nd.scratch + nd.tab_off + 16, 0xff, 8 * nd.tab_cap, s));
+        }
+
+    // items: patch scratch offsets into device addresses, group into launches
+    auto build = [&](std::vector<Pass> &ps, std::vector<BItem> &items, std::vector<Launch> &launches) {
+        std::stable_sort(ps.begin(), ps.end(), [](const Pass &a, const Pass &b) {
+            return std::make_tuple(a.level, a.op) < std::make_tuple(b.level, b.op);
+        });
+        for (size_t i = 0; i < ps.size();) {
+            size_t j = i;
+            Launch L{ps[i].op, (int)items.size(), 0, 0};
+            while (j < ps.size() && ps[j].level == ps[i].level && ps[j].op == ps[i].op) {
+                BItem it = ps[j].item;
+                it.scratch = A + nodes[ps[j].node].scratch;
+                it.tile_base = L.tiles;
+                L.tiles += it.tiles;
+                items.push_back(it);
+                j++;
+            }
+            L.count = (int)items.size() - L.first;
+            launches.push_back(L);
+            i = j;
+        }
+    };
+    build(pass_c, items_c, launch_c);
+    build(pass_d, items_d, launch_d);
+
+    // zero ranges per step
+    auto zr = [](std::vector<unsigned long long> &z, uint8_t *p, uint64_t bytes) {
+        z.push_back((unsigned long long)(uintptr_t)p);
+        z.push_back(align_up(bytes, 4));
+    };
+    for (auto &nd : nodes) {
+        uint8_t *sc = A + nd.scratch;
+        zr(zero_c, sc, 64);
+        if (nd.enc == GTSC_FLOAT_TO_INT) zr(zero_c, sc + 64, 64);
+        if (nd.split_tiles) zr(zero_c, sc + 64, lookback_zero_bytes(nd.split_tiles));
+        if (nd.gfc_warps) zr(zero_c, sc + 64, lookback_zero_bytes(std::max<uint64_t>(1, cdiv(nd.gfc_warps, kBTile))));
+        const uint64_t n = nd.in_cap / nd.es;
+        const uint64_t t2k = std::max<uint64_t>(1, cdiv(n, kBTile));
+        switch (nd.enc) {
+        case GTSC_DELTA: case GTSC_PATCH: case GTSC_DICT: case GTSC_CONST: case GTSC_RLE:
+            zr(zero_d, sc + nd.dlb_off, lookback_zero_bytes(t2k));
+            break;
+        case GTSC_GFC:
+            if (nd.gfc_warps) zr(zero_d, sc + nd.dlb_off, lookback_zero_bytes(std::max<uint64_t>(1, cdiv(nd.gfc_warps, kBTile))));
+            break;
+        default: break;
+        }
+    }
+
+    // framing tables
+    for (size_t c = 0; c < col_root.size(); c++) {
+        BColumnDev cd;
+        cd.first = (int)nodes_c.size();
+        int cnt = 0;
+        for (size_t id = 0; id < nodes.size(); id++) {
+            if (nodes[id].col != (int)c) continue;
+            const HNode &nd = nodes[id];
+            BNodeDev a{nd.enc, nd.dt, nd.enc == GTSC_NONE ? -1 : nd.out_sid[0], nd.enc == GTSC_NONE ? nd.in_sid : -1, 0, 0};
+            BNodeDev b{nd.enc, nd.dt, nd.dec_meta_sid, nd.dec_data_sid, 0, 0};
+            nodes_c.push_back(a);
+            nodes_d.push_back(b);
+            cnt++;
+        }
+        cd.n_nodes = cnt;
+        cols_dev.push_back(cd);
+    }
+    // copy items: every metadata and every none leaf's data
+    for (size_t k = 0; k < nodes_c.size(); k++) {
+        const BNodeDev &nd = nodes_c[k];
+        for (int which = 0; which < 2; which++) {
+            const int sid = which ? nd.data : nd.meta;
+            if (sid < 0) continue;
+            const uint64_t cap = streams[sid].cap;
+            BItem it{};
+            it.tiles = (uint32_t)std::max<uint64_t>(1, cdiv(cap, batch_copy_piece()));
+            it.tile_base = copy_tiles;
+            it.p[0] = k;
+            it.p[1] = (uint64_t)which;
+            copy_tiles += it.tiles;
+            items_copy.push_back(it);
+        }
+    }
+    // counters: one per launch
+    n_counters = (int)(launch_c.size() + launch_d.size()) + 4;
+
+    // device tables in one allocation
+    auto sz = [](size_t n, size_t e) { return align_up(n * e + 16, 256); };
+    uint64_t t_off = 0;
+    const uint64_t o_streams = t_off; t_off += sz(streams.size(), sizeof(StreamDesc));
+    const uint64_t o_ic = t_off; t_off += sz(items_c.size(), sizeof(BItem));
+    const uint64_t o_id = t_off; t_off += sz(items_d.size(), sizeof(BItem));
+    const uint64_t o_icp = t_off; t_off += sz(items_copy.size(), sizeof(BItem));
+    const uint64_t o_cols = t_off; t_off += sz(cols_dev.size(), sizeof(BColumnDev));
+    const uint64_t o_nc = t_off; t_off += sz(nodes_c.size(), sizeof(BNodeDev));
+    const uint64_t o_nd = t_off; t_off += sz(nodes_d.size(), sizeof(BNodeDev));
+    const uint64_t o_coloff = t_off; t_off += sz(col_root.size() + 1, 8);
+    const uint64_t o_coloff_d = t_off; t_off += sz(col_root.size() + 1, 8);
+    const uint64_t o_total = t_off; t_off += 256;
+    const uint64_t o_zc = t_off; t_off += sz(zero_c.size() + 8, 8);
+    const uint64_t o_zd = t_off; t_off += sz(zero_d.size() + 8, 8);
+    // (pointer, length) pairs: the inputs of compress, then the outputs of decompress
+    const uint64_t o_setv = t_off; t_off += sz(4 * col_root.size() + 2, 8);
+    const uint64_t o_sets = t_off; t_off += sz(2 * col_root.size() + 2, 4);
+    const uint64_t o_frame = t_off; t_off += 256;
+    const uint64_t o_status = t_off; t_off += 256;
+    const uint64_t o_counters = t_off; t_off += sz(n_counters, 4);
+    tables = dev_alloc(t_off, s);
+    uint8_t *T = tables.get();
+    GTSC_CUDA(cudaMemsetAsync(T, 0, t_off, s));
+    d_streams = (StreamDesc *)(T + o_streams);
+    d_items_c = (BItem *)(T + o_ic);
+    d_items_d = (BItem *)(T + o_id);
+    d_items_copy = (BItem *)(T + o_icp);
+    d_cols = (BColumnDev *)(T + o_cols);
+    d_nodes_c = (BNodeDev *)(T + o_nc);
+    d_nodes_d = (BNodeDev *)(T + o_nd);
+    d_col_off = (unsigned long long *)(T + o_coloff);
+    d_col_off_d = (unsigned long long *)(T + o_coloff_d);
+    d_total = (unsigned long long *)(T + o_total);
+    d_zero_c = (unsigned long long *)(T + o_zc);
+    d_zero_d = (unsigned long long *)(T + o_zd);
+    d_set_vals = (unsigned long long *)(T + o_setv);
+    d_set_sids = (int *)(T + o_sets);
+    d_frame_ptr = (uint8_t **)(T + o_frame);
+    d_frame_len = (unsigned long long *)(T + o_frame + 8);
+    d_status = (uint32_t *)(T + o_status);
+    d_counters = (uint32_t *)(T + o_counters);
+    // the status word and the counters are zeroed with the other ranges at each step
+    zr(zero_c, (uint8_t *)d_status, 8);   // [0] error code, [1] decode: the frames did not parse
+    zr(zero_d, (uint8_t *)d_status, 8);
+    zr(zero_c, (uint8_t *)d_counters, 4ull * n_counters);
+    zr(zero_d, (uint8_t *)d_counters, 4ull * n_counters);
+    auto h2d = [&](void *dst, const void *src, size_t bytes) {
+        if (bytes) GTSC_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    };
+    h2d(d_streams, streams.data(), streams.size() * sizeof(StreamDesc));
+    h2d(d_items_c, items_c.data(), items_c.size() * sizeof(BItem));
+    h2d(d_items_d, items_d.data(), items_d.size() * sizeof(BItem));
+    h2d(d_items_copy, items_copy.data(), items_copy.size() * sizeof(BItem));
+    h2d(d_cols, cols_dev.data(), cols_dev.size() * sizeof(BColumnDev));
+    h2d(d_nodes_c, nodes_c.data(), nodes_c.size() * sizeof(BNodeDev));
+    h2d(d_nodes_d, nodes_d.data(), nodes_d.size() * sizeof(BNodeDev));
+    h2d(d_zero_c, zero_c.data(), zero_c.size() * 8);
+    h2d(d_zero_d, zero_d.data(), zero_d.size() * 8);
+    GTSC_CUDA(cudaStreamSynchronize(s));
+}
+
+void BatchEngine::record_compress(cudaStream_t s)
+{
+    const int nc = (int)col_root.size();
+    k_set_streams<<<(nc + 127) / 128, 128, 0, s>>>(d_set_vals, d_set_sids, nc, d_streams);
+    launch_zero_ranges(d_zero_c, (int)zero_c.size() / 2, s);
+    int ctr = 0;
+    for (auto &L : launch_c)
+        launch_batch_stage(L.op, d_items_c + L.first, L.count, L.tiles, d_streams, d_counters + ctr++, d_status, s);
+    launch_frame_sizes(d_cols, nc, d_nodes_c, d_streams, d_col_off, d_total, d_framed, s);
+    launch_frame_layout(d_cols, nc, d_nodes_c, d_streams, d_col_off, d_framed, s);
+    launch_frame_copy(d_items_copy, (int)items_copy.size(), copy_tiles, d_nodes_c, d_streams, d_framed, s);
+}
+
+void BatchEngine::record_decompress(cudaStream_t s)
+{
+    const int nc = (int)col_root.size();
+    k_set_streams<<<(nc + 127) / 128, 128, 0, s>>>(d_set_vals + 2 * nc, d_set_sids + nc, nc, d_streams);
+    launch_zero_ranges(d_zero_d, (int)zero_d.size() / 2, s);
+    launch_parse_frames(d_cols, nc, d_nodes_d, d_streams, d_col_off_d, (const uint8_t *const *)d_frame_ptr,
+                        d_frame_len, d_status, s);
+    int ctr = (int)launch_c.size();
+    for (auto &L : launch_d)
+        launch_batch_stage(L.op, d_items_d + L.first, L.count, L.tiles, d_streams, d_counters + ctr++, d_status, s);
+}
+
+void BatchEngine::capture(cudaStream_t s)
+{
+    for (int which = 0; which < 2; which++) {
+        cudaGraph_t g;
+        GTSC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+            if (which == 0) record_compress(s);
+            else record_decompress(s);
+        } catch (...) {
+            cudaGraph_t junk;
+            cudaStreamEndCapture(s, &junk);
+            if (junk) cudaGraphDestroy(junk);
+            throw;
+        }
+        GTSC_CUDA(cudaStreamEndCapture(s, &g));
+        cudaGraphExec_t ex;
+        GTSC_CUDA(cudaGraphInstantiate(&ex, g, 0));
+        cudaGraphDestroy(g);
+        (which == 0 ? graph_c : graph_d) = ex;
+    }
+}
+
+// ---------------------------------------------------------------------------------- public
+
+BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vector<Tree> &trees, cudaStream_t s)
+{
+    if (cols.empty() || cols.size() != trees.size()) fail(GTSC_ERR_ARG, "batch: columns and trees differ in number");
+    if (!s) fail(GTSC_ERR_ARG, "batch: needs a non-default stream (steps are captured as CUDA graphs)");
+    if (cols.size() >= (1u << 24)) fail(GTSC_ERR_ARG, "batch: at most 2^24 - 1 columns");
+    for (const auto &c : cols)
+        if (!aligned16(c.data)) fail(GTSC_ERR_ARG, "batch: column pointers must be 16-byte aligned");
+    std::unique_ptr<BatchEngine> e(new BatchEngine());
+    for (size_t c = 0; c < cols.size(); c++) {
+        const Tree &t = trees[c];
+        if (t.size() == 0 || t.dt[0] != cols[c].dtype) fail(GTSC_ERR_ARG, "batch: tree root type differs from the column");
+        const int in_sid = e->new_stream(0);
+        const int out_sid = e->new_stream(0);
+        e->col_in_sid.push_back(in_sid);
+        e->col_out_sid.push_back(out_sid);
+        e->col_bytes.push_back(cols[c].bytes);
+        e->col_root.push_back((int)e->nodes.size());
+        int k = 0;
+        e->build_node(t, k, (int)c, -1, in_sid, cols[c].bytes, 0);
+        if (k != t.size()) fail(GTSC_ERR_ARG, "batch: extra nodes in tree");
+        e->nodes[e->col_root.back()].dec_out_sid = out_sid;
+    }
+    e->plan_passes();
+    e->layout(s);
+    // column inputs
+    std::vector<unsigned long long> vals;
+    std::vector<int> sids;
+    for (size_t c = 0; c < cols.size(); c++) {
+        vals.push_back((unsigned long long)(uintptr_t)cols[c].data);
+        vals.push_back(cols[c].bytes);
+        sids.push_back(e->col_in_sid[c]);
+    }
+    for (size_t c = 0; c < cols.size(); c++) sids.push_back(e->col_out_sid[c]);
+    GTSC_CUDA(cudaMemcpyAsync(e->d_set_vals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, s));
+    GTSC_CUDA(cudaMemcpyAsync(e->d_set_sids, sids.data(), sids.size() * 4, cudaMemcpyHostToDevice, s));
+    GTSC_CUDA(cudaStreamSynchronize(s));
+    e->capture(s);
+    return e.release();
+}
+
+void batch_destroy(BatchEngine *e)
+{
+    if (!e) return;
+    if (e->graph_c) cudaGraphExecDestroy(e->graph_c);
+    if (e->graph_d) cudaGraphExecDestroy(e->graph_d);
+    delete e;
+}
+
+void batch_compress(BatchEngine *e, cudaStream_t s) { GTSC_CUDA(cudaGraphLaunch(e->graph_c, s)); }
+
+void batch_set_inputs(BatchEngine *e, const std::vector<const void *> &inputs, cudaStream_t s)
+{
+    const size_t nc = e->col_root.size();
+    if (inputs.size() != nc) fail(GTSC_ERR_ARG, "batch: one input per column");
+    for (const void *p : inputs)
+        if (!aligned16(p)) fail(GTSC_ERR_ARG, "batch: column pointers must be 16-byte aligned");
+    std::vector<unsigned long long> vals;
+    for (size_t c = 0; c < nc; c++) {
+        vals.push_back((unsigned long long)(uintptr_t)inputs[c]);
+        vals.push_back(e->col_bytes[c]);
+    }
+    GTSC_CUDA(cudaMemcpyAsync(e->d_set_vals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, s));
+}
+
+uint64_t batch_output_bytes(BatchEngine *e, cudaStream_t s)
+{
+    unsigned long long t = 0;
+    d2h(&t, e->d_total, 8, s);
+    return t;
+}
+
+const uint8_t *batch_output(BatchEngine *e) { return e->d_framed; }
+
+std::vector<uint64_t> batch_blob_sizes(BatchEngine *e, cudaStream_t s)
+{
+    const size_t nc = e->col_root.size();
+    std::vector<uint64_t> r(nc);
+    d2h(r.data(), e->d_framed + 8, 8 * nc, s);  // the directory of the framed output
+    return r;
+}
+
+void batch_decompress(BatchEngine *e, const uint8_t *framed, uint64_t framed_bytes, const std::vector<void *> &outputs,
+                      cudaStream_t s)
+{
+    const size_t nc = e->col_root.size();
+    if (outputs.size() != nc) fail(GTSC_ERR_ARG, "batch: one output per column");
+    for (const void *p : outputs)
+        if (!aligned16(p)) fail(GTSC_ERR_ARG, "batch: output pointers must be 16-byte aligned");
+    std::vector<unsigned long long> vals;
+    for (size_t c = 0; c < nc; c++) {
+        vals.push_back((unsigned long long)(uintptr_t)outputs[c]);
+        vals.push_back(0);
+    }
+    GTSC_CUDA(cudaMemcpyAsync(e->d_set_vals + 2 * nc, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, s));
+    unsigned long long fr[2] = {(unsigned long long)(uintptr_t)framed, framed_bytes};
+    GTSC_CUDA(cudaMemcpyAsync(e->d_frame_ptr, fr, 16, cudaMemcpyHostToDevice, s));
+    GTSC_CUDA(cudaGraphLaunch(e->graph_d, s));
+}
+
+gtsc_status batch_status(BatchEngine *e, cudaStream_t s)
+{
+    uint32_t w = 0;
+    d2h(&w, e->d_status, 4, s);
+    return w ? -(gtsc_status)w : GTSC_OK;
+}
+
+int batch_launches(BatchEngine *e, bool compress)
+{
+    return compress ? (int)e->launch_c.size() + 5 : (int)e->launch_d.size() + 3;
+}
+
+}  // namespace gtsc

@@ -1,0 +1,144 @@
+// batch.hpp -- the batched multi-column tree engine.
+//
+// Many columns, each with its own compression tree, are processed together: every tree node is
+// split into passes (min/max, histogram, split, pack, ...), passes of the same kind whose inputs
+// are ready are grouped into one stage, and a stage is ONE launch whose blocks pull (item, tile)
+// work across all columns.  Stream lengths live in device words, so no stage needs the host: a
+// whole compress (or decompress) step is a fixed sequence of launches, captured once in a CUDA
+// graph and replayed.
+#pragma once
+
+#include "common.cuh"
+#include "tree.hpp"
+
+namespace gtsc {
+
+// pass kinds (one batched kernel each)
+enum BOp : int {
+    B_MINMAX = 0,      // min/max accumulators (AFL, scale, patch)
+    B_DELTA_ENC,
+    B_SCALE_SUB,
+    B_AFL_PACK,
+    B_HIST,            // dict / const histogram
+    B_TOPK,            // one block per item
+    B_SPLIT,           // patch / const / dict split (mode in item.mode)
+    B_RLE_HEADS,
+    B_RLE_LENGTHS,
+    B_F2I_STATS,
+    B_F2I_ENC,
+    B_F2I_RAW,
+    B_GFC_COMPRESS,
+    B_GFC_SCAN,
+    B_GFC_COMPACT,
+    B_NONE_COPY,       // decode: none leaf copied to an aligned stream
+    // decode
+    B_AFL_UNPACK,
+    B_DELTA_DEC,
+    B_SCALE_ADD,
+    B_MERGE,
+    B_RLE_SCAN,
+    B_RLE_EXPAND,
+    B_F2I_DEC,
+    B_GFC_SIZES,
+    B_GFC_DEC,
+    B_NUM_OPS
+};
+
+// A stream: device bytes and their length.  The table lives in device memory; compress passes
+// write lengths, the decode parser writes the pointers of streams that sit inside a blob.
+struct StreamDesc {
+    uint8_t *ptr;
+    uint64_t len;   // bytes
+    uint64_t cap;   // bytes reserved (arena streams)
+    uint64_t pad;
+};
+
+// One unit of batched work: a pass of one tree node of one column.
+struct BItem {
+    uint64_t tile_base;          // first global tile of this item
+    uint32_t tiles;              // tiles reserved (worst case; tiles past the real length exit)
+    int16_t op, mode;            // pass kind; SplitMode / top-k size / merge mode
+    int16_t es, order;           // element size, Order of the node's data type
+    int32_t dt;
+    int32_t in[3];               // input stream ids (-1 = none)
+    int32_t out[3];              // output stream ids (compress: meta, out1, out2; decode: out[0])
+    uint8_t *scratch;            // the node's scratch: accumulators, look-back state, tables
+    uint64_t p[4];               // pass parameters (scratch offsets, capacities)
+};
+
+// A tree node as the framing / parse kernels see it.
+struct BNodeDev {
+    int32_t enc, dt;
+    int32_t meta;                // stream id of the node's metadata (-1 for none: 8 size bytes)
+    int32_t data;                // none leaves: stream id of the data (-1 otherwise)
+    uint64_t meta_dst, data_dst; // destinations in the framed buffer (set by the layout pass)
+};
+struct BColumnDev {
+    int32_t first, n_nodes;      // the column's nodes in the node table, pre-order
+};
+
+void launch_frame_sizes(const BColumnDev *cols, int ncols, const BNodeDev *nodes, const StreamDesc *S,
+                        unsigned long long *col_off, unsigned long long *total, uint8_t *framed, cudaStream_t s);
+void launch_frame_layout(const BColumnDev *cols, int ncols, BNodeDev *nodes, const StreamDesc *S,
+                         const unsigned long long *col_off, uint8_t *framed, cudaStream_t s);
+void launch_frame_copy(const BItem *items, int n_items, uint64_t total_tiles, const BNodeDev *nodes,
+                       const StreamDesc *S, uint8_t *framed, cudaStream_t s);
+void launch_parse_frames(const BColumnDev *cols, int ncols, const BNodeDev *nodes, StreamDesc *S,
+                         unsigned long long *col_off, const uint8_t *const *framed_p,
+                         const unsigned long long *framed_bytes_p, uint32_t *status, cudaStream_t s);
+void launch_zero_ranges(const unsigned long long *ranges, int n, cudaStream_t s);
+uint64_t batch_copy_piece();
+
+struct BatchColumn {
+    const void *data;  // device column
+    uint64_t bytes;
+    int dtype;
+};
+
+class BatchEngine;
+
+// Compile a batch: columns + their (Fix()ed) trees.  Owns the arena and the graphs.
+BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vector<Tree> &trees, cudaStream_t s);
+void batch_destroy(BatchEngine *e);
+// compress all columns into the framed output: uint64 column count, uint64 blob bytes per column,
+// then the blobs (CompressionTree::Compress of each column) back to back
+void batch_compress(BatchEngine *e, cudaStream_t s);
+// new device pointers for the columns (same sizes), used by the next compress
+void batch_set_inputs(BatchEngine *e, const std::vector<const void *> &inputs, cudaStream_t s);
+// total framed bytes (synchronises) and the device framed buffer
+uint64_t batch_output_bytes(BatchEngine *e, cudaStream_t s);
+const uint8_t *batch_output(BatchEngine *e);
+// per-column blob sizes (synchronises)
+std::vector<uint64_t> batch_blob_sizes(BatchEngine *e, cudaStream_t s);
+// decompress a framed buffer produced with the same trees (any step) into the columns' outputs
+void batch_decompress(BatchEngine *e, const uint8_t *framed, uint64_t framed_bytes,
+                      const std::vector<void *> &outputs, cudaStream_t s);
+// status word of the last step (0 = ok); synchronises
+gtsc_status batch_status(BatchEngine *e, cudaStream_t s);
+// number of kernel launches in one compress / decompress step
+int batch_launches(BatchEngine *e, bool compress);
+
+// stage launcher (batch_kernels.cu / batch_decode.cu): one launch of `total_tiles` blocks
+void launch_batch_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,
+                        uint32_t *d_counter, uint32_t *d_status, cudaStream_t s);
+
+// tile sizes (elements) of the batched passes
+constexpr uint32_t kBTile = 2048;       // element-wise, look-back and pack passes
+constexpr uint32_t kBMinMaxTile = 8192;
+constexpr uint32_t kBHistTile = 16384;
+constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
+constexpr uint32_t kBHistSmem = 2048;
+
+// scratch layout of a histogram item
+struct BHistHdr {
+    unsigned int used;      // slots taken in the global table
+    unsigned int special;   // occurrences of the all-ones value
+    unsigned int overflow;
+    unsigned int pad;
+};
+inline uint64_t bhist_bytes(uint64_t cap, uint64_t tiles)
+{
+    return 16 + 8 * cap + 4 * cap + 4 * cap + 32 * tiles + 64;
+}
+
+}  // namespace gtsc

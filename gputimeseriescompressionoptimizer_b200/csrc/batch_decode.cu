@@ -1,0 +1,809 @@
+// batch_decode.cu -- decode passes of the batched engine, plus the kernels that frame compressed
+// columns (assembly) and locate their nodes again (parse).
+//
+// Framed output: for every column, a uint64 blob length followed by the column's serialized tree
+// (the reference's per-column-chunk file framing, optimizer/compression_task.cpp:35-40, with
+// the blob of CompressionTree::Compress).
+#include "batch_dev.cuh"
+
+namespace gtsc {
+
+namespace {
+
+// ------------------------------------------------------------------------------- block copy
+// Copies n bytes from src to dst (any alignment) with the whole block: byte head up to a 4-byte
+// aligned destination, then 32-bit words assembled from the two source words that cover them.
+// Source words are read at most 3 bytes past its end, inside the same aligned word.
+__device__ void block_copy(uint8_t *dst, const uint8_t *src, uint64_t n)
+{
+    const uint64_t head = (4 - ((uintptr_t)dst & 3)) & 3;
+    const uint64_t h = head < n ? head : n;
+    if (threadIdx.x < h) dst[threadIdx.x] = src[threadIdx.x];
+    if (n <= h) return;
+    uint8_t *d = dst + h;
+    const uint8_t *sp = src + h;
+    const uint64_t words = (n - h) / 4;
+    const uint32_t sh = 8 * (uint32_t)((uintptr_t)sp & 3);
+    const uint32_t *sw = (const uint32_t *)((uintptr_t)sp & ~(uintptr_t)3);
+    uint32_t *dw = (uint32_t *)d;
+    if (sh == 0) {
+        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = sw[k];
+    } else {
+        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = __funnelshift_r(sw[k], sw[k + 1], sh);
+    }
+    const uint64_t tail = (n - h) - 4 * words;
+    if (threadIdx.x < tail) d[4 * words + threadIdx.x] = sp[4 * words + threadIdx.x];
+}
+
+constexpr uint64_t kCopyPiece = 1ull << 22;  // bytes of one copy tile
+
+// ------------------------------------------------------------------------------- none / copy
+// in[0] = source stream, out[0] = destination stream; p[0] = destination byte offset inside it
+__device__ void p_none_copy(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t off = (uint64_t)tile * kCopyPiece;
+    if (in.len > S[it.out[0]].cap) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+        return;
+    }
+    if (tile == 0 && threadIdx.x == 0) S[it.out[0]].len = in.len;
+    if (off >= in.len) return;
+    const uint64_t n = in.len - off < kCopyPiece ? in.len - off : kCopyPiece;
+    block_copy(S[it.out[0]].ptr + off, in.ptr + off, n);
+}
+
+// ------------------------------------------------------------------------------- AFL unpack
+template <int ES>
+__device__ void p_afl_unpack(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    const StreamDesc meta = S[it.in[0]], data = S[it.in[1]];
+    StreamDesc &out = S[it.out[0]];
+    if (data.len == 0) {
+        if (tile == 0 && threadIdx.x == 0) out.len = 0;
+        return;
+    }
+    if (meta.len < 2) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+        return;
+    }
+    const int b = (int8_t)meta.ptr[0], rest = (int8_t)meta.ptr[1];
+    const int64_t bits = (int64_t)data.len * 8 - rest;
+    if (b < 1 || b > 8 * ES || bits < 0) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+        return;
+    }
+    const uint64_t n = (uint64_t)bits / b;
+    if (n * ES > out.cap) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+        return;
+    }
+    if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
+    const uintptr_t mis = (uintptr_t)data.ptr & 3;
+    const StreamReader rd{(const uint32_t *)(data.ptr - mis), data.len + mis};
+    const uint64_t off_bits = 8 * mis;
+    const uint64_t mask = b >= 64 ? ~0ull : ((1ull << b) - 1);
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    if (base >= n) return;
+    uint64_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        v[j] = 0;
+        const uint64_t i = base + j;
+        if (i >= n) continue;
+        const uint64_t p = off_bits + i * (uint64_t)b;
+        const uint64_t w = p >> 5;
+        const uint32_t s = (uint32_t)(p & 31);
+        if (b <= 32) {
+            const uint32_t lo = rd.word(w);
+            const uint32_t hi = (s + b > 32) ? rd.word(w + 1) : 0u;
+            v[j] = __funnelshift_r(lo, hi, s) & mask;
+        } else {
+            const uint64_t q0 = (uint64_t)rd.word(w) | ((uint64_t)rd.word(w + 1) << 32);
+            uint64_t x = q0 >> s;
+            if (s + b > 64) x |= (uint64_t)rd.word(w + 2) << (64 - s);
+            v[j] = x & mask;
+        }
+    }
+    uint8_t *o = out.ptr;
+    if (base + 8 <= n && (8 * ES) % 16 == 0) {
+        constexpr int PER = 16 / ES;
+#pragma unroll
+        for (int c = 0; c < 8 / PER; c++)
+            reinterpret_cast<uint4 *>(o + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
+    } else {
+        for (int j = 0; j < 8; j++)
+            if (base + j < n) st_elem<ES>(o, base + j, v[j]);
+    }
+}
+
+// ------------------------------------------------------------------------------- delta decode
+template <int ES>
+__device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    __shared__ unsigned long long ws[32];
+    __shared__ unsigned long long s_prefix;
+    const StreamDesc meta = S[it.in[0]], d = S[it.in[1]];
+    StreamDesc &out = S[it.out[0]];
+    const uint64_t n = meta.len ? d.len / ES + 1 : 0;
+    if (n * ES > out.cap) {  // item-uniform: no tile of this item enters the look-back
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+        return;
+    }
+    if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
+    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
+    const uint64_t m = n ? n - 1 : 0;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    uint64_t v[8];
+    unsigned long long local = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        v[j] = base + j < m ? ld_unaligned<ES>(d.ptr + (base + j) * ES) : 0;
+        local += v[j];
+    }
+    unsigned long long total;
+    const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
+    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    __syncthreads();
+    if (base >= n) return;
+    unsigned long long acc = ld_unaligned<ES>(meta.ptr) + s_prefix + excl;
+    uint64_t o[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        o[j] = wrap_es(acc, ES);
+        acc += v[j];
+    }
+    if (base + 8 <= n && (8 * ES) % 16 == 0) {
+        constexpr int PER = 16 / ES;
+#pragma unroll
+        for (int c = 0; c < 8 / PER; c++)
+            reinterpret_cast<uint4 *>(out.ptr + (base + c * PER) * ES)[0] = make_chunk<ES>(o + c * PER);
+    } else {
+        for (int j = 0; j < 8; j++)
+            if (base + j < n) st_elem<ES>(out.ptr, base + j, o[j]);
+    }
+}
+
+// ------------------------------------------------------------------------------- scale add
+template <int ES>
+__device__ void p_scale_add(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    const StreamDesc meta = S[it.in[0]], d = S[it.in[1]];
+    StreamDesc &out = S[it.out[0]];
+    const uint64_t n = d.len / ES;
+    if (n * ES > out.cap || (n && meta.len < (uint64_t)ES)) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+        return;
+    }
+    if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    if (base >= n) return;
+    const uint64_t mn = ld_unaligned<ES>(meta.ptr);
+    uint64_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = base + j < n ? wrap_es(ld_unaligned<ES>(d.ptr + (base + j) * ES) + mn, ES) : 0;
+    if (base + 8 <= n && (8 * ES) % 16 == 0) {
+        constexpr int PER = 16 / ES;
+#pragma unroll
+        for (int c = 0; c < 8 / PER; c++)
+            reinterpret_cast<uint4 *>(out.ptr + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
+    } else {
+        for (int j = 0; j < 8; j++)
+            if (base + j < n) st_elem<ES>(out.ptr, base + j, v[j]);
+    }
+}
+
+// ------------------------------------------------------------------------------- merge
+template <int ES>
+__device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    __shared__ unsigned long long ws[32];
+    __shared__ unsigned long long s_prefix;
+    const int mode = it.mode;
+    const StreamDesc meta = S[it.in[0]], in1 = S[it.in[1]];
+    const StreamDesc in2 = mode == SPLIT_NOT_CONST ? StreamDesc{nullptr, 0, 0, 0} : S[it.in[2]];
+    StreamDesc &out = S[it.out[0]];
+    // empty-input rules of the three Decode()s
+    const bool empty = mode == SPLIT_NOT_CONST ? meta.len == 0 : (in1.len == 0 && in2.len == 0);
+    const uint8_t *stencil = mode == SPLIT_NOT_CONST ? meta.ptr + ES : meta.ptr;
+    const uint64_t sbytes = mode == SPLIT_NOT_CONST ? (meta.len > (uint64_t)ES ? meta.len - ES : 0) : meta.len;
+    uint64_t n = 0;
+    if (!empty) {
+        if (sbytes < 1) {
+            if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+            return;
+        }
+        const int rest = (int8_t)stencil[0];
+        int64_t nn = (int64_t)(sbytes - 1) * 8;
+        if (rest) nn -= 8 - rest;
+        if (nn < 0 || rest < 0 || rest > 7) {
+            if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+            return;
+        }
+        n = (uint64_t)nn;
+    }
+    if (n * ES > out.cap) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+        return;
+    }
+    if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
+    // dictionary stream: 16-byte header, 4 values, codes
+    uint64_t top[4] = {0, 0, 0, 0}, yes_cap = 0, no_cap = in2.len / ES;
+    const uint8_t *codes = nullptr;
+    if (mode == SPLIT_DICT) {
+        if (in1.len >= 16 + 4ull * ES) {
+            const uint64_t m = ld_unaligned<8>(in1.ptr + 8);
+            for (int k = 0; k < 4; k++) top[k] = ld_unaligned<ES>(in1.ptr + 16 + k * ES);
+            codes = in1.ptr + 16 + 4 * ES;
+            yes_cap = (in1.len - 16 - 4ull * ES) / 4 * 16;
+            if (m < yes_cap) yes_cap = m;
+        }
+    } else if (mode == SPLIT_NOT_CONST) {
+        if (meta.len >= (uint64_t)ES) top[0] = ld_unaligned<ES>(meta.ptr);
+        yes_cap = in1.len / ES;
+    } else {
+        yes_cap = in1.len / ES;
+    }
+    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const uint32_t valid_mask = base >= n ? 0u : (n - base >= 8 ? 0xffu : ((1u << (n - base)) - 1));
+    const uint32_t bits = base < n ? ((uint32_t)stencil[1 + base / 8] & valid_mask) : 0u;
+    unsigned long long total;
+    const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(bits), ws, total);
+    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    __syncthreads();
+    if (base >= n) return;
+    uint64_t yes_pos = s_prefix + excl, no_pos = base - yes_pos;
+    uint64_t v[8];
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        v[j] = 0;
+        if (!((valid_mask >> j) & 1u)) continue;
+        if ((bits >> j) & 1u) {
+            if (yes_pos >= yes_cap) bad = true;
+            else if (mode == SPLIT_DICT) {
+                const uint32_t w = (uint32_t)ld_unaligned<4>(codes + 4 * (yes_pos >> 4));
+                v[j] = top[(w >> (2 * (yes_pos & 15))) & 3u];
+            } else {
+                v[j] = ld_unaligned<ES>(in1.ptr + yes_pos * ES);
+            }
+            ++yes_pos;
+        } else {
+            if (mode == SPLIT_NOT_CONST) v[j] = top[0];
+            else if (no_pos >= no_cap) bad = true;
+            else v[j] = ld_unaligned<ES>(in2.ptr + no_pos * ES);
+            ++no_pos;
+        }
+    }
+    if (bad) set_status(status, GTSC_ERR_FORMAT);
+    if (base + 8 <= n && (8 * ES) % 16 == 0) {
+        constexpr int PER = 16 / ES;
+#pragma unroll
+        for (int c = 0; c < 8 / PER; c++)
+            reinterpret_cast<uint4 *>(out.ptr + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
+    } else {
+        for (int j = 0; j < 8; j++)
+            if (base + j < n) st_elem<ES>(out.ptr, base + j, v[j]);
+    }
+}
+
+// ------------------------------------------------------------------------------- RLE decode
+// node scratch: p[0] look-back, p[1] run ends (u64)
+__device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    __shared__ unsigned long long ws[32];
+    __shared__ unsigned long long s_prefix;
+    const StreamDesc meta = S[it.in[0]], lengths = S[it.in[1]], values = S[it.in[2]];
+    int64_t runs = 0;
+    if (lengths.len) {
+        runs = meta.len >= 4 ? (int32_t)ld_unaligned<4>(meta.ptr) : -1;
+        if (runs < 0 || (uint64_t)runs * 4 > lengths.len || (uint64_t)runs * it.es > values.len) {
+            if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+            runs = 0;
+        }
+    }
+    unsigned long long *ends = (unsigned long long *)(it.scratch + it.p[1]);
+    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    long long v[8];
+    unsigned long long local = 0;
+    bool neg = false;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        v[j] = base + j < (uint64_t)runs ? (long long)(int32_t)ld_unaligned<4>(lengths.ptr + 4 * (base + j)) : 0;
+        neg |= v[j] < 0;
+        local += (unsigned long long)v[j];
+    }
+    if (neg) set_status(status, GTSC_ERR_FORMAT);
+    unsigned long long total;
+    const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
+    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    __syncthreads();
+    unsigned long long acc = s_prefix + excl;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        acc += (unsigned long long)v[j];
+        if (base + j < (uint64_t)runs) ends[base + j] = acc;
+    }
+    // p[2] holds the run count for the expand pass
+    if (tile == 0 && threadIdx.x == 0) *(unsigned long long *)(it.scratch + it.p[2]) = (unsigned long long)runs;
+}
+
+template <int ES>
+__device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    __shared__ uint64_t s_lo, s_hi;
+    const StreamDesc values = S[it.in[2]];
+    StreamDesc &out = S[it.out[0]];
+    const uint64_t runs = *(const unsigned long long *)(it.scratch + it.p[2]);
+    const unsigned long long *ends = (const unsigned long long *)(it.scratch + it.p[1]);
+    const uint64_t n = runs ? ends[runs - 1] : 0;
+    if (n * ES > out.cap) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+        return;
+    }
+    if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
+    const uint64_t t0 = (uint64_t)tile * kBTile;
+    if (t0 >= n) return;
+    auto ub = [&](uint64_t lo, uint64_t hi, uint64_t pos) {
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (ends[mid] > pos) hi = mid;
+            else lo = mid + 1;
+        }
+        return lo;
+    };
+    if (threadIdx.x == 0) {
+        s_lo = ub(0, runs, t0);
+        const uint64_t last = t0 + kBTile - 1 < n ? t0 + kBTile - 1 : n - 1;
+        const uint64_t hi = ub(s_lo, runs, last);
+        s_hi = hi < runs ? hi + 1 : runs;
+    }
+    __syncthreads();
+    const uint64_t base = t0 + (uint64_t)threadIdx.x * 8;
+    if (base >= n) return;
+    uint64_t r = ub(s_lo, s_hi, base);
+    uint64_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const uint64_t i = base + j;
+        while (r < runs && ends[r] <= i) ++r;
+        v[j] = (i < n && r < runs) ? ld_unaligned<ES>(values.ptr + r * ES) : 0;
+    }
+    if (base + 8 <= n && (8 * ES) % 16 == 0) {
+        constexpr int PER = 16 / ES;
+#pragma unroll
+        for (int c = 0; c < 8 / PER; c++)
+            reinterpret_cast<uint4 *>(out.ptr + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
+    } else {
+        for (int j = 0; j < 8; j++)
+            if (base + j < n) st_elem<ES>(out.ptr, base + j, v[j]);
+    }
+    (void)status;
+}
+
+// ------------------------------------------------------------------------------- floatToInt
+template <int ES>
+__device__ void p_f2i_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    __shared__ double p10[10];
+    if (threadIdx.x < 10) {
+        double v = 1.0;
+        for (unsigned i = 0; i < threadIdx.x; i++) v *= 10.0;
+        p10[threadIdx.x] = v;
+    }
+    __syncthreads();
+    const StreamDesc meta = S[it.in[0]], d = S[it.in[1]];
+    StreamDesc &out = S[it.out[0]];
+    if (d.len == 0) {
+        if (tile == 0 && threadIdx.x == 0) out.len = 0;
+        return;
+    }
+    const int p = meta.len >= 4 ? (int32_t)ld_unaligned<4>(meta.ptr) : -1;
+    if (p < 0) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+        return;
+    }
+    const uint64_t n = p < 10 ? d.len / 4 : d.len / ES;
+    if (n * ES > out.cap) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+        return;
+    }
+    if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const Order o = (Order)it.order;
+    for (int j = 0; j < 8 && base + j < n; j++) {
+        uint64_t v;
+        if (p < 10) {
+            const int k = (int32_t)ld_unaligned<4>(d.ptr + 4 * (base + j));
+            if (o == ORD_F32) v = __float_as_uint(__double2float_rn(__ddiv_rn((double)__int2float_rn(k), p10[p])));
+            else if (o == ORD_F64) v = (uint64_t)__double_as_longlong(__ddiv_rn((double)k, p10[p]));
+            else if (ES == 8) v = (uint64_t)__double2ll_rz(__ddiv_rn((double)k, p10[p]));
+            else v = (uint64_t)(long long)__double2int_rz(__ddiv_rn((double)sext((uint64_t)(long long)k, ES), p10[p]));
+        } else {
+            v = ld_unaligned<ES>(d.ptr + (base + j) * ES);
+        }
+        st_elem<ES>(out.ptr, base + j, v);
+    }
+}
+
+// ------------------------------------------------------------------------------- GFC decode
+// node scratch: p[0] look-back, p[1] sizes (int32), p[2] inclusive ends (u64)
+__device__ bool gfc_meta(const StreamDesc &m, bool dbl, DGfc &g)
+{
+    if (m.len < 12) return false;
+    const int blocks = (int32_t)ld_unaligned<4>(m.ptr), wpb = (int32_t)ld_unaligned<4>(m.ptr + 4);
+    const int nn = (int32_t)ld_unaligned<4>(m.ptr + 8);
+    if (blocks <= 0 || wpb <= 0 || nn < 0 || (int64_t)blocks * wpb > (1ll << 26)) return false;
+    g = d_gfc_geom(dbl, (uint64_t)nn, blocks, wpb);
+    return true;
+}
+
+__device__ void p_gfc_sizes(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    const bool dbl = it.es == 8;
+    const StreamDesc meta = S[it.in[0]], ends = S[it.in[1]], payload = S[it.in[2]];
+    if (payload.len == 0) return;
+    DGfc g;
+    if (!gfc_meta(meta, dbl, g) || ends.len < 4ull * g.warps || (uint64_t)g.warps > it.p[3]) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+        return;
+    }
+    int32_t *sizes = (int32_t *)(it.scratch + it.p[1]);
+    const uint64_t w0 = (uint64_t)tile * kBTile;
+    for (uint64_t w = w0 + threadIdx.x; w < (uint64_t)g.warps && w < w0 + kBTile; w += kBThreads) {
+        const int64_t e = (int32_t)ld_unaligned<4>(ends.ptr + 4 * w);
+        const int64_t sz = e - (int64_t)d_gfc_start(g, (int64_t)w);
+        const uint64_t subs = (d_gfc_cut(g, (int64_t)w) - d_gfc_begin(g, (int64_t)w)) / 32;
+        if (sz < 0 || sz > (int64_t)(subs * (16 + 32 * (dbl ? 8 : 4)))) {
+            set_status(status, GTSC_ERR_FORMAT);
+            sizes[w] = 0;
+        } else {
+            sizes[w] = (int32_t)sz;
+        }
+    }
+}
+
+template <bool DBL>
+__device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    const StreamDesc meta = S[it.in[0]], payload = S[it.in[2]];
+    StreamDesc &out = S[it.out[0]];
+    if (payload.len == 0) {
+        if (tile == 0 && threadIdx.x == 0) out.len = 0;
+        return;
+    }
+    DGfc g;
+    if (!gfc_meta(meta, DBL, g) || (uint64_t)g.warps > it.p[3]) return;  // reported by p_gfc_sizes
+    constexpr int ES = DBL ? 8 : 4;
+    if (g.n * ES > out.cap) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+        return;
+    }
+    if (tile == 0 && threadIdx.x == 0) out.len = g.n * ES;
+    const int lane = threadIdx.x & 31;
+    const int64_t w = (int64_t)tile * kBGfcChunks + (threadIdx.x >> 5);
+    if (w >= g.warps) return;
+    const int32_t *sizes = (const int32_t *)(it.scratch + it.p[1]);
+    const unsigned long long *incl = (const unsigned long long *)(it.scratch + it.p[2]);
+    const uint64_t size = (uint64_t)(uint32_t)sizes[w], end = incl[w];
+    if (end > payload.len || end < size) {
+        if (lane == 0) set_status(status, GTSC_ERR_FORMAT);
+        return;
+    }
+    const uint64_t cb = d_gfc_begin(g, w), ce = d_gfc_cut(g, w);
+    uint64_t pos = end - size, last = 0;
+    const uint8_t *pl = payload.ptr;
+    for (uint64_t s = cb; s < ce; s += 32) {
+        if (pos + 16 > end) {
+            if (lane == 0) set_status(status, GTSC_ERR_FORMAT);
+            return;
+        }
+        const uint32_t nib = ((uint32_t)pl[pos + (lane >> 1)] >> (4 * (lane & 1))) & 15u;
+        const uint32_t code = nib & 7u;
+        uint32_t mb = DBL ? (code >= 2 ? code + 1 : code) : code;
+        if (!DBL && mb > 4) {
+            set_status(status, GTSC_ERR_FORMAT);
+            mb = 4;
+        }
+        uint32_t inc = mb;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+        if (pos + 16 + total > end) {
+            if (lane == 0) set_status(status, GTSC_ERR_FORMAT);
+            return;
+        }
+        const uint8_t *src = pl + pos + 16 + (inc - mb);
+        uint64_t diff = 0;
+        for (int b = (int)mb - 1; b >= 0; b--) diff = (diff << 8) | src[b];
+        if (nib & 8u) diff = 0ull - diff;
+        uint64_t x = last + diff;
+        if (!DBL) x &= 0xffffffffull;
+        if (s + lane < g.n) st_elem<ES>(out.ptr, s + lane, x);
+        pos += 16 + total;
+        if (s == cb) last = __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0 && pos != end) set_status(status, GTSC_ERR_FORMAT);
+}
+
+// ------------------------------------------------------------------------------- dispatch
+// A framed buffer that does not parse leaves blob-resident stream pointers unset, so status[1]
+// (set only by the parse kernel, which runs before every decode stage) turns all stages off.
+__device__ __forceinline__ void parse_fail(uint32_t *status)
+{
+    set_status(status, GTSC_ERR_FORMAT);
+    atomicExch(status + 1, 1u);
+}
+
+template <int OP>
+__global__ void __launch_bounds__(kBThreads)
+k_bdec(const BItem *items, int n_items, StreamDesc *S, uint32_t *counter, uint32_t *status)
+{
+    constexpr bool DYN = OP == B_DELTA_DEC || OP == B_MERGE || OP == B_RLE_SCAN;
+    if (*(volatile uint32_t *)(status + 1)) return;
+    BItem it;
+    uint32_t tile;
+    locate<DYN>(items, n_items, counter, it, tile);
+    if (tile >= it.tiles) return;
+#define GTSC_ES_SWITCH(CALL)                       \
+    switch (it.es) {                               \
+    case 1: { constexpr int E = 1; CALL; } break;  \
+    case 2: { constexpr int E = 2; CALL; } break;  \
+    case 4: { constexpr int E = 4; CALL; } break;  \
+    default: { constexpr int E = 8; CALL; } break; \
+    }
+    if constexpr (OP == B_NONE_COPY) p_none_copy(it, tile, S, status);
+    else if constexpr (OP == B_AFL_UNPACK) { GTSC_ES_SWITCH(p_afl_unpack<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_DELTA_DEC) { GTSC_ES_SWITCH(p_delta_dec<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_SCALE_ADD) { GTSC_ES_SWITCH(p_scale_add<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_MERGE) { GTSC_ES_SWITCH(p_merge<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_RLE_SCAN) p_rle_scan(it, tile, S, status);
+    else if constexpr (OP == B_RLE_EXPAND) { GTSC_ES_SWITCH(p_rle_expand<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_F2I_DEC) { GTSC_ES_SWITCH(p_f2i_dec<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_GFC_SIZES) p_gfc_sizes(it, tile, S, status);
+    else if constexpr (OP == B_GFC_DEC) {
+        if (it.es == 8) p_gfc_dec<true>(it, tile, S, status);
+        else p_gfc_dec<false>(it, tile, S, status);
+    }
+#undef GTSC_ES_SWITCH
+}
+
+// ------------------------------------------------------------------------------- framing
+// Framed buffer: uint64 column count C, uint64 blob bytes of every column (the directory), then the
+// C blobs back to back.  The directory lets decode find every column without walking the blobs.
+// Per column: pre-order nodes; node k of column c is cols[c].first + k in the node table.
+__device__ __forceinline__ uint64_t frame_header_bytes(int ncols) { return 8 + 8 * (uint64_t)ncols; }
+
+// col_off[0..ncols] = blob offsets, col_off[ncols] = total framed bytes; writes the directory
+__global__ void k_frame_sizes(const BColumnDev *cols, int ncols, const BNodeDev *nodes, const StreamDesc *S,
+                              unsigned long long *col_off, unsigned long long *total, uint8_t *framed)
+{
+    // one block: thread t sums its columns' blob sizes, then an exclusive scan gives offsets
+    __shared__ unsigned long long ws[32];
+    const int per = (ncols + kBThreads - 1) / kBThreads;
+    unsigned long long mine = 0;
+    for (int c = threadIdx.x * per; c < ncols && c < (int)(threadIdx.x + 1) * per; c++) {
+        unsigned long long sz = 0;
+        for (int k = 0; k < cols[c].n_nodes; k++) {
+            const BNodeDev &nd = nodes[cols[c].first + k];
+            sz += 8 + (nd.meta >= 0 ? S[nd.meta].len : 8);
+            if (nd.data >= 0) sz += S[nd.data].len;
+        }
+        col_off[c] = sz;  // temporarily the blob size
+        mine += sz;
+    }
+    unsigned long long tot;
+    unsigned long long excl = block_exclusive_scan<kBThreads>(mine, ws, tot) + frame_header_bytes(ncols);
+    unsigned long long *dir = (unsigned long long *)framed;  // the framed buffer is 256-byte aligned
+    for (int c = threadIdx.x * per; c < ncols && c < (int)(threadIdx.x + 1) * per; c++) {
+        const unsigned long long sz = col_off[c];
+        dir[1 + c] = sz;
+        col_off[c] = excl;
+        excl += sz;
+    }
+    if (threadIdx.x == 0) {
+        dir[0] = (unsigned long long)ncols;
+        col_off[ncols] = tot + frame_header_bytes(ncols);
+        *total = tot + frame_header_bytes(ncols);
+    }
+}
+
+// one thread per column: node headers and the destinations of every segment
+__global__ void k_frame_layout(const BColumnDev *cols, int ncols, BNodeDev *nodes, const StreamDesc *S,
+                               const unsigned long long *col_off, uint8_t *framed)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncols) return;
+    unsigned long long pos = col_off[c];
+    for (int k = 0; k < cols[c].n_nodes; k++) {
+        BNodeDev &nd = nodes[cols[c].first + k];
+        const uint64_t ml = nd.meta >= 0 ? S[nd.meta].len : 8;
+        const uint8_t h[8] = {(uint8_t)nd.enc, (uint8_t)(nd.enc >> 8), (uint8_t)nd.dt, (uint8_t)(nd.dt >> 8),
+                              (uint8_t)ml, (uint8_t)(ml >> 8), (uint8_t)(ml >> 16), (uint8_t)(ml >> 24)};
+        for (int b = 0; b < 8; b++) framed[pos + b] = h[b];
+        nd.meta_dst = pos + 8;
+        if (nd.meta < 0) {  // NoneEncoding metadata: size_t byte count of the data
+            const uint64_t ds = S[nd.data].len;
+            for (int b = 0; b < 8; b++) framed[pos + 8 + b] = (uint8_t)(ds >> (8 * b));
+        }
+        pos += 8 + ml;
+        if (nd.data >= 0) {
+            nd.data_dst = pos;
+            pos += S[nd.data].len;
+        }
+    }
+}
+
+// copy items: p[0] = node table index, p[1] = 0 copy the node's metadata, 1 its data
+__global__ void __launch_bounds__(kBThreads)
+k_frame_copy(const BItem *items, int n_items, const BNodeDev *nodes, const StreamDesc *S, uint8_t *framed)
+{
+    BItem it;
+    uint32_t tile;
+    locate<false>(items, n_items, nullptr, it, tile);
+    const BNodeDev &nd = nodes[it.p[0]];
+    const StreamDesc src = S[it.p[1] ? nd.data : nd.meta];
+    const uint64_t dst = it.p[1] ? nd.data_dst : nd.meta_dst;
+    const uint64_t off = (uint64_t)tile * kCopyPiece;
+    if (off >= src.len) return;
+    const uint64_t n = src.len - off < kCopyPiece ? src.len - off : kCopyPiece;
+    block_copy(framed + dst + off, src.ptr + off, n);
+}
+
+// decode, one block: reads the directory of the framed buffer into col_off[0..ncols]
+__global__ void k_parse_directory(int ncols, unsigned long long *col_off, const uint8_t *const *framed_p,
+                                  const unsigned long long *framed_bytes_p, uint32_t *status)
+{
+    __shared__ unsigned long long ws[32];
+    __shared__ int s_bad;
+    const uint8_t *framed = *framed_p;
+    const uint64_t fb = *framed_bytes_p;
+    const uint64_t hdr = frame_header_bytes(ncols);
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    // every length is at most fb < 2^40, so the sums below cannot wrap (ncols < 2^24)
+    if (fb < hdr || fb >= (1ull << 40) || ld_unaligned<8>(framed) != (uint64_t)ncols) {
+        if (threadIdx.x == 0) parse_fail(status);
+        return;
+    }
+    const int per = (ncols + kBThreads - 1) / kBThreads;
+    unsigned long long mine = 0;
+    for (int c = threadIdx.x * per; c < ncols && c < (int)(threadIdx.x + 1) * per; c++) {
+        const uint64_t len = ld_unaligned<8>(framed + 8 + 8 * (uint64_t)c);
+        if (len > fb) s_bad = 1;
+        mine += len > fb ? fb : len;
+    }
+    unsigned long long tot;
+    unsigned long long excl = block_exclusive_scan<kBThreads>(mine, ws, tot) + hdr;
+    for (int c = threadIdx.x * per; c < ncols && c < (int)(threadIdx.x + 1) * per; c++) {
+        const uint64_t len = ld_unaligned<8>(framed + 8 + 8 * (uint64_t)c);
+        col_off[c] = excl;
+        excl += len > fb ? fb : len;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        col_off[ncols] = tot + hdr;
+        if (s_bad || tot + hdr > fb) parse_fail(status);
+    }
+}
+
+// decode, one thread per column: walks the column's blob and points its meta / data streams into it
+__global__ void k_parse_frames(const BColumnDev *cols, int ncols, const BNodeDev *nodes, StreamDesc *S,
+                               const unsigned long long *col_off, const uint8_t *const *framed_p, uint32_t *status)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncols) return;
+    if (*(volatile uint32_t *)(status + 1)) return;  // the directory did not parse
+    const uint8_t *framed = *framed_p;
+    uint64_t pos = col_off[c];
+    const uint64_t end = col_off[c + 1];
+    for (int k = 0; k < cols[c].n_nodes; k++) {
+        const BNodeDev &nd = nodes[cols[c].first + k];
+        if (pos + 8 > end) { parse_fail(status); return; }
+        const int enc = (int16_t)ld_unaligned<2>(framed + pos), dt = (int16_t)ld_unaligned<2>(framed + pos + 2);
+        const int64_t ml = (int32_t)ld_unaligned<4>(framed + pos + 4);
+        if (enc != nd.enc || dt != nd.dt || ml < 0 || pos + 8 + (uint64_t)ml > end) {
+            parse_fail(status);
+            return;
+        }
+        if (nd.meta >= 0) {
+            S[nd.meta].ptr = (uint8_t *)framed + pos + 8;
+            S[nd.meta].len = (uint64_t)ml;
+        }
+        pos += 8 + (uint64_t)ml;
+        if (nd.data >= 0) {
+            if (ml < 8) { parse_fail(status); return; }
+            const uint64_t ds = ld_unaligned<8>(framed + pos - ml);
+            if (ds > end - pos) { parse_fail(status); return; }
+            S[nd.data].ptr = (uint8_t *)framed + pos;
+            S[nd.data].len = ds;
+            pos += ds;
+        }
+    }
+    if (pos != end) parse_fail(status);
+}
+
+__global__ void k_zero_ranges(const unsigned long long *ranges, int n)
+{
+    // ranges: (pointer, bytes) pairs; bytes are multiples of 4 and pointers 4-byte aligned
+    for (int r = blockIdx.x; r < n; r += gridDim.x) {
+        uint32_t *p = (uint32_t *)ranges[2 * r];
+        const uint64_t words = ranges[2 * r + 1] / 4;
+        for (uint64_t k = threadIdx.x; k < words; k += blockDim.x) p[k] = 0u;
+    }
+}
+
+}  // namespace
+
+void launch_batch_decode_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,
+                               uint32_t *d_counter, uint32_t *d_status, cudaStream_t s)
+{
+    if (n_items == 0 || total_tiles == 0) return;
+    if (total_tiles > 0x7fffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles in one stage");
+    const unsigned g = (unsigned)total_tiles;
+    switch (op) {
+#define GTSC_STAGE(OPC) \
+    case OPC: k_bdec<OPC><<<g, kBThreads, 0, s>>>(d_items, n_items, d_streams, d_counter, d_status); break;
+        GTSC_STAGE(B_NONE_COPY)
+        GTSC_STAGE(B_AFL_UNPACK)
+        GTSC_STAGE(B_DELTA_DEC)
+        GTSC_STAGE(B_SCALE_ADD)
+        GTSC_STAGE(B_MERGE)
+        GTSC_STAGE(B_RLE_SCAN)
+        GTSC_STAGE(B_RLE_EXPAND)
+        GTSC_STAGE(B_F2I_DEC)
+        GTSC_STAGE(B_GFC_SIZES)
+        GTSC_STAGE(B_GFC_DEC)
+#undef GTSC_STAGE
+    default: fail(GTSC_ERR_ARG, "batch: unknown pass");
+    }
+    GTSC_CUDA(cudaGetLastError());
+}
+
+uint64_t batch_copy_piece() { return kCopyPiece; }
+
+void launch_frame_sizes(const BColumnDev *cols, int ncols, const BNodeDev *nodes, const StreamDesc *S,
+                        unsigned long long *col_off, unsigned long long *total, uint8_t *framed, cudaStream_t s)
+{
+    k_frame_sizes<<<1, kBThreads, 0, s>>>(cols, ncols, nodes, S, col_off, total, framed);
+    GTSC_CUDA(cudaGetLastError());
+}
+
+void launch_frame_layout(const BColumnDev *cols, int ncols, BNodeDev *nodes, const StreamDesc *S,
+                         const unsigned long long *col_off, uint8_t *framed, cudaStream_t s)
+{
+    k_frame_layout<<<(ncols + 127) / 128, 128, 0, s>>>(cols, ncols, nodes, S, col_off, framed);
+    GTSC_CUDA(cudaGetLastError());
+}
+
+void launch_frame_copy(const BItem *items, int n_items, uint64_t total_tiles, const BNodeDev *nodes,
+                       const StreamDesc *S, uint8_t *framed, cudaStream_t s)
+{
+    if (!n_items || !total_tiles) return;
+    k_frame_copy<<<(unsigned)total_tiles, kBThreads, 0, s>>>(items, n_items, nodes, S, framed);
+    GTSC_CUDA(cudaGetLastError());
+}
+
+void launch_parse_frames(const BColumnDev *cols, int ncols, const BNodeDev *nodes, StreamDesc *S,
+                         unsigned long long *col_off, const uint8_t *const *framed_p,
+                         const unsigned long long *framed_bytes_p, uint32_t *status, cudaStream_t s)
+{
+    k_parse_directory<<<1, kBThreads, 0, s>>>(ncols, col_off, framed_p, framed_bytes_p, status);
+    GTSC_CUDA(cudaGetLastError());
+    k_parse_frames<<<(ncols + 127) / 128, 128, 0, s>>>(cols, ncols, nodes, S, col_off, framed_p, status);
+    GTSC_CUDA(cudaGetLastError());
+}
+
+void launch_zero_ranges(const unsigned long long *ranges, int n, cudaStream_t s)
+{
+    if (!n) return;
+    k_zero_ranges<<<n < 1024 ? n : 1024, 256, 0, s>>>(ranges, n);
+    GTSC_CUDA(cudaGetLastError());
+}
+
+}  // namespace gtsc

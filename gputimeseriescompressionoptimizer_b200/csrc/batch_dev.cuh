@@ -1,0 +1,180 @@
+// batch_dev.cuh -- device helpers shared by the batched pass kernels.
+#pragma once
+
+#include "batch.hpp"
+#include "kernels.hpp"
+#include "scan.cuh"
+#include "vec.cuh"
+
+namespace gtsc {
+
+constexpr int kBThreads = 256;
+
+__device__ __forceinline__ void set_status(uint32_t *status, gtsc_status code)
+{
+    atomicCAS(status, 0u, (uint32_t)(-code));
+}
+
+__device__ __forceinline__ bool bsame(uint64_t a, uint64_t b, Order o) { return a == b && !is_nan_bits(a, o); }
+
+__device__ __forceinline__ uint64_t wrap_es(uint64_t v, int es) { return es == 8 ? v : (v & ((1ull << (8 * es)) - 1)); }
+
+// block-wide min/max of order keys (all threads call; result valid in thread 0)
+__device__ __forceinline__ void block_minmax(uint64_t &kmin, uint64_t &kmax)
+{
+    __shared__ uint64_t smin[kBThreads / 32], smax[kBThreads / 32];
+    for (int off = 16; off > 0; off >>= 1) {
+        const uint64_t a = __shfl_xor_sync(0xffffffffu, kmin, off);
+        const uint64_t b = __shfl_xor_sync(0xffffffffu, kmax, off);
+        kmin = a < kmin ? a : kmin;
+        kmax = b > kmax ? b : kmax;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { smin[warp] = kmin; smax[warp] = kmax; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int w = 1; w < kBThreads / 32; w++) {
+            kmin = smin[w] < kmin ? smin[w] : kmin;
+            kmax = smax[w] > kmax ? smax[w] : kmax;
+        }
+    __syncthreads();
+}
+
+// raw bits of min / max from an accumulator; false when nothing (non-NaN) was seen
+__device__ __forceinline__ bool acc_minmax(const MinMaxAcc *acc, int es, Order o, uint64_t &mn, uint64_t &mx)
+{
+    const unsigned long long a = acc->nkmin, b = acc->kmax;
+    if (a == 0 && b == 0) return false;
+    mn = order_unkey(~(uint64_t)a, es, o);
+    mx = order_unkey(b, es, o);
+    return true;
+}
+
+// ScaleEncoding's min with the overflow rule of scale_encoding.cu:49-50 (x86 wrap for int/long)
+__device__ __forceinline__ uint64_t scale_min(uint64_t mnb, uint64_t mxb, int es)
+{
+    int64_t mn = sext(mnb, es), mx = sext(mxb, es);
+    if (mn < 0) {
+        if (es <= 2) {
+            const int64_t tmax = es == 1 ? 127 : 32767;
+            if ((tmax - mx) < (mn < 0 ? -mn : mn)) mn = 0;
+        } else {
+            const uint64_t msk = es == 8 ? ~0ull : ((1ull << (8 * es)) - 1);
+            const uint64_t tmax = msk >> 1;
+            const int64_t diff = sext((tmax - (uint64_t)mx) & msk, es);
+            const int64_t absmn = sext((0 - (uint64_t)mn) & msk, es);
+            if (diff < absmn) mn = 0;
+        }
+    }
+    return wrap_es((uint64_t)mn, es);
+}
+
+// static_cast<T>(double) as the reference's x86 host build evaluates it (cvttsd2si)
+__device__ __forceinline__ uint64_t d_cast_double_to_T(double d, int dt, int es)
+{
+    if (dt == GTSC_FLOAT) return __float_as_uint(__double2float_rn(d));
+    if (dt == GTSC_DOUBLE) return (uint64_t)__double_as_longlong(d);
+    if (dt == GTSC_TIME) {
+        if (!(d >= -9223372036854775808.0 && d < 9223372036854775808.0)) return 0x8000000000000000ull;
+        return (uint64_t)__double2ll_rz(d);
+    }
+    (void)es;
+    if (!(d > -2147483649.0 && d < 2147483648.0)) return (uint64_t)(int64_t)INT32_MIN;
+    return (uint64_t)(int64_t)__double2int_rz(d);
+}
+__device__ __forceinline__ double d_T_to_double(uint64_t u, int dt, int es)
+{
+    if (dt == GTSC_FLOAT) return (double)__uint_as_float((uint32_t)u);
+    if (dt == GTSC_DOUBLE) return __longlong_as_double((long long)u);
+    if (dt == GTSC_TIME) return __ll2double_rn((long long)u);
+    return (double)sext(u, es);
+}
+// LowerPatchEncoding::GetOperator<T> (lower_patch_encoding.cu:22-31), factor 0.1, x86 casts
+__device__ __forceinline__ uint64_t d_patch_threshold(uint64_t mnb, uint64_t mxb, int dt, int es)
+{
+    const double dmin = d_T_to_double(mnb, dt, es), dmax = d_T_to_double(mxb, dt, es);
+    const uint64_t dist_bits = d_cast_double_to_T(__dsub_rn(dmax, dmin), dt, es);
+    const double ddist = (dt == GTSC_FLOAT || dt == GTSC_DOUBLE) ? d_T_to_double(dist_bits, dt, es)
+                                                                   : (double)sext(dist_bits, es);
+    return d_cast_double_to_T(__dsub_rn(dmax, __dmul_rn(0.1, ddist)), dt, es);
+}
+
+// (int)(logf(10^k) / logf(10)) with CUDA's logf (cuda_array_statistics.cu:43)
+__device__ __forceinline__ int d_precision_of(int steps)
+{
+    long long e = 1;
+    for (int i = 0; i < steps; i++) e *= 10;
+    return (int)(logf((float)e) / logf(10.0f));
+}
+
+__device__ __forceinline__ int d_precision_steps(float x)
+{
+    long long e = 1;
+    int k = 0;
+    while (true) {
+        const float fe = (float)e;
+        const float q = __fdiv_rn(roundf(__fmul_rn(x, fe)), fe);
+        if (!(q != x && e < 10000000000ll)) break;
+        e *= 10;
+        ++k;
+    }
+    return k;
+}
+
+// GFC geometry (gfc_encoding.cpp:29-33 / 76-80, impl_double.cu:156-179)
+struct DGfc {
+    uint64_t n, npad, per;
+    int64_t warps;
+    int blocks, wpb, unit;
+};
+__device__ __forceinline__ DGfc d_gfc_geom(bool dbl, uint64_t n, int blocks, int wpb)
+{
+    DGfc g;
+    g.n = n;
+    g.npad = (n + 31) & ~31ull;
+    g.unit = dbl ? 17 : 9;
+    if (blocks > 0) {
+        g.blocks = blocks;
+        g.wpb = wpb;
+    } else {
+        g.wpb = dbl ? 16 : 32;
+        const uint64_t bs = (uint64_t)g.wpb * (dbl ? 64 : 32) * 32;
+        g.blocks = (int)((n + bs - 1) / bs);
+    }
+    g.warps = (int64_t)g.blocks * g.wpb;
+    uint64_t per = g.warps ? (g.npad + g.warps - 1) / g.warps : 32;
+    if (per < 32) per = 32;
+    g.per = (per + 31) & ~31ull;
+    return g;
+}
+__device__ __forceinline__ uint64_t d_gfc_cut(const DGfc &g, int64_t i)
+{
+    const uint64_t c = (uint64_t)(i + 1) * g.per;
+    return c < g.npad ? c : g.npad;
+}
+__device__ __forceinline__ uint64_t d_gfc_begin(const DGfc &g, int64_t w) { return w ? d_gfc_cut(g, w - 1) : 0; }
+__device__ __forceinline__ uint64_t d_gfc_start(const DGfc &g, int64_t w) { return (d_gfc_begin(g, w) + 1) / 2 * (uint64_t)g.unit; }
+
+// the stage kernel skeleton: finds this block's (item, tile)
+template <bool DYN>
+__device__ __forceinline__ void locate(const BItem *items, int n_items, uint32_t *counter, BItem &it, uint32_t &tile)
+{
+    __shared__ uint32_t s_tile;
+    __shared__ int s_idx;
+    if (threadIdx.x == 0) {
+        const uint64_t t = DYN ? (uint64_t)atomicAdd(counter, 1u) : (uint64_t)blockIdx.x;
+        int lo = 0, hi = n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (items[mid].tile_base <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        s_idx = lo;
+        s_tile = (uint32_t)(t - items[lo].tile_base);
+    }
+    __syncthreads();
+    it = items[s_idx];
+    tile = s_tile;
+}
+
+}  // namespace gtsc

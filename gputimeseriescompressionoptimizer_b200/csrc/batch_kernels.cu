@@ -1,0 +1,965 @@
+// batch_kernels.cu -- the compress passes of the batched engine.
+//
+// Each pass is one templated stage kernel launched with one block per (item, tile); the block finds
+// its item by binary search over the items' first tiles.  Passes that rank elements across tiles
+// (split, RLE heads, GFC offsets) claim tiles from a counter and chain them with the decoupled
+// look-back of scan.cuh, per item.  Every pass reads its input length from the stream table and
+// writes its outputs' lengths there; tile 0 (or the tile that ends the input) writes metadata.
+// Byte layouts are the per-encoding ones of encodings.cu (and of the reference).
+#include "batch_dev.cuh"
+
+#include <type_traits>
+
+namespace gtsc {
+
+namespace {
+
+// ------------------------------------------------------------------------------- min / max
+template <int ES>
+__device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    const uint64_t t0 = (uint64_t)tile * kBMinMaxTile;
+    if (t0 >= n) return;
+    const uint64_t end = n < t0 + kBMinMaxTile ? n : t0 + kBMinMaxTile;
+    const Order o = (Order)it.order;
+    constexpr int PER = 16 / ES;
+    uint64_t kmin = ~0ull, kmax = 0;
+    for (uint64_t i = t0 + (uint64_t)threadIdx.x * PER; i < end; i += (uint64_t)kBThreads * PER) {
+        if (i + PER <= end) {
+            const uint4 c = ld_chunk(in.ptr + i * ES);
+#pragma unroll
+            for (int j = 0; j < PER; j++) {
+                const uint64_t u = chunk_elem<ES>(c, j);
+                if (is_nan_bits(u, o)) continue;
+                const uint64_t k = order_key(u, ES, o);
+                kmin = k < kmin ? k : kmin;
+                kmax = k > kmax ? k : kmax;
+            }
+        } else {
+            for (uint64_t j = i; j < end; j++) {
+                const uint64_t u = ld_elem<ES>(in.ptr, j);
+                if (is_nan_bits(u, o)) continue;
+                const uint64_t k = order_key(u, ES, o);
+                kmin = k < kmin ? k : kmin;
+                kmax = k > kmax ? k : kmax;
+            }
+        }
+    }
+    block_minmax(kmin, kmax);
+    if (threadIdx.x == 0) {
+        MinMaxAcc *acc = (MinMaxAcc *)it.scratch;
+        if (kmin != ~0ull) atomicMax(&acc->nkmin, (unsigned long long)~kmin);
+        if (kmax != 0) atomicMax(&acc->kmax, (unsigned long long)kmax);
+    }
+}
+
+// ------------------------------------------------------------------------------- delta
+template <int ES>
+__device__ void p_delta_enc(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    if (tile == 0 && threadIdx.x == 0) {
+        StreamDesc &m = S[it.out[0]];
+        if (n) {
+            st_elem<ES>(m.ptr, 0, ld_elem<ES>(in.ptr, 0));
+            m.len = ES;
+            S[it.out[1]].len = (n - 1) * ES;
+        } else {
+            m.len = 0;
+            S[it.out[1]].len = 0;
+        }
+    }
+    const uint64_t m = n ? n - 1 : 0;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    if (base >= m) return;
+    uint8_t *out = S[it.out[1]].ptr;
+    uint64_t v[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) v[j] = base + j < n ? ld_elem<ES>(in.ptr, base + j) : 0;
+    uint64_t d[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) d[j] = wrap_es(v[j + 1] - v[j], ES);
+    if (base + 8 <= m && (8 * ES) % 16 == 0) {
+        constexpr int PER = 16 / ES;
+#pragma unroll
+        for (int c = 0; c < 8 / PER; c++)
+            reinterpret_cast<uint4 *>(out + (base + c * PER) * ES)[0] = make_chunk<ES>(d + c * PER);
+    } else {
+        for (int j = 0; j < 8; j++)
+            if (base + j < m) st_elem<ES>(out, base + j, d[j]);
+    }
+}
+
+// ------------------------------------------------------------------------------- scale
+template <int ES>
+__device__ void p_scale_sub(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    uint64_t mnb = 0, mxb = 0;
+    acc_minmax((const MinMaxAcc *)it.scratch, ES, ORD_INT, mnb, mxb);
+    const uint64_t mn = scale_min(mnb, mxb, ES);
+    if (tile == 0 && threadIdx.x == 0) {
+        if (n) {
+            st_elem<ES>(S[it.out[0]].ptr, 0, mn);
+            S[it.out[0]].len = ES;
+        } else {
+            S[it.out[0]].len = 0;
+        }
+        S[it.out[1]].len = n * ES;
+    }
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    if (base >= n) return;
+    uint8_t *out = S[it.out[1]].ptr;
+    uint64_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = base + j < n ? wrap_es(ld_elem<ES>(in.ptr, base + j) - mn, ES) : 0;
+    if (base + 8 <= n && (8 * ES) % 16 == 0) {
+        constexpr int PER = 16 / ES;
+#pragma unroll
+        for (int c = 0; c < 8 / PER; c++)
+            reinterpret_cast<uint4 *>(out + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
+    } else {
+        for (int j = 0; j < 8; j++)
+            if (base + j < n) st_elem<ES>(out, base + j, v[j]);
+    }
+}
+
+// ------------------------------------------------------------------------------- AFL pack
+template <int ES>
+__device__ void p_afl_pack(const BItem &it, uint32_t tile, StreamDesc *S, unsigned long long *sv)
+{
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    uint64_t mnb = 0, mxb = 0;
+    acc_minmax((const MinMaxAcc *)it.scratch, ES, ORD_INT, mnb, mxb);
+    const int b = bitlen_signed(sext(mnb, ES), sext(mxb, ES), ES);
+    const uint64_t W = 8ull * ES;
+    const uint64_t out_bytes = n ? (b * n + W - 1) / W * ES : 0;
+    if (tile == 0 && threadIdx.x == 0) {
+        StreamDesc &m = S[it.out[0]];
+        if (n) {
+            m.ptr[0] = (uint8_t)b;
+            m.ptr[1] = (uint8_t)(int8_t)(out_bytes * 8 - n * (uint64_t)b);
+            m.ptr[2] = 0;
+            m.ptr[3] = 0;
+            m.len = 4;
+        } else {
+            m.len = 0;
+        }
+        S[it.out[1]].len = out_bytes;
+    }
+    const uint64_t t0 = (uint64_t)tile * kBTile;
+    if (t0 >= n) return;
+    uint8_t *out = S[it.out[1]].ptr;
+    const uint64_t vmask = b >= 64 ? ~0ull : ((1ull << b) - 1);
+    const uint64_t cnt = n - t0 < kBTile ? n - t0 : kBTile;
+    const uint8_t *src = in.ptr + t0 * ES;
+    if (cnt == kBTile) {
+        constexpr int PER = 16 / ES;
+        for (int c = threadIdx.x; c < (int)kBTile / PER; c += kBThreads) {
+            const uint4 v = ld_chunk(src + 16 * c);
+#pragma unroll
+            for (int j = 0; j < PER; j++) sv[c * PER + j] = chunk_elem<ES>(v, j) & vmask;
+        }
+    } else {
+        for (int i = threadIdx.x; i < (int)kBTile; i += kBThreads)
+            sv[i] = (uint64_t)i < cnt ? (ld_elem<ES>(src, i) & vmask) : 0ull;
+    }
+    if (threadIdx.x < 4) sv[kBTile + threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t total_words = (out_bytes + 3) / 4;
+    const uint64_t w0 = t0 * (uint64_t)b / 32;
+    uint64_t w_end = (t0 + kBTile) * (uint64_t)b / 32;
+    if (w_end > total_words) w_end = total_words;
+    for (uint64_t w = w0 + threadIdx.x; w < w_end; w += kBThreads) {
+        const uint32_t p = (uint32_t)(w - w0) * 32u;
+        uint32_t a = p / (uint32_t)b;
+        const uint32_t s = p - a * (uint32_t)b;
+        uint64_t acc = sv[a] >> s;
+        int filled = b - (int)s;
+        ++a;
+        while (filled < 32) {
+            acc |= sv[a] << filled;
+            filled += b;
+            ++a;
+        }
+        const uint32_t word = (uint32_t)acc;
+        if (4 * w + 4 <= out_bytes) {
+            reinterpret_cast<uint32_t *>(out)[w] = word;
+        } else {
+            for (int k = 0; k < 4; k++)
+                if (4 * w + k < out_bytes) out[4 * w + k] = (uint8_t)(word >> (8 * k));
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------- histogram
+__device__ __forceinline__ uint64_t bhash(uint64_t k)
+{
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return k;
+}
+
+struct HTab {
+    BHistHdr *hdr;
+    unsigned long long *keys;
+    unsigned int *counts;
+    unsigned int *used;
+    unsigned long long *nan;
+    uint64_t cap;
+};
+__device__ __forceinline__ HTab htab(const BItem &it)
+{
+    // p[0] = table capacity, p[1] = histogram tiles, p[2] = table offset in the node scratch
+    HTab t;
+    t.cap = it.p[0];
+    uint8_t *b = it.scratch + it.p[2];
+    t.hdr = (BHistHdr *)b;
+    t.keys = (unsigned long long *)(b + 16);
+    t.counts = (unsigned int *)(b + 16 + 8 * t.cap);
+    t.used = (unsigned int *)(b + 16 + 12 * t.cap);
+    t.nan = (unsigned long long *)(b + 16 + 16 * t.cap);
+    return t;
+}
+
+__device__ void g_insert(const HTab &t, unsigned long long key, unsigned int c, uint32_t *status)
+{
+    constexpr unsigned long long EMPTY = ~0ull;
+    if (key == EMPTY) {
+        atomicAdd(&t.hdr->special, c);
+        return;
+    }
+    const uint64_t mask = t.cap - 1;
+    uint64_t h = bhash(key) & mask;
+    for (uint64_t probe = 0; probe < t.cap && probe < 8192; probe++) {
+        const unsigned long long prev = atomicCAS(t.keys + h, EMPTY, key);
+        if (prev == EMPTY) {
+            const unsigned int u = atomicAdd(&t.hdr->used, 1u);
+            t.used[u] = (unsigned int)h;
+            atomicAdd(t.counts + h, c);
+            return;
+        }
+        if (prev == key) {
+            atomicAdd(t.counts + h, c);
+            return;
+        }
+        h = (h + 1) & mask;
+    }
+    atomicExch(&t.hdr->overflow, 1u);
+    set_status(status, GTSC_ERR_CAPACITY);
+}
+
+template <int ES>
+__device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, unsigned char *smem)
+{
+    constexpr unsigned long long EMPTY = ~0ull;
+    unsigned long long *skeys = (unsigned long long *)smem;
+    unsigned int *scounts = (unsigned int *)(smem + 8 * kBHistSmem);
+    unsigned long long(*snan)[4] = (unsigned long long(*)[4])(smem + 12 * kBHistSmem);
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    const uint64_t t0 = (uint64_t)tile * kBHistTile;
+    const HTab t = htab(it);
+    const Order o = (Order)it.order;
+    if (it.mode == 4 && t0 < n) {
+        // dict: clear this tile's share of the 2-bit code words (out1 after its 16 + 4*es header)
+        uint32_t *words = (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES);
+        const uint64_t e_end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
+        for (uint64_t w = t0 / 16 + threadIdx.x; w < (e_end + 15) / 16; w += kBThreads) words[w] = 0u;
+    }
+    unsigned long long nan_min[4] = {EMPTY, EMPTY, EMPTY, EMPTY};
+    if (t0 < n) {
+        for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads) {
+            skeys[i] = EMPTY;
+            scounts[i] = 0;
+        }
+        __syncthreads();
+        const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
+        for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
+            const unsigned long long key = ld_elem<ES>(in.ptr, i);
+            if (is_nan_bits(key, o)) {
+                unsigned long long k = order_key(key, ES, o);
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
+                continue;
+            }
+            bool done = false;
+            if (key != EMPTY) {
+                uint32_t h = (uint32_t)bhash(key) & (kBHistSmem - 1);
+                for (int p = 0; p < 8; p++) {
+                    const unsigned long long prev = atomicCAS(&skeys[h], EMPTY, key);
+                    if (prev == EMPTY || prev == key) {
+                        atomicAdd(&scounts[h], 1u);
+                        done = true;
+                        break;
+                    }
+                    h = (h + 1) & (kBHistSmem - 1);
+                }
+            }
+            if (!done) g_insert(t, key, 1u, status);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads)
+            if (skeys[i] != EMPTY) g_insert(t, skeys[i], scounts[i], status);
+    }
+    // this tile's 4 smallest NaN sort keys
+    for (int off = 16; off > 0; off >>= 1) {
+        unsigned long long other[4], merged[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) other[j] = __shfl_xor_sync(0xffffffffu, nan_min[j], off);
+        int a = 0, b2 = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) merged[j] = (nan_min[a] <= other[b2]) ? nan_min[a++] : other[b2++];
+#pragma unroll
+        for (int j = 0; j < 4; j++) nan_min[j] = merged[j];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int j = 0; j < 4; j++) snan[warp][j] = nan_min[j];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long best[4] = {EMPTY, EMPTY, EMPTY, EMPTY};
+        for (int w = 0; w < kBThreads / 32; w++)
+            for (int j = 0; j < 4; j++) {
+                unsigned long long k = snan[w][j];
+                for (int q = 0; q < 4; q++)
+                    if (k < best[q]) { const unsigned long long x = best[q]; best[q] = k; k = x; }
+            }
+        for (int j = 0; j < 4; j++) t.nan[4 * tile + j] = best[j];
+    }
+}
+
+struct Cand {
+    unsigned long long key, bits;
+    unsigned int count;
+};
+__device__ __forceinline__ bool cbetter(const Cand &a, const Cand &b)
+{
+    return a.count > b.count || (a.count == b.count && a.count != 0 && a.key < b.key);
+}
+__device__ __forceinline__ void cpush(Cand *l, const Cand &c)
+{
+    if (!cbetter(c, l[3])) return;
+    l[3] = c;
+#pragma unroll
+    for (int i = 3; i > 0; i--)
+        if (cbetter(l[i], l[i - 1])) { const Cand x = l[i]; l[i] = l[i - 1]; l[i - 1] = x; }
+}
+
+// one block per item: the k most frequent values, then the table is cleared for the next step
+template <int ES>
+__device__ void p_topk(const BItem &it, StreamDesc *S, unsigned char *smem)
+{
+    constexpr unsigned long long EMPTY = ~0ull;
+    Cand *sc = (Cand *)smem;
+    const HTab t = htab(it);
+    const Order o = (Order)it.order;
+    const unsigned int used = t.hdr->used;
+    Cand l[4];
+    for (int j = 0; j < 4; j++) l[j] = Cand{EMPTY, 0, 0};
+    for (unsigned int i = threadIdx.x; i < used; i += kBThreads) {
+        const unsigned int h = t.used[i];
+        const unsigned long long k = t.keys[h];
+        cpush(l, Cand{order_key(k, ES, o), k, t.counts[h]});
+    }
+    if (threadIdx.x == 0 && t.hdr->special) cpush(l, Cand{order_key(EMPTY, ES, o), EMPTY, t.hdr->special});
+    for (uint64_t i = threadIdx.x; i < 4 * it.p[1]; i += kBThreads) {
+        const unsigned long long k = t.nan[i];
+        if (k != EMPTY) cpush(l, Cand{k, order_unkey(k, ES, o), 1u});
+    }
+    for (int j = 0; j < 4; j++) sc[threadIdx.x * 4 + j] = l[j];
+    __syncthreads();
+    for (int width = kBThreads / 2; width > 0; width >>= 1) {
+        if ((int)threadIdx.x < width) {
+            Cand mine[4] = {sc[threadIdx.x * 4], sc[threadIdx.x * 4 + 1], sc[threadIdx.x * 4 + 2], sc[threadIdx.x * 4 + 3]};
+            for (int j = 0; j < 4; j++) cpush(mine, sc[(threadIdx.x + width) * 4 + j]);
+            for (int j = 0; j < 4; j++) sc[threadIdx.x * 4 + j] = mine[j];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const int k = it.mode;  // 1: const -> meta[0..es), 4: dict -> out1[16 ..)
+        uint8_t *dst = k == 1 ? S[it.out[0]].ptr : S[it.out[1]].ptr + 16;
+        for (int j = 0; j < k; j++) st_elem<ES>(dst, j, sc[j].count ? sc[j].bits : 0ull);
+    }
+    __syncthreads();
+    for (unsigned int i = threadIdx.x; i < used; i += kBThreads) {
+        const unsigned int h = t.used[i];
+        t.keys[h] = EMPTY;
+        t.counts[h] = 0;
+    }
+    if (threadIdx.x == 0) {
+        t.hdr->used = 0;
+        t.hdr->special = 0;
+        t.hdr->overflow = 0;
+    }
+}
+
+// ------------------------------------------------------------------------------- split
+template <int ES>
+__device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+{
+    __shared__ unsigned long long ws[32];
+    __shared__ unsigned long long s_prefix;
+    const int mode = it.mode;
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    const Order o = (Order)it.order;
+    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
+    // stencil location and the values matched against
+    uint8_t *meta = S[it.out[0]].ptr;
+    uint8_t *stencil = mode == SPLIT_NOT_CONST ? meta + ES + 1 : meta + 1;
+    uint64_t top[4] = {0, 0, 0, 0}, thr = 0;
+    if (mode == SPLIT_LOWER) {
+        uint64_t mnb = 0, mxb = 0;
+        if (!acc_minmax((const MinMaxAcc *)it.scratch, ES, o, mnb, mxb) && n) mnb = mxb = ld_elem<ES>(in.ptr, 0);
+        thr = d_patch_threshold(mnb, mxb, it.dt, ES);
+    } else if (mode == SPLIT_NOT_CONST) {
+        top[0] = ld_elem<ES>(meta, 0);
+    } else {
+        const uint8_t *tp = S[it.out[1]].ptr + 16;
+        for (int k = 0; k < 4; k++) top[k] = ld_unaligned<ES>(tp + k * ES);
+    }
+    if (tile == 0 && threadIdx.x == 0) {
+        (mode == SPLIT_NOT_CONST ? meta[ES] : meta[0]) = (uint8_t)(n % 8);
+        if (n == 0) {
+            S[it.out[0]].len = 0;
+            S[it.out[1]].len = 0;
+            if (mode != SPLIT_NOT_CONST) S[it.out[2]].len = 0;
+        }
+    }
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    uint64_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = base + j < n ? ld_elem<ES>(in.ptr, base + j) : 0;
+    uint32_t bits = 0, codes = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        bool f = false;
+        uint32_t code = 0;
+        if (mode == SPLIT_LOWER) f = lt_native(v[j], thr, ES, o);
+        else if (mode == SPLIT_NOT_CONST) f = !bsame(v[j], top[0], o);
+        else {
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (bsame(v[j], top[k], o)) { f = true; code |= (uint32_t)k; }
+        }
+        bits |= (uint32_t)f << j;
+        codes |= code << (2 * j);
+    }
+    if (base < n) {
+        const uint64_t valid = n - base;
+        if (valid < 8) {
+            const uint32_t last = (bits >> (valid - 1)) & 1u;
+            for (int j = (int)valid; j < 8; j++) bits = (bits & ~(1u << j)) | (last << j);
+        }
+        stencil[base / 8] = (uint8_t)bits;
+    }
+    const uint32_t valid_mask = base >= n ? 0u : (n - base >= 8 ? 0xffu : ((1u << (n - base)) - 1));
+    const uint32_t yes_bits = bits & valid_mask;
+    unsigned long long total;
+    const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(yes_bits), ws, total);
+    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    __syncthreads();
+    uint64_t yes_pos = s_prefix + excl;
+    uint64_t no_pos = (base < n ? base : n) - yes_pos;
+    uint8_t *yes = S[it.out[1]].ptr;
+    uint8_t *no = mode == SPLIT_NOT_CONST ? nullptr : S[it.out[2]].ptr;
+    uint32_t *words = mode == SPLIT_DICT ? (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES) : nullptr;
+    for (int j = 0; j < 8; j++) {
+        if (!((valid_mask >> j) & 1u)) break;
+        if ((yes_bits >> j) & 1u) {
+            if (mode == SPLIT_DICT) {
+                const uint32_t c = (codes >> (2 * j)) & 3u;
+                if (c) atomicOr(words + (yes_pos >> 4), c << (2 * (yes_pos & 15)));
+            } else {
+                st_elem<ES>(yes, yes_pos, v[j]);
+            }
+            ++yes_pos;
+        } else {
+            if (mode != SPLIT_NOT_CONST) st_elem<ES>(no, no_pos, v[j]);
+            ++no_pos;
+        }
+    }
+    if (base < n && base + 8 >= n) {  // the thread holding the last element: lengths and headers
+        const uint64_t m = yes_pos;
+        if (mode == SPLIT_LOWER) {
+            S[it.out[0]].len = 1 + (n + 7) / 8;
+            S[it.out[1]].len = m * ES;
+            S[it.out[2]].len = (n - m) * ES;
+        } else if (mode == SPLIT_NOT_CONST) {
+            S[it.out[0]].len = ES + 1 + (n + 7) / 8;
+            S[it.out[1]].len = m * ES;
+        } else {
+            uint64_t *sz = (uint64_t *)S[it.out[1]].ptr;
+            sz[0] = 4;
+            sz[1] = m;
+            S[it.out[0]].len = 1 + (n + 7) / 8;
+            S[it.out[1]].len = m ? 16 + 4 * ES + 4 * ((m + 15) / 16) : 0;
+            S[it.out[2]].len = (n - m) * ES;
+        }
+    }
+    (void)status;
+}
+
+// ------------------------------------------------------------------------------- RLE
+template <int ES>
+__device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    __shared__ unsigned long long ws[32];
+    __shared__ unsigned long long s_prefix;
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    const Order o = (Order)it.order;
+    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
+    uint32_t *starts = (uint32_t *)(it.scratch + it.p[1]);
+    if (n == 0) {
+        if (tile == 0 && threadIdx.x == 0) {
+            *(int32_t *)S[it.out[0]].ptr = 0;
+            S[it.out[0]].len = 4;
+            S[it.out[1]].len = 0;
+            S[it.out[2]].len = 0;
+        }
+        return;
+    }
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    uint64_t v[9];
+    v[0] = base > 0 && base - 1 < n ? ld_elem<ES>(in.ptr, base - 1) : 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j + 1] = base + j < n ? ld_elem<ES>(in.ptr, base + j) : 0;
+    uint32_t heads = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const uint64_t i = base + j;
+        if (i < n && (i == 0 || !bsame(v[j + 1], v[j], o))) heads |= 1u << j;
+    }
+    unsigned long long total;
+    const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(heads), ws, total);
+    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    __syncthreads();
+    uint64_t r = s_prefix + excl;
+    uint8_t *values = S[it.out[2]].ptr;
+    for (int j = 0; j < 8; j++)
+        if ((heads >> j) & 1u) {
+            st_elem<ES>(values, r, v[j + 1]);
+            starts[r] = (uint32_t)(base + j);
+            ++r;
+        }
+    if (base < n && base + 8 >= n) {
+        *(int32_t *)S[it.out[0]].ptr = (int32_t)r;
+        S[it.out[0]].len = 4;
+        S[it.out[1]].len = 4 * r;
+        S[it.out[2]].len = ES * r;
+    }
+}
+
+__device__ void p_rle_lengths(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    const uint64_t n = S[it.in[0]].len / it.es;
+    const uint64_t runs = S[it.out[1]].len / 4;
+    const uint32_t *starts = (const uint32_t *)(it.scratch + it.p[1]);
+    int32_t *lengths = (int32_t *)S[it.out[1]].ptr;
+    const uint64_t r0 = (uint64_t)tile * kBTile;
+    for (uint64_t r = r0 + threadIdx.x; r < runs && r < r0 + kBTile; r += kBThreads) {
+        const uint64_t next = r + 1 < runs ? starts[r + 1] : n;
+        lengths[r] = (int32_t)(next - starts[r]);
+    }
+}
+
+// ------------------------------------------------------------------------------- floatToInt
+__device__ __forceinline__ const double *pow10_table()
+{
+    __shared__ double t[10];
+    if (threadIdx.x < 10) {
+        double v = 1.0;
+        for (unsigned i = 0; i < threadIdx.x; i++) v *= 10.0;
+        t[threadIdx.x] = v;
+    }
+    __syncthreads();
+    return t;
+}
+
+template <int ES>
+__device__ __forceinline__ double as_double(uint64_t u, Order o)
+{
+    if (o == ORD_F32) return (double)__uint_as_float((uint32_t)u);
+    if (o == ORD_F64) return __longlong_as_double((long long)u);
+    if (ES == 8) return __ll2double_rn((long long)u);
+    return (double)sext(u, ES);
+}
+
+template <int ES>
+__device__ __forceinline__ float as_float_T(uint64_t u, Order o)
+{
+    if (o == ORD_F32) return __uint_as_float((uint32_t)u);
+    if (o == ORD_F64) return __double2float_rn(__longlong_as_double((long long)u));
+    if (ES == 8) return __ll2float_rn((long long)u);
+    return __int2float_rn((int)sext(u, ES));
+}
+
+template <int ES>
+__device__ __forceinline__ uint64_t f2i_dec_one(int k, int p, Order o, const double *p10)
+{
+    if (o == ORD_F32) return __float_as_uint(__double2float_rn(__ddiv_rn((double)__int2float_rn(k), p10[p])));
+    if (o == ORD_F64) return (uint64_t)__double_as_longlong(__ddiv_rn((double)k, p10[p]));
+    if (ES == 8) return (uint64_t)__double2ll_rz(__ddiv_rn((double)k, p10[p]));
+    const long long t = sext((uint64_t)(long long)k, ES);
+    return (uint64_t)(long long)__double2int_rz(__ddiv_rn((double)t, p10[p]));
+}
+
+// node scratch of floatToInt: StatsAcc at 0, lossy flag at 64
+template <int ES>
+__device__ void p_f2i_stats(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    const uint64_t t0 = (uint64_t)tile * kBTile;
+    if (t0 >= n) return;
+    const Order o = (Order)it.order;
+    uint64_t kmin = ~0ull, kmax = 0;
+    int steps = 0;
+    const uint64_t end = n < t0 + kBTile ? n : t0 + kBTile;
+    for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
+        const uint64_t u = ld_elem<ES>(in.ptr, i);
+        if (!is_nan_bits(u, o)) {
+            const uint64_t k = order_key(u, ES, o);
+            kmin = k < kmin ? k : kmin;
+            kmax = k > kmax ? k : kmax;
+        }
+        const int s = d_precision_steps(as_float_T<ES>(u, o));
+        steps = s > steps ? s : steps;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const int x = __shfl_xor_sync(0xffffffffu, steps, off);
+        steps = x > steps ? x : steps;
+    }
+    __shared__ int s_steps[kBThreads / 32];
+    if ((threadIdx.x & 31) == 0) s_steps[threadIdx.x >> 5] = steps;
+    block_minmax(kmin, kmax);
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kBThreads / 32; w++) steps = s_steps[w] > steps ? s_steps[w] : steps;
+        StatsAcc *acc = (StatsAcc *)it.scratch;
+        if (kmin != ~0ull) atomicMax(&acc->mm.nkmin, (unsigned long long)~kmin);
+        if (kmax != 0) atomicMax(&acc->mm.kmax, (unsigned long long)kmax);
+        atomicMax(&acc->prec_steps, (unsigned int)steps);
+    }
+}
+
+// FloatEncoding::Encode's decision (float_encoding.cu:29-43) from the stats pass
+template <int ES>
+__device__ __forceinline__ int f2i_decide(const BItem &it, const uint8_t *col, uint64_t n, bool &transform)
+{
+    const StatsAcc *acc = (const StatsAcc *)it.scratch;
+    const Order o = (Order)it.order;
+    const unsigned steps = acc->prec_steps > 10 ? 10 : acc->prec_steps;
+    int p = d_precision_of((int)steps);
+    transform = false;
+    if (p < 10 && n) {
+        uint64_t mnb = 0, mxb = 0;
+        if (!acc_minmax(&acc->mm, ES, o, mnb, mxb)) mnb = mxb = ld_elem<ES>(col, 0);
+        long long sc = 1;
+        for (int i = 0; i < p; i++) sc *= 10;
+        bool ok;
+        if (o == ORD_F32) {
+            const float a = __fmul_rn(__uint_as_float((uint32_t)mnb), (float)sc);
+            const float b = __fmul_rn(__uint_as_float((uint32_t)mxb), (float)sc);
+            ok = a > -2147483648.0f && b < 2147483648.0f;
+        } else if (o == ORD_F64) {
+            const double a = __dmul_rn(__longlong_as_double((long long)mnb), (double)sc);
+            const double b = __dmul_rn(__longlong_as_double((long long)mxb), (double)sc);
+            ok = a > -2147483648.0 && b < 2147483647.0;
+        } else {
+            ok = sext(mnb, ES) * sc > (long long)INT32_MIN && sext(mxb, ES) * sc < (long long)INT32_MAX;
+        }
+        if (ok) transform = true;
+        else p = 10;
+    }
+    return p;
+}
+
+template <int ES>
+__device__ void p_f2i_enc(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    const double *p10 = pow10_table();
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    bool transform;
+    const int p = f2i_decide<ES>(it, in.ptr, n, transform);
+    if (tile == 0 && threadIdx.x == 0) {
+        if (n) {
+            *(int32_t *)S[it.out[0]].ptr = p;
+            S[it.out[0]].len = 4;
+            S[it.out[1]].len = transform ? 4 * n : (n * ES) / 4 * 4;
+        } else {
+            S[it.out[0]].len = 0;
+            S[it.out[1]].len = 0;
+        }
+    }
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    if (base >= n) return;
+    uint8_t *out = S[it.out[1]].ptr;
+    if (transform) {
+        const Order o = (Order)it.order;
+        const uint64_t wm = ES == 8 ? ~0ull : ((1ull << (8 * ES)) - 1);
+        bool bad = false;
+        for (int j = 0; j < 8 && base + j < n; j++) {
+            const uint64_t u = ld_elem<ES>(in.ptr, base + j);
+            const int k = (int)(long long)__double2ll_rn(__dmul_rn(as_double<ES>(u, o), p10[p]));
+            ((int32_t *)out)[base + j] = k;
+            if (((f2i_dec_one<ES>(k, p, o, p10) ^ u) & wm) != 0) bad = true;
+        }
+        if (bad) atomicExch((unsigned int *)(it.scratch + 64), 1u);
+    } else {
+        const uint64_t bytes = (n * ES) / 4 * 4;
+        for (uint64_t b = base * ES; b < (base + 8) * ES && b < bytes; b++) out[b] = in.ptr[b];
+    }
+}
+
+// the lossless check failed: the raw p = 10 branch
+template <int ES>
+__device__ void p_f2i_raw(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    if (*(volatile unsigned int *)(it.scratch + 64) == 0) return;
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / ES;
+    const uint64_t bytes = (n * ES) / 4 * 4;
+    if (tile == 0 && threadIdx.x == 0) {
+        *(int32_t *)S[it.out[0]].ptr = 10;
+        S[it.out[1]].len = bytes;
+    }
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    uint8_t *out = S[it.out[1]].ptr;
+    for (uint64_t b = base * ES; b < (base + 8) * ES && b < bytes; b++) out[b] = in.ptr[b];
+}
+
+// ------------------------------------------------------------------------------- GFC
+// node scratch of GFC: p[0] look-back, p[1] chunk sizes (int32), p[2] inclusive ends (u64), p[3] layout
+template <bool DBL>
+__device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    const StreamDesc in = S[it.in[0]];
+    const uint64_t n = in.len / (DBL ? 8 : 4);
+    const DGfc g = d_gfc_geom(DBL, n, 0, 0);
+    if (tile == 0 && threadIdx.x == 0) {
+        if (n) {
+            int32_t *m = (int32_t *)S[it.out[0]].ptr;
+            m[0] = g.blocks;
+            m[1] = g.wpb;
+            m[2] = (int32_t)n;
+            S[it.out[0]].len = 12;
+            S[it.out[1]].len = 4 * (uint64_t)g.warps;
+        } else {
+            S[it.out[0]].len = 0;
+            S[it.out[1]].len = 0;
+            S[it.out[2]].len = 0;
+        }
+    }
+    const int lane = threadIdx.x & 31;
+    const int64_t w = (int64_t)tile * kBGfcChunks + (threadIdx.x >> 5);
+    if (w >= g.warps) return;
+    uint8_t *layout = it.scratch + it.p[3];
+    int32_t *sizes = (int32_t *)(it.scratch + it.p[1]);
+    int32_t *ends = (int32_t *)S[it.out[1]].ptr;
+    const uint64_t cb = d_gfc_begin(g, w), ce = d_gfc_cut(g, w);
+    const uint64_t start = d_gfc_start(g, w);
+    uint64_t off = start, last = 0;
+    for (uint64_t s = cb; s < ce; s += 32) {
+        const uint64_t i = s + lane;
+        uint64_t x = 0;
+        if (i < n) x = DBL ? ld_elem<8>(in.ptr, i) : ld_elem<4>(in.ptr, i);
+        uint64_t diff;
+        uint32_t sign, mb, code;
+        if (DBL) {
+            diff = x - last;
+            sign = (uint32_t)((diff >> 60) & 8);
+            if (sign) diff = 0ull - diff;
+            const uint32_t lz = (uint32_t)__clzll((long long)diff) >> 3;
+            mb = lz == 6 ? 3 : 8 - lz;
+            code = mb >= 3 ? mb - 1 : mb;
+        } else {
+            uint32_t d = (uint32_t)x - (uint32_t)last;
+            sign = (d >> 28) & 8;
+            if (sign) d = 0u - d;
+            mb = 4 - ((uint32_t)__clz((int)d) >> 3);
+            code = mb;
+            diff = d;
+        }
+        const uint32_t nib = sign | code;
+        uint32_t incl = mb;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t prev_nib = __shfl_up_sync(0xffffffffu, nib, 1);
+        if (lane & 1) layout[off + (lane >> 1)] = (uint8_t)(prev_nib | (nib << 4));
+        uint8_t *dst = layout + off + 16 + (incl - mb);
+        for (uint32_t b = 0; b < mb; b++) dst[b] = (uint8_t)(diff >> (8 * b));
+        off += 16 + total;
+        if (s == cb) last = __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 31) {
+        ends[w] = (int32_t)off;
+        sizes[w] = (int32_t)(off - start);
+    }
+}
+
+// inclusive scan of the chunk sizes (compress: this node's; decode: p[1])
+__device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool dbl, bool decode)
+{
+    __shared__ unsigned long long ws[32];
+    __shared__ unsigned long long s_prefix;
+    uint64_t n;
+    int blocks = 0, wpb = 0;
+    if (decode) {
+        const StreamDesc m = S[it.in[0]];
+        if (m.len < 12) return;
+        blocks = (int32_t)ld_unaligned<4>(m.ptr);
+        wpb = (int32_t)ld_unaligned<4>(m.ptr + 4);
+        n = (uint64_t)(int32_t)ld_unaligned<4>(m.ptr + 8);
+        if (blocks <= 0 || wpb <= 0) return;
+    } else {
+        n = S[it.in[0]].len / (dbl ? 8 : 4);
+    }
+    const DGfc g = d_gfc_geom(dbl, n, blocks, wpb);
+    // decode: p[3] = the chunks the scratch holds (a larger count is reported by the sizes pass)
+    if (decode && (uint64_t)g.warps > it.p[3]) return;
+    const int32_t *sizes = (const int32_t *)(it.scratch + it.p[1]);
+    unsigned long long *incl = (unsigned long long *)(it.scratch + it.p[2]);
+    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    unsigned long long v[8], local = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        v[j] = base + j < (uint64_t)g.warps ? (unsigned long long)(uint32_t)sizes[base + j] : 0ull;
+        local += v[j];
+    }
+    unsigned long long total;
+    const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
+    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    __syncthreads();
+    unsigned long long acc = s_prefix + excl;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        acc += v[j];
+        if (base + j < (uint64_t)g.warps) incl[base + j] = acc;
+    }
+}
+
+template <bool DBL>
+__device__ void p_gfc_compact(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    const uint64_t n = S[it.in[0]].len / (DBL ? 8 : 4);
+    const DGfc g = d_gfc_geom(DBL, n, 0, 0);
+    const int lane = threadIdx.x & 31;
+    const int64_t w = (int64_t)tile * kBGfcChunks + (threadIdx.x >> 5);
+    if (w >= g.warps) return;
+    const int32_t *sizes = (const int32_t *)(it.scratch + it.p[1]);
+    const unsigned long long *incl = (const unsigned long long *)(it.scratch + it.p[2]);
+    const uint8_t *layout = it.scratch + it.p[3];
+    const uint64_t size = (uint64_t)(uint32_t)sizes[w];
+    const uint64_t dst0 = incl[w] - size;
+    const uint8_t *src = layout + d_gfc_start(g, w);
+    uint8_t *out = S[it.out[2]].ptr;
+    for (uint64_t b = lane; b < size; b += 32) out[dst0 + b] = src[b];
+    if (w == g.warps - 1 && lane == 0) S[it.out[2]].len = incl[w];
+}
+
+// ------------------------------------------------------------------------------- dispatch
+constexpr size_t stage_smem(int op)
+{
+    return op == B_AFL_PACK ? 8 * (kBTile + 4)
+         : op == B_HIST     ? 12 * kBHistSmem + 8 * 4 * (kBThreads / 32)
+         : op == B_TOPK     ? sizeof(Cand) * kBThreads * 4
+                            : 16;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(kBThreads)
+k_bstage(const BItem *items, int n_items, StreamDesc *S, uint32_t *counter, uint32_t *status)
+{
+    constexpr bool DYN = OP == B_SPLIT || OP == B_RLE_HEADS || OP == B_GFC_SCAN;
+    __shared__ __align__(16) unsigned char smem[stage_smem(OP)];
+    BItem it;
+    uint32_t tile;
+    locate<DYN>(items, n_items, counter, it, tile);
+    if (tile >= it.tiles) return;
+#define GTSC_ES_SWITCH(CALL)                       \
+    switch (it.es) {                               \
+    case 1: { constexpr int E = 1; CALL; } break;  \
+    case 2: { constexpr int E = 2; CALL; } break;  \
+    case 4: { constexpr int E = 4; CALL; } break;  \
+    default: { constexpr int E = 8; CALL; } break; \
+    }
+    if constexpr (OP == B_MINMAX) { GTSC_ES_SWITCH(p_minmax<E>(it, tile, S)) }
+    else if constexpr (OP == B_DELTA_ENC) { GTSC_ES_SWITCH(p_delta_enc<E>(it, tile, S)) }
+    else if constexpr (OP == B_SCALE_SUB) { GTSC_ES_SWITCH(p_scale_sub<E>(it, tile, S)) }
+    else if constexpr (OP == B_AFL_PACK) { GTSC_ES_SWITCH(p_afl_pack<E>(it, tile, S, (unsigned long long *)smem)) }
+    else if constexpr (OP == B_HIST) { GTSC_ES_SWITCH(p_hist<E>(it, tile, S, status, smem)) }
+    else if constexpr (OP == B_TOPK) { GTSC_ES_SWITCH(p_topk<E>(it, S, smem)) }
+    else if constexpr (OP == B_SPLIT) { GTSC_ES_SWITCH(p_split<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_RLE_HEADS) { GTSC_ES_SWITCH(p_rle_heads<E>(it, tile, S)) }
+    else if constexpr (OP == B_RLE_LENGTHS) { p_rle_lengths(it, tile, S); }
+    else if constexpr (OP == B_F2I_STATS) { GTSC_ES_SWITCH(p_f2i_stats<E>(it, tile, S)) }
+    else if constexpr (OP == B_F2I_ENC) { GTSC_ES_SWITCH(p_f2i_enc<E>(it, tile, S)) }
+    else if constexpr (OP == B_F2I_RAW) { GTSC_ES_SWITCH(p_f2i_raw<E>(it, tile, S)) }
+    else if constexpr (OP == B_GFC_COMPRESS) {
+        if (it.es == 8) p_gfc_compress<true>(it, tile, S);
+        else p_gfc_compress<false>(it, tile, S);
+    } else if constexpr (OP == B_GFC_SCAN) {
+        p_gfc_scan(it, tile, S, it.es == 8, it.mode != 0);
+    } else if constexpr (OP == B_GFC_COMPACT) {
+        if (it.es == 8) p_gfc_compact<true>(it, tile, S);
+        else p_gfc_compact<false>(it, tile, S);
+    }
+#undef GTSC_ES_SWITCH
+}
+
+}  // namespace
+
+void launch_batch_decode_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,
+                               uint32_t *d_counter, uint32_t *d_status, cudaStream_t s);
+
+void launch_batch_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,
+                        uint32_t *d_counter, uint32_t *d_status, cudaStream_t s)
+{
+    if (n_items == 0 || total_tiles == 0) return;
+    if (total_tiles > 0x7fffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles in one stage");
+    const unsigned g = (unsigned)total_tiles;
+    switch (op) {
+#define GTSC_STAGE(OPC) \
+    case OPC: k_bstage<OPC><<<g, kBThreads, 0, s>>>(d_items, n_items, d_streams, d_counter, d_status); break;
+        GTSC_STAGE(B_MINMAX)
+        GTSC_STAGE(B_DELTA_ENC)
+        GTSC_STAGE(B_SCALE_SUB)
+        GTSC_STAGE(B_AFL_PACK)
+        GTSC_STAGE(B_HIST)
+        GTSC_STAGE(B_TOPK)
+        GTSC_STAGE(B_SPLIT)
+        GTSC_STAGE(B_RLE_HEADS)
+        GTSC_STAGE(B_RLE_LENGTHS)
+        GTSC_STAGE(B_F2I_STATS)
+        GTSC_STAGE(B_F2I_ENC)
+        GTSC_STAGE(B_F2I_RAW)
+        GTSC_STAGE(B_GFC_COMPRESS)
+        GTSC_STAGE(B_GFC_SCAN)
+        GTSC_STAGE(B_GFC_COMPACT)
+#undef GTSC_STAGE
+    default:
+        launch_batch_decode_stage(op, d_items, n_items, total_tiles, d_streams, d_counter, d_status, s);
+        return;
+    }
+    GTSC_CUDA(cudaGetLastError());
+}
+
+}  // namespace gtsc

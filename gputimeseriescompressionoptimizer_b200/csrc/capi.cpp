@@ -3,6 +3,7 @@
 #include "common.cuh"
 #include "encodings.hpp"
 #include "kernels.hpp"
+#include "batch.hpp"
 #include "planner.hpp"
 #include "tree.hpp"
 
@@ -84,6 +85,23 @@ gtsc_status gtsc_memcpy(void *dst, const void *src, uint64_t bytes, int32_t kind
 gtsc_status gtsc_stream_synchronize(void *stream)
 {
     return guard([&] { GTSC_CUDA(cudaStreamSynchronize(S(stream))); });
+}
+
+gtsc_status gtsc_stream_create(void **stream)
+{
+    return guard([&] {
+        if (!stream) fail(GTSC_ERR_ARG, "null argument");
+        cudaStream_t s;
+        GTSC_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        *stream = (void *)s;
+    });
+}
+
+gtsc_status gtsc_stream_destroy(void *stream)
+{
+    return guard([&] {
+        if (stream) GTSC_CUDA(cudaStreamDestroy(S(stream)));
+    });
 }
 
 gtsc_status gtsc_encode(int32_t encoding, int32_t dtype, const void *d_in, uint64_t in_bytes,
@@ -195,6 +213,95 @@ gtsc_status gtsc_optimize_tree(int32_t dtype, const void *d_in, uint64_t in_byte
 }
 
 uint64_t gtsc_sample_bytes(int32_t dtype, uint64_t in_bytes) { return sample_bytes(dtype, in_bytes); }
+
+struct gtsc_batch {
+    BatchEngine *e;
+    uint32_t n_cols;
+};
+
+gtsc_status gtsc_batch_create(const gtsc_column *cols, uint32_t n_cols, const int16_t *nodes,
+                              const int32_t *node_counts, gtsc_batch **out, void *stream)
+{
+    return guard([&] {
+        if (!cols || !nodes || !node_counts || !out || !n_cols) fail(GTSC_ERR_ARG, "null argument");
+        std::vector<BatchColumn> c;
+        std::vector<Tree> t;
+        const int16_t *p = nodes;
+        for (uint32_t i = 0; i < n_cols; i++) {
+            c.push_back(BatchColumn{cols[i].d_data, cols[i].bytes, cols[i].dtype});
+            t.push_back(tree_from_nodes(p, node_counts[i]));
+            p += 2 * node_counts[i];
+        }
+        BatchEngine *e = batch_create(c, t, S(stream));
+        *out = new gtsc_batch{e, n_cols};
+    });
+}
+
+gtsc_status gtsc_batch_set_inputs(gtsc_batch *b, const void *const *d_inputs, void *stream)
+{
+    return guard([&] {
+        if (!b || !d_inputs) fail(GTSC_ERR_ARG, "null argument");
+        batch_set_inputs(b->e, std::vector<const void *>(d_inputs, d_inputs + b->n_cols), S(stream));
+    });
+}
+
+gtsc_status gtsc_batch_compress(gtsc_batch *b, void *stream)
+{
+    return guard([&] {
+        if (!b) fail(GTSC_ERR_ARG, "null batch");
+        batch_compress(b->e, S(stream));
+    });
+}
+
+gtsc_status gtsc_batch_output(gtsc_batch *b, const void **d_framed, uint64_t *bytes, void *stream)
+{
+    return guard([&] {
+        if (!b || !d_framed || !bytes) fail(GTSC_ERR_ARG, "null argument");
+        *bytes = batch_output_bytes(b->e, S(stream));
+        *d_framed = batch_output(b->e);
+    });
+}
+
+gtsc_status gtsc_batch_blob_sizes(gtsc_batch *b, uint64_t *sizes, void *stream)
+{
+    return guard([&] {
+        if (!b || !sizes) fail(GTSC_ERR_ARG, "null argument");
+        std::vector<uint64_t> v = batch_blob_sizes(b->e, S(stream));
+        std::memcpy(sizes, v.data(), 8 * v.size());
+    });
+}
+
+gtsc_status gtsc_batch_decompress(gtsc_batch *b, const void *d_framed, uint64_t framed_bytes,
+                                  void *const *d_outputs, void *stream)
+{
+    return guard([&] {
+        if (!b || !d_framed || !d_outputs) fail(GTSC_ERR_ARG, "null argument");
+        batch_decompress(b->e, (const uint8_t *)d_framed, framed_bytes,
+                         std::vector<void *>(d_outputs, d_outputs + b->n_cols), S(stream));
+    });
+}
+
+gtsc_status gtsc_batch_status(gtsc_batch *b, void *stream)
+{
+    gtsc_status st = GTSC_OK;
+    gtsc_status g = guard([&] {
+        if (!b) fail(GTSC_ERR_ARG, "null batch");
+        st = batch_status(b->e, S(stream));
+        if (st) set_last_error("batch: a device-side check failed in a step");
+    });
+    return g ? g : st;
+}
+
+int32_t gtsc_batch_launches(gtsc_batch *b, int32_t compress) { return b ? batch_launches(b->e, compress != 0) : 0; }
+
+gtsc_status gtsc_batch_destroy(gtsc_batch *b)
+{
+    return guard([&] {
+        if (!b) return;
+        batch_destroy(b->e);
+        delete b;
+    });
+}
 
 gtsc_status gtsc_afl_compress_gpu(int32_t dtype, uint32_t bit_length, const void *d_data, uint64_t n,
                                   void *d_out, uint64_t out_bytes, void *stream)

@@ -27,14 +27,14 @@ struct Lookback {
 };
 
 // bytes of scratch for `tiles` tiles; layout: counter, error, pad, flags[tiles], agg[tiles], pre[tiles]
-inline uint64_t lookback_bytes(uint64_t tiles)
+__host__ __device__ inline uint64_t lookback_bytes(uint64_t tiles)
 {
     return 16 + ((4 * tiles + 15) & ~15ull) + 16 * tiles;
 }
 // bytes that must be zeroed before each launch (counter, error and the flags)
-inline uint64_t lookback_zero_bytes(uint64_t tiles) { return 16 + 4 * tiles; }
+__host__ __device__ inline uint64_t lookback_zero_bytes(uint64_t tiles) { return 16 + 4 * tiles; }
 
-inline Lookback lookback_at(uint8_t *scratch, uint64_t tiles)
+__host__ __device__ inline Lookback lookback_at(uint8_t *scratch, uint64_t tiles)
 {
     Lookback l;
     l.counter = (uint32_t *)scratch;

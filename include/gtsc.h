@@ -62,6 +62,9 @@ gtsc_status gtsc_free(void *d_ptr, void *stream);
 /* Copies; `kind` 1 = host->device, 2 = device->host, 3 = device->device (cudaMemcpyKind). */
 gtsc_status gtsc_memcpy(void *dst, const void *src, uint64_t bytes, int32_t kind, void *stream);
 gtsc_status gtsc_stream_synchronize(void *stream);
+/* A non-blocking CUDA stream (the batched steps need one they can capture on). */
+gtsc_status gtsc_stream_create(void **stream);
+gtsc_status gtsc_stream_destroy(void *stream);
 
 /* ------------------------------------------------------------------ encodings */
 
@@ -139,6 +142,47 @@ gtsc_status gtsc_optimize_tree(int32_t dtype, const void *d_in, uint64_t in_byte
 
 /* GetSampleDataForFullUpdateSize (optimizer/compression_optimizer.cpp:148-154). */
 uint64_t gtsc_sample_bytes(int32_t dtype, uint64_t in_bytes);
+
+/* ------------------------------------------------------------------ batched columns */
+
+/*
+ * Compresses many columns, each with its own tree, in a fixed sequence of batched launches that is
+ * recorded once as a CUDA graph.  It replaces the per-column task loop of the reference
+ * (ParallelTSCompressor::Compress, parallel_ts_compressor.cpp:39-63, one CompressionTask per column,
+ * optimizer/compression_task.cpp:42-77) for columns whose trees are known.  Framed output: uint64
+ * column count C, a directory of C uint64 blob byte counts (the size_t length the reference writes
+ * before each chunk, compression_task.cpp:35-40, gathered in front so decode finds every column at
+ * once), then the C blobs of CompressionTree::Compress back to back.  All column and output
+ * pointers must be 16-byte aligned.
+ */
+typedef struct gtsc_batch gtsc_batch;
+typedef struct {
+    const void *d_data;   /* device column */
+    uint64_t bytes;
+    int32_t dtype;
+    int32_t reserved;
+} gtsc_column;
+
+/* nodes: the columns' node lists concatenated; node_counts[c] = nodes of column c.  stream must
+ * not be the legacy default stream (steps are captured on it). */
+gtsc_status gtsc_batch_create(const gtsc_column *cols, uint32_t n_cols, const int16_t *nodes,
+                              const int32_t *node_counts, gtsc_batch **out, void *stream);
+/* new device pointers for the columns (same sizes), used by the next compress */
+gtsc_status gtsc_batch_set_inputs(gtsc_batch *b, const void *const *d_inputs, void *stream);
+/* one compress step (asynchronous): framed output in the batch's device buffer */
+gtsc_status gtsc_batch_compress(gtsc_batch *b, void *stream);
+/* the framed output of the last compress and its byte count (synchronises) */
+gtsc_status gtsc_batch_output(gtsc_batch *b, const void **d_framed, uint64_t *bytes, void *stream);
+/* blob bytes of every column in the last compress (synchronises) */
+gtsc_status gtsc_batch_blob_sizes(gtsc_batch *b, uint64_t *sizes, void *stream);
+/* one decompress step (asynchronous) of a framed buffer made by any compress step of this batch */
+gtsc_status gtsc_batch_decompress(gtsc_batch *b, const void *d_framed, uint64_t framed_bytes,
+                                  void *const *d_outputs, void *stream);
+/* status of the steps run so far (synchronises): a device-side format, capacity or timeout error */
+gtsc_status gtsc_batch_status(gtsc_batch *b, void *stream);
+/* kernel launches in one step (compress != 0: compress step) */
+int32_t gtsc_batch_launches(gtsc_batch *b, int32_t compress);
+gtsc_status gtsc_batch_destroy(gtsc_batch *b);
 
 /* ------------------------------------------------------------------ kernel-level entry points */
 

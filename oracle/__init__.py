@@ -117,8 +117,7 @@ def encode(enc, dtype, data):
     """Encoding::Encode -> list of byte arrays [metadata, out1, (out2)]."""
     src = as_bytes(data)
     n = src.size
-    cap = 4 * n + n // 2 + 1 << 0
-    cap = 4 * n + 65536
+    cap = 5 * n + 65536  # RLE of 1-byte values: 4 bytes of run length per value
     outs = [np.zeros(cap, np.uint8) for _ in range(3)]
     ob = (ctypes.c_uint64 * 3)()
     n_out = ctypes.c_int(0)

@@ -776,6 +776,7 @@ static uint64_t worst_case(int enc, int dt, uint64_t in_bytes)
     switch (enc) {
     case OR_GFC: return in_bytes + n / 2 + 4096 + 4 * ((n + 32767) / 32768 + 1) * 32;
     case OR_UNIQUE: return 16 + in_bytes + 4 * n + 64;
+    case OR_RLE: return 4 * n + in_bytes + 64;
     default: return 2 * in_bytes + n / 8 + 64;
     }
 }

@@ -28,7 +28,8 @@ static int ret_type(int enc, int dt, int j)
     return dt;
 }
 
-static uint64_t enc_cap(uint64_t in_bytes) { return 3 * in_bytes + in_bytes / 2 + 8192; }
+/* room for any encoding's outputs: RLE of 1-byte values writes 4 bytes of run length per value */
+static uint64_t enc_cap(uint64_t in_bytes) { return 5 * in_bytes + 8192; }
 
 /* ---------------------------------------------------------------- path -> tree ------------ */
 

@@ -1,0 +1,178 @@
+"""The batched multi-column engine against the per-column path and the oracle: every column's blob
+in the framed output is byte-identical to CompressionTree::Compress of that column alone
+(tree/compression_tree.cpp), decompression is bit-exact, and replayed steps (CUDA graphs) give
+the same bytes.  The reference has no batched path; its per-column tests
+(compression_tree_unittest.cpp, optimizer_unittest.cpp) are the model for the cases."""
+import numpy as np
+import pytest
+
+import oracle as OR
+from gputimeseriescompressionoptimizer_b200 import workloads as W
+from test_tree_gpu import PATHS, TREES, pattern_a, pattern_b, ts_like
+
+pytestmark = pytest.mark.gpu
+
+
+def gen(rng, kind, dt, n):
+    npt = OR.NP_TYPES[dt]
+    if kind == "int":
+        return rng.integers(-1000, 1000, n).astype(npt)
+    if kind == "ts":
+        return ts_like(rng, n).astype(npt)
+    if kind == "a":
+        return pattern_a(rng, n, npt)
+    if kind == "b":
+        return pattern_b(rng, n).astype(npt)
+    return np.round(rng.normal(0, 100, n), 3).astype(npt)
+
+
+def framed_blobs(G, b):
+    p, nb = b.output()
+    framed = G.to_host(G.DeviceBuffer(p, nb, owned=False))
+    return p, nb, framed, G.split_framed(framed)
+
+
+def run_batch(G, O, cols, dtypes, trees, steps=1):
+    st = G.Stream()
+    devs = [G.to_device(x) for x in cols]
+    b = G.Batch(devs, dtypes, trees, st)
+    assert b.launches(True) > 0 and b.launches(False) > 0
+    first = None
+    for _ in range(steps):
+        b.compress()
+        b.status()
+        p, nb, framed, blobs = framed_blobs(G, b)
+        if first is None:
+            first = framed
+        else:
+            assert np.array_equal(framed, first)  # a replayed step writes the same bytes
+    assert len(blobs) == len(cols)
+    sizes = b.blob_sizes()
+    for i, (x, t) in enumerate(zip(cols, trees)):
+        ob = O.tree_compress(t, x)
+        assert sizes[i] == blobs[i].size == ob.size, (i, G.tree_names(t), x.dtype, x.size)
+        assert np.array_equal(blobs[i], ob), (i, G.tree_names(t), x.dtype, x.size)
+    for _ in range(steps):
+        outs = [G.alloc(x.nbytes) for x in cols]
+        b.decompress(p, nb, outs)
+        b.status()
+        for i, x in enumerate(cols):
+            assert G.to_host(outs[i]).tobytes() == x.tobytes(), (i, G.tree_names(trees[i]), x.dtype, x.size)
+    return b, st, devs
+
+
+def test_batch_reference_tree_shapes(G, O, rng):
+    cols, dts, trees = [], [], []
+    for path, dt, kind in TREES:
+        for n in [10, 1000, 10000]:
+            cols.append(gen(rng, kind, dt, n))
+            dts.append(dt)
+            trees.append(G.tree_from_path(path, dt))
+    run_batch(G, O, cols, dts, trees, steps=2)
+
+
+def test_batch_generated_paths(G, O, rng):
+    cols, dts, trees = [], [], []
+    for path in PATHS:
+        cols.append(ts_like(rng, 20000))
+        dts.append(OR.INT)
+        trees.append(G.tree_from_path(path, OR.INT))
+    run_batch(G, O, cols, dts, trees)
+
+
+SINGLE = [[OR.AFL, OR.NONE], [OR.DELTA, OR.NONE], [OR.SCALE, OR.NONE], [OR.RLE, OR.NONE, OR.NONE],
+          [OR.DICT, OR.NONE, OR.NONE], [OR.CONST, OR.NONE], [OR.PATCH, OR.NONE, OR.NONE],
+          [OR.NONE], [OR.GFC, OR.NONE, OR.NONE]]
+
+
+@pytest.mark.parametrize("dt", [OR.CHAR, OR.SHORT, OR.INT, OR.TIME, OR.FLOAT, OR.DOUBLE],
+                         ids=["char", "short", "int", "time", "float", "double"])
+def test_batch_single_encodings_all_types(G, O, rng, dt):
+    """each encoding alone on tiny, ragged and multi-tile columns of every data type"""
+    cols, dts, trees = [], [], []
+    for path in SINGLE + [[OR.FLOAT2INT, OR.AFL, OR.NONE]]:
+        if path[0] == OR.FLOAT2INT and dt not in (OR.FLOAT, OR.DOUBLE):
+            continue
+        if path[0] == OR.AFL and dt in (OR.FLOAT, OR.DOUBLE):
+            continue  # the float split of AflEncoding (afl_encoding.cu:116-170) is not in this tree path
+        for n in [1, 2, 31, 33, 2047, 2049, 70001]:
+            for kind in ["int", "a", "b"]:
+                x = gen(rng, kind, dt, n)
+                cols.append(x)
+                dts.append(dt)
+                trees.append(G.tree_from_path(path, dt))
+    run_batch(G, O, cols, dts, trees)
+
+
+def test_batch_generators_with_planned_trees(G, O, rng):
+    """the mixed workload's generators (NaN payloads, +-inf, -0.0 in float prices) with the trees the
+    exhaustive planner picks on each column's sample"""
+    cols, dts, trees = [], [], []
+    seed = 11
+    for kind in W.KINDS:
+        for dt in [OR.INT, OR.FLOAT, OR.DOUBLE, OR.TIME, OR.SHORT]:
+            for n in [4096, 50000, 300001]:
+                x = W.column(kind, dt, n, seed)
+                seed += 1
+                dev = G.to_device(x)
+                sb = G.sample_bytes(dt, x.nbytes)
+                nodes, _ = G.plan_exhaustive(dt, G.to_device(x.view(np.uint8)[:sb].view(x.dtype)))
+                cols.append(x)
+                dts.append(dt)
+                trees.append(nodes)
+                del dev
+    run_batch(G, O, cols, dts, trees, steps=2)
+
+
+def test_batch_set_inputs_and_decompress_from_copy(G, O, rng):
+    trees = [G.tree_from_path(p, OR.INT) for p in PATHS[:8]]
+    cols = [ts_like(rng, 5000 + 777 * i) for i in range(8)]
+    b, st, devs = run_batch(G, O, cols, [OR.INT] * 8, trees)
+    # new columns of the same sizes through the same graphs
+    cols2 = [pattern_b(rng, x.size) for x in cols]
+    devs2 = [G.to_device(x) for x in cols2]
+    b.set_inputs(devs2)
+    b.compress()
+    b.status()
+    p, nb, framed, blobs = framed_blobs(G, b)
+    for i, x in enumerate(cols2):
+        assert np.array_equal(blobs[i], O.tree_compress(trees[i], x))
+    # decompress a copy of the framed buffer at another address
+    copy = G.to_device(framed)
+    outs = [G.alloc(x.nbytes) for x in cols2]
+    b.decompress(copy.ptr, copy.nbytes, outs)
+    b.status()
+    for i, x in enumerate(cols2):
+        assert G.to_host(outs[i]).tobytes() == x.tobytes()
+
+
+def test_batch_corrupt_frames_fail_cleanly(G, O, rng):
+    trees = [G.tree_from_path([OR.DELTA, OR.PATCH, OR.AFL, OR.NONE, OR.AFL, OR.NONE], OR.INT),
+             G.tree_from_path([OR.DICT, OR.AFL, OR.NONE, OR.NONE], OR.INT)]
+    cols = [ts_like(rng, 5000), pattern_b(rng, 3000)]
+    b, st, devs = run_batch(G, O, cols, [OR.INT] * 2, trees)
+    p, nb, framed, blobs = framed_blobs(G, b)
+    outs = [G.alloc(x.nbytes) for x in cols]
+    for cut in [5, 20, nb // 2, nb - 1]:
+        bad = G.to_device(framed[:cut])
+        b.decompress(bad.ptr, bad.nbytes, outs)
+        with pytest.raises(G.GtscError):
+            b.status()
+    bad = framed.copy()
+    bad[8 + 8 * len(cols)] = 99  # unknown encoding type in the first node header
+    d = G.to_device(bad)
+    b.decompress(d.ptr, d.nbytes, outs)
+    with pytest.raises(G.GtscError):
+        b.status()
+    bad = framed.copy()
+    bad[0] = 3  # wrong column count
+    d = G.to_device(bad)
+    b.decompress(d.ptr, d.nbytes, outs)
+    with pytest.raises(G.GtscError):
+        b.status()
+    # the engine still works after the errors
+    good = G.to_device(framed)
+    b.decompress(good.ptr, good.nbytes, outs)
+    b.status()
+    for i, x in enumerate(cols):
+        assert G.to_host(outs[i]).tobytes() == x.tobytes()
