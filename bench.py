@@ -1,15 +1,23 @@
 #!/usr/bin/env python
-"""Benchmark of the column-compression hot path on B200.
+"""Benchmark of the column-compression hot path on B200: the batched mixed workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One step = compress + decompress of one batch of synthetic input resident in HBM.  Prints one JSON
-line (rank 0).  N > 1 runs N independent replicas (one process per GPU, launched by torchrun): the
-path has no exchange step, so `value` is the work of all ranks over the slowest rank's time.
+Workload: 512 synthetic columns (lengths log-uniform in [4096, 2^24], int32 : float32 : float64 =
+2 : 1 : 1, generators walk / runs / zipf / const / outliers / price chosen by seed), each with the
+compression tree the planner picks on its sample.  One step = compress all 512 columns into one
+framed buffer and decompress it again, with the columns resident in HBM; `value` is uncompressed
+GB/s.  Beside it: the plain path (one column at a time through gtsc_tree_compress /
+gtsc_tree_decompress, host-synchronising as the reference's per-column calls do), the planners'
+cost, the dominant kernel against the HBM roofline, an end-to-end step from pinned host memory,
+and the CPU oracle on a bounded sample.
+
+N > 1 runs N independent replicas (one process per GPU, launched by torchrun): the columns are
+independent and the path has no exchange step, so `value` is the work of all ranks over the
+slowest rank's time.
 """
 import argparse
 import concurrent.futures as cf
-import ctypes
 import json
 import os
 import statistics
@@ -25,11 +33,12 @@ sys.path.insert(0, ROOT)
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
-
-# workload: AFL fixed-width packing of one int32 column, U[0, 2^11), 11 bits per value
-AFL_N = 1 << int(os.environ.get("GTSC_BENCH_AFL_LOG2N", "28"))
-AFL_BITS = 11
-AFL_SEED = 0xB200
+N_COLUMNS = int(os.environ.get("GTSC_BENCH_COLUMNS", "512"))
+MAX_LEN = 1 << int(os.environ.get("GTSC_BENCH_MAX_LOG2", "24"))
+CPU_SAMPLE_LEN = 1 << 18     # CPU legs: every column cut to its first 2^18 values
+METRIC = "batched mixed-workload compress+decompress throughput (uncompressed GB/s)"
+WORKLOAD = (f"mixed {N_COLUMNS} columns, lengths log-uniform [4096, {MAX_LEN}], int32:float32:float64 = 2:1:1, "
+            "generators walk/runs/zipf/const/outliers/price, seed 0xB204")
 
 
 def parse():
@@ -93,82 +102,102 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def dist_setup(args):
+def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
 
 
-def gen_afl_column(n):
-    rng = np.random.default_rng(AFL_SEED)
-    x = rng.integers(0, 1 << AFL_BITS, n, dtype=np.int32)
-    x[0] = (1 << AFL_BITS) - 1
-    return x
+def workload_specs():
+    from gputimeseriescompressionoptimizer_b200 import workloads as W
+    return W.mixed_columns(N_COLUMNS, max_len=MAX_LEN)
+
+
+def gen_columns(specs, max_len=None, threads=None):
+    """The columns of `specs` as numpy arrays (each cut to max_len values when given)."""
+    from gputimeseriescompressionoptimizer_b200 import workloads as W
+
+    def one(s):
+        kind, dt, n, seed = s
+        return W.column(kind, dt, n if max_len is None else min(n, max_len), seed)
+
+    with cf.ThreadPoolExecutor(threads or os.cpu_count() or 1) as ex:
+        return list(ex.map(one, specs))
 
 
 # ------------------------------------------------------------------------------- CPU legs
-def cpu_afl_reference(x, threads):
-    """The reference's own AFL host path (oracle/_ref, run_afl_compress_cpu / decompress) over
-    chunks of 2^16 values split across threads; returns (seconds, bytes)."""
+def cpu_roundtrip(cols, trees, threads):
+    """The oracle's CompressionTree::Compress + Decompress of every column (one task per column,
+    `threads` host threads; ctypes releases the GIL).  Returns (seconds, input bytes, blob bytes)."""
     import oracle
-    oracle.build_ref()
-    R = oracle.ref()
-    if R is None:
-        raise RuntimeError("oracle/_ref not built")
-    comp = R.ref_afl_compress_int
-    comp.argtypes = [ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulong, ctypes.c_ulong]
-    dec = R.ref_afl_decompress_int
-    dec.argtypes = [ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulong]
-    chunk = 1 << 16
-    words = chunk * AFL_BITS // 32
-    packed = np.zeros(x.size * AFL_BITS // 32 + 64, np.int32)
-    out = np.zeros_like(x)
 
-    def work(c):
-        lo = c * chunk
-        cnt = min(chunk, x.size - lo)
-        w0 = lo * AFL_BITS // 32
-        cw = (cnt * AFL_BITS + 31) // 32
-        comp(AFL_BITS, x.ctypes.data + 4 * lo, packed.ctypes.data + 4 * w0, cnt, cw)
-        dec(AFL_BITS, packed.ctypes.data + 4 * w0, out.ctypes.data + 4 * lo, cnt)
+    def work(i):
+        blob = oracle.tree_compress(trees[i], cols[i])
+        out, _ = oracle.tree_decompress(blob, cols[i].nbytes)
+        return blob.size, out.size
 
-    nchunks = (x.size + chunk - 1) // chunk
     t = time.perf_counter()
     with cf.ThreadPoolExecutor(threads) as ex:
-        list(ex.map(work, range(nchunks)))
+        res = list(ex.map(work, range(len(cols))))
     dt = time.perf_counter() - t
-    assert np.array_equal(out, x), "reference AFL round trip failed"
-    del words
-    return dt, x.nbytes
+    assert all(o == c.nbytes for (_, o), c in zip(res, cols))
+    return dt, sum(c.nbytes for c in cols), sum(b for b, _ in res)
+
+
+def cpu_trees(cols, specs):
+    """The oracle's exhaustive planner on each column's sample."""
+    import oracle
+    trees = []
+    for x, (_, dt, _, _) in zip(cols, specs):
+        sb = oracle.sample_bytes(dt, x.nbytes)
+        nodes, _ = oracle.plan_exhaustive(dt, x.view(np.uint8)[:sb].view(x.dtype))
+        trees.append(nodes)
+    return trees
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU implementation of the path (the oracle restatement: no part of the
+    reference's own tree code compiles here), all host threads, on a bounded sample per step."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    n = 1 << 25
-    x = gen_afl_column(n)
+    specs = workload_specs()
+    cols = gen_columns(specs, CPU_SAMPLE_LEN)
+    trees = cpu_trees(cols, specs)
     for _ in range(max(args.warmup, 1)):
-        cpu_afl_reference(x, threads)
-    times = [cpu_afl_reference(x, threads)[0] for _ in range(args.steps)]
+        cpu_roundtrip(cols, trees, threads)
+    times = []
+    for _ in range(args.steps):
+        t, in_bytes, blob_bytes = cpu_roundtrip(cols, trees, threads)
+        times.append(t)
     t = sum(times) / len(times)
-    gbs = x.nbytes / t / 1e9
+    gbs = in_bytes / t / 1e9
+    sample = f"all {len(cols)} columns cut to their first 2^18 values ({in_bytes} B), trees planned on them"
     line = {
-        "impl": "reference", "metric": "AFL compress+decompress throughput (uncompressed GB/s)",
-        "value": round(gbs, 4), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(1e3 * t, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": f"afl int32 U[0,2^{AFL_BITS}) b={AFL_BITS}, CPU sample 2^25 of the 2^28-value column",
-                   "inputs": "host memory"},
-        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "reference",
-                         "sample": "2^25 int32 values per step"},
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32/float32/float64 (integer arithmetic on bits)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "inputs": "host memory",
+                   "step": "CompressionTree::Compress + Decompress of every column (CPU restatement)",
+                   "compression_ratio": round(in_bytes / blob_bytes, 4)},
+        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------------------- GPU leg
+class DevView:
+    """(ptr, nbytes) of a torch tensor, the shape the package's calls take."""
+
+    def __init__(self, t):
+        self.t = t
+        self.ptr = t.data_ptr()
+        self.nbytes = t.numel() * t.element_size()
+
+
 def run_ours(args, world, rank, local):
     import torch
     import gputimeseriescompressionoptimizer_b200 as g
@@ -177,32 +206,68 @@ def run_ours(args, world, rank, local):
     dist = None
     if world > 1:
         import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
-    stream = torch.cuda.current_stream()
-    sp = stream.cuda_stream
+        from datetime import timedelta
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local), timeout=timedelta(seconds=600))
     L = g.lib()
+    st = g.Stream()
+    stream = torch.cuda.ExternalStream(st.handle)
+    sp = st.handle
 
-    n = AFL_N
-    x = gen_afl_column(n)
-    host_in = torch.from_numpy(x).pin_memory()
-    host_out = torch.empty(n, dtype=torch.int32).pin_memory()
-    dev_in = torch.empty(n, dtype=torch.int32, device="cuda")
-    dev_in.copy_(host_in)
+    specs = workload_specs()
+    t0 = time.perf_counter()
+    cols = gen_columns(specs)
+    t_gen = time.perf_counter() - t0
+    dts = [dt for _, dt, _, _ in specs]
+    in_bytes = sum(c.nbytes for c in cols)
+    host = [torch.from_numpy(c.view(np.uint8)).pin_memory() for c in cols]
+    dev = [torch.empty(c.nbytes, dtype=torch.uint8, device="cuda") for c in cols]
+    for d, h in zip(dev, host):
+        d.copy_(h)
     torch.cuda.synchronize()
-    col = g.DeviceBuffer(dev_in.data_ptr(), dev_in.numel() * 4, owned=False)
+    dv = [DevView(d) for d in dev]
+
+    # plain exhaustive planner on every column's sample (the reference's CompressData full update)
+    t0 = time.perf_counter()
+    trees = []
+    for d, dt in zip(dv, dts):
+        sb = g.sample_bytes(dt, d.nbytes)
+        nodes, _ = g.plan_exhaustive(dt, g.DeviceBuffer(d.ptr, sb, owned=False), sp)
+        trees.append(nodes)
+    torch.cuda.synchronize()
+    t_plan_exh = time.perf_counter() - t0
+
+    t0 = time.perf_counter()
+    batch = g.Batch(dv, dts, trees, st)
+    t_create = time.perf_counter() - t0
+    outs = [torch.empty_like(d) for d in dev]
+    ov = [DevView(o) for o in outs]
+
+    def compress():
+        batch.compress()
+
+    framed = {}
+
+    def decompress():
+        batch.decompress(framed["p"], framed["n"], ov)
 
     def step():
-        parts = g.encode(g.AFL, g.INT, col, sp)
-        out = g.decode(g.AFL, g.INT, parts, sp)
-        return parts, out
+        compress()
+        decompress()
 
-    # correctness of one step before timing
-    parts, out = step()
-    back = torch.empty(n, dtype=torch.int32, device="cuda")
-    g.check(L.gtsc_memcpy(back.data_ptr(), out.ptr, out.nbytes, 3, sp), "copy")
-    assert torch.equal(back, dev_in), "round trip failed"
-    comp_bytes = sum(p.nbytes for p in parts)
-    del back
+    # parity at full size: the batched blobs against the plain per-column path, and the round trip
+    compress()
+    batch.status()
+    framed["p"], framed["n"] = batch.output()
+    decompress()
+    batch.status()
+    framed_host = g.to_host(g.DeviceBuffer(framed["p"], framed["n"], owned=False))
+    blobs = g.split_framed(framed_host)
+    blob_bytes = sum(b.size for b in blobs)
+    for i in range(len(cols)):
+        pb = g.tree_compress(trees[i], g.DeviceBuffer(dv[i].ptr, dv[i].nbytes, owned=False), sp)
+        assert np.array_equal(g.to_host(pb, stream=sp), blobs[i]), f"column {i}: batched blob differs"
+        assert torch.equal(outs[i], dev[i]), f"column {i}: round trip differs"
+    del framed_host
 
     def barrier():
         torch.cuda.synchronize()
@@ -229,69 +294,97 @@ def run_ours(args, world, rank, local):
     clocks = ClockSampler(local)
     clocks.start()
     t_step = timed(step, args.steps)
+    t_comp = timed(compress, args.steps)
+    t_dec = timed(decompress, args.steps)
+    batch.status()
 
-    # dominant kernel alone: the AFL pack (2 launches of our kernels per step: minmax + pack,
-    # plus the unpack)
-    data_part = parts[1]
-    pack = lambda: g.check(L.gtsc_afl_compress_gpu(g.INT, AFL_BITS, col.ptr, n, data_part.ptr,
-                                                   data_part.nbytes, sp), "pack")
-    unpack = lambda: g.check(L.gtsc_afl_decompress_gpu(g.INT, AFL_BITS, data_part.ptr, data_part.nbytes,
-                                                       out.ptr, n, sp), "unpack")
-    for _ in range(3):
-        pack()
-        unpack()
-    t_pack = timed(pack, args.steps)
-    t_unpack = timed(unpack, args.steps)
+    # the plain path: one column at a time, planner excluded (trees as above)
+    def plain():
+        for i in range(len(cols)):
+            blob = g.tree_compress(trees[i], g.DeviceBuffer(dv[i].ptr, dv[i].nbytes, owned=False), sp)
+            g.tree_decompress(blob, sp)
 
-    # end to end through the public API: pinned host column in, decoded column back to the host
+    plain()
+    t_plain = timed(plain, 1)
+
+    # end to end through the public API: pinned host columns in, framed output back to the host
+    host_framed = torch.empty(framed["n"] + 4096, dtype=torch.uint8).pin_memory()
+
     def e2e_step():
-        dev_in.copy_(host_in, non_blocking=True)
-        p, o = step()
-        tmp = torch.empty(0)
-        g.check(L.gtsc_memcpy(host_out.data_ptr(), o.ptr, o.nbytes, 2, sp), "d2h")
-        return tmp
+        for d, h in zip(dv, host):
+            g.check(L.gtsc_memcpy(d.ptr, h.data_ptr(), d.nbytes, 1, sp), "h2d")
+        batch.compress()
+        p, n = batch.output()
+        g.check(L.gtsc_memcpy(host_framed.data_ptr(), p, n, 2, sp), "d2h")
+        batch.decompress(p, n, ov)
+        batch.status()
+        e2e_step.d2h = n + 4
 
-    for _ in range(2):
-        e2e_step()
+    e2e_step()
     t_e2e = timed(e2e_step, max(2, args.steps // 2))
     clk = clocks.stop()
+
+    # launch-by-launch profile (events between launches, outside the graphs), a few repeats
+    prof = {}
+    for name, comp in (("compress", True), ("decompress", False)):
+        runs = [batch.profile(comp) for _ in range(3)]
+        prof[name] = [(runs[0][j][0], min(r[j][1] for r in runs), runs[0][j][2], runs[0][j][3])
+                      for j in range(len(runs[0]))]
+    batch.status()
 
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return
+
     peak, peak_kind = peak_hbm()
-    in_bytes = n * 4
-    alg_pack = in_bytes + data_part.nbytes
-    achieved = alg_pack / t_pack / 1e9
+    allp = [(phase, *x) for phase, lst in prof.items() for x in lst]
+    top = max(allp, key=lambda r: r[2])
+    t_prof = {k: sum(x[1] for x in v) for k, v in prof.items()}
+    top_ach = top[3] / (top[2] / 1e3) / 1e9 if top[2] > 0 else 0.0
+    alg_step = 2 * (in_bytes + blob_bytes + 8 + 8 * len(cols))
     value = world * in_bytes / t_step / 1e9
 
-    # CPU baseline: the reference's AFL host path on a bounded sample, all host threads
+    # CPU baseline: the oracle on a bounded sample (same trees), all host threads
     threads = os.cpu_count() or 1
-    sample = x[: 1 << 25]
-    cpu_afl_reference(sample, threads)
-    ct = min(cpu_afl_reference(sample, threads)[0] for _ in range(2))
-    cpu_gbs = sample.nbytes / ct / 1e9
+    scols = gen_columns(specs, CPU_SAMPLE_LEN)
+    cpu_roundtrip(scols, trees, threads)
+    ct, cin, _ = min((cpu_roundtrip(scols, trees, threads) for _ in range(2)), key=lambda r: r[0])
+    cpu_gbs = cin / ct / 1e9
 
+    tree_names = {}
+    for t in trees:
+        k = "-".join(g.tree_names(t))
+        tree_names[k] = tree_names.get(k, 0) + 1
     line = {
-        "metric": "AFL compress+decompress throughput (uncompressed GB/s)",
-        "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * t_step, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": f"afl: 2^28 int32 U[0,2^{AFL_BITS}) at b={AFL_BITS} (1 GiB per GPU)",
-                   "inputs": "larger than L2 (1 GiB), no flush needed",
-                   "step": "gtsc_encode(AFL) + gtsc_decode(AFL), device-resident input"},
-        "roofline": {"bound": "hbm", "kernel": "k_afl_pack", "achieved": round(achieved, 1),
-                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "traffic": None, "algorithmic_bytes_per_launch": alg_pack,
-                     "launch_ms": round(1e3 * t_pack, 4),
-                     "unpack_GBps": round((in_bytes + data_part.nbytes) / t_unpack / 1e9, 1)},
-        "cpu_baseline": {"value": round(cpu_gbs, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
-                         "sample": "first 2^25 values of the column, run_afl_compress_cpu + decompress"},
-        "e2e": {"value": round(world * in_bytes / t_e2e / 1e9, 3), "unit": "GB/s",
-                "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": in_bytes},
-        "gpu_launches": 3 * args.steps,
-        "compressed_bytes": comp_bytes,
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * t_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32/float32/float64 (integer arithmetic on bits)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "columns": len(cols), "input_bytes": in_bytes, "blob_bytes": blob_bytes,
+                   "compression_ratio": round(in_bytes / blob_bytes, 4),
+                   "inputs": f"larger than L2 ({in_bytes / 1e9:.2f} GB), no flush needed",
+                   "planner": "plain exhaustive (FullStatisticsUpdate on each column's sample)",
+                   "step": "gtsc_batch_compress + gtsc_batch_decompress (CUDA graphs), device-resident columns",
+                   "compress_ms": round(1e3 * t_comp, 4), "decompress_ms": round(1e3 * t_dec, 4),
+                   "hbm_frac_step": round(alg_step / t_step / 1e9 / peak, 4),
+                   "algorithmic_bytes_per_step": alg_step,
+                   "plain_path_ms": round(1e3 * t_plain, 2),
+                   "speedup_vs_plain": round(t_plain / t_step, 2),
+                   "plan_exhaustive_ms": round(1e3 * t_plan_exh, 1),
+                   "batch_create_ms": round(1e3 * t_create, 1), "generate_s": round(t_gen, 1),
+                   "trees": dict(sorted(tree_names.items(), key=lambda kv: -kv[1]))},
+        "roofline": {"bound": "hbm", "kernel": f"{top[0]}:{top[1]}", "achieved": round(top_ach, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(top_ach / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": top[3], "launch_ms": round(top[2], 4), "blocks": top[4],
+                     "share_of_step": round(top[2] / (t_prof["compress"] + t_prof["decompress"]), 4),
+                     "timing": "CUDA events around each launch of one step replayed launch by launch"},
+        "launches": {k: [[x[0], round(x[1], 4), x[2], x[3]] for x in v] for k, v in prof.items()},
+        "cpu_baseline": {"value": round(cpu_gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"all {len(scols)} columns cut to their first 2^18 values ({cin} B), same trees, "
+                                   "oracle tree compress + decompress"},
+        "e2e": {"value": round(world * in_bytes / t_e2e / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": e2e_step.d2h},
+        "gpu_launches": (batch.launches(True) + batch.launches(False)) * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -301,7 +394,7 @@ def run_ours(args, world, rank, local):
 
 def main():
     args = parse()
-    world, rank, local = dist_setup(args)
+    world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
     else:

@@ -107,6 +107,7 @@ def lib():
         L.gtsc_batch_status.argtypes = [vp, vp]
         L.gtsc_batch_launches.argtypes = [vp, i32]
         L.gtsc_batch_destroy.argtypes = [vp]
+        L.gtsc_batch_profile.argtypes = [vp, i32, i32p, ctypes.POINTER(ctypes.c_float), u64p, u64p, i32, i32p, vp]
         _lib = L
     return _lib
 
@@ -280,6 +281,15 @@ class Stream:
             self.handle = None
 
 
+# pass kinds of the batched engine (batch.hpp BOp) and the fixed kernels of a step
+PASS_NAMES = dict(enumerate(
+    ["minmax", "delta_enc", "scale_sub", "afl_pack", "hist", "topk", "split", "rle_heads", "rle_lengths",
+     "f2i_stats", "f2i_enc", "f2i_raw", "gfc_compress", "gfc_scan", "gfc_compact", "none_copy", "afl_unpack",
+     "delta_dec", "scale_add", "merge", "rle_scan", "rle_expand", "f2i_dec", "gfc_sizes", "gfc_dec"]))
+PASS_NAMES.update({-1: "set_streams", -2: "zero", -3: "frame_sizes", -4: "frame_layout", -5: "frame_copy",
+                   -6: "parse_frames"})
+
+
 class Batch:
     """Many columns with their trees, compressed / decompressed by the batched engine.
 
@@ -332,6 +342,23 @@ class Batch:
 
     def launches(self, compress=True):
         return lib().gtsc_batch_launches(self.handle, 1 if compress else 0)
+
+    def profile(self, compress=True):
+        """One step launch by launch: [(pass name, ms, bytes moved at least, blocks)]."""
+        cap = 4096
+        ops = np.zeros(cap, np.int32)
+        ms = np.zeros(cap, np.float32)
+        by = np.zeros(cap, np.uint64)
+        bl = np.zeros(cap, np.uint64)
+        n = ctypes.c_int32(0)
+        check(lib().gtsc_batch_profile(self.handle, 1 if compress else 0,
+                                       ops.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                       ms.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                       by.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                       bl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), cap, ctypes.byref(n),
+                                       self.stream.handle), "batch_profile")
+        return [(PASS_NAMES.get(int(ops[i]), str(int(ops[i]))), float(ms[i]), int(by[i]), int(bl[i]))
+                for i in range(n.value)]
 
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:

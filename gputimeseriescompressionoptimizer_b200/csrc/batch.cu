@@ -13,6 +13,7 @@
 #include "scan.cuh"
 
 #include <algorithm>
+#include <functional>
 #include <map>
 #include <tuple>
 
@@ -115,8 +116,8 @@ public:
     void plan_passes();
     void layout(cudaStream_t s);
     void capture(cudaStream_t s);
-    void record_compress(cudaStream_t s);
-    void record_decompress(cudaStream_t s);
+    void record_compress(cudaStream_t s, const std::function<void(int)> &mark);
+    void record_decompress(cudaStream_t s, const std::function<void(int)> &mark);
 };
 
 // ---------------------------------------------------------------------------------- compile
@@ -628,29 +629,46 @@ void BatchEngine::layout(cudaStream_t s)
     GTSC_CUDA(cudaStreamSynchronize(s));
 }
 
-void BatchEngine::record_compress(cudaStream_t s)
+// Launch-sequence markers: the stage op, or one of these for the fixed kernels of a step.
+enum : int { M_SET = -1, M_ZERO = -2, M_FRAME_SIZES = -3, M_FRAME_LAYOUT = -4, M_FRAME_COPY = -5, M_PARSE = -6 };
+
+void BatchEngine::record_compress(cudaStream_t s, const std::function<void(int)> &mark)
 {
     const int nc = (int)col_root.size();
     k_set_streams<<<(nc + 127) / 128, 128, 0, s>>>(d_set_vals, d_set_sids, nc, d_streams);
+    GTSC_CUDA(cudaGetLastError());
+    mark(M_SET);
     launch_zero_ranges(d_zero_c, (int)zero_c.size() / 2, s);
+    mark(M_ZERO);
     int ctr = 0;
-    for (auto &L : launch_c)
+    for (auto &L : launch_c) {
         launch_batch_stage(L.op, d_items_c + L.first, L.count, L.tiles, d_streams, d_counters + ctr++, d_status, s);
+        mark(L.op);
+    }
     launch_frame_sizes(d_cols, nc, d_nodes_c, d_streams, d_col_off, d_total, d_framed, s);
+    mark(M_FRAME_SIZES);
     launch_frame_layout(d_cols, nc, d_nodes_c, d_streams, d_col_off, d_framed, s);
+    mark(M_FRAME_LAYOUT);
     launch_frame_copy(d_items_copy, (int)items_copy.size(), copy_tiles, d_nodes_c, d_streams, d_framed, s);
+    mark(M_FRAME_COPY);
 }
 
-void BatchEngine::record_decompress(cudaStream_t s)
+void BatchEngine::record_decompress(cudaStream_t s, const std::function<void(int)> &mark)
 {
     const int nc = (int)col_root.size();
     k_set_streams<<<(nc + 127) / 128, 128, 0, s>>>(d_set_vals + 2 * nc, d_set_sids + nc, nc, d_streams);
+    GTSC_CUDA(cudaGetLastError());
+    mark(M_SET);
     launch_zero_ranges(d_zero_d, (int)zero_d.size() / 2, s);
+    mark(M_ZERO);
     launch_parse_frames(d_cols, nc, d_nodes_d, d_streams, d_col_off_d, (const uint8_t *const *)d_frame_ptr,
                         d_frame_len, d_status, s);
+    mark(M_PARSE);
     int ctr = (int)launch_c.size();
-    for (auto &L : launch_d)
+    for (auto &L : launch_d) {
         launch_batch_stage(L.op, d_items_d + L.first, L.count, L.tiles, d_streams, d_counters + ctr++, d_status, s);
+        mark(L.op);
+    }
 }
 
 void BatchEngine::capture(cudaStream_t s)
@@ -659,8 +677,8 @@ void BatchEngine::capture(cudaStream_t s)
         cudaGraph_t g;
         GTSC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         try {
-            if (which == 0) record_compress(s);
-            else record_decompress(s);
+            if (which == 0) record_compress(s, [](int) {});
+            else record_decompress(s, [](int) {});
         } catch (...) {
             cudaGraph_t junk;
             cudaStreamEndCapture(s, &junk);
@@ -776,6 +794,81 @@ void batch_decompress(BatchEngine *e, const uint8_t *framed, uint64_t framed_byt
     GTSC_CUDA(cudaGraphLaunch(e->graph_d, s));
 }
 
+// Bytes a pass must move at least: its inputs read and its outputs written (from the stream table
+// after the step).  Scratch, look-back state and hash tables are not counted.
+static uint64_t item_bytes(const BItem &it, const std::vector<StreamDesc> &S)
+{
+    auto L = [&](int sid) -> uint64_t { return sid >= 0 ? S[sid].len : 0; };
+    const uint64_t in = L(it.in[0]);
+    switch (it.op) {
+    case B_MINMAX: case B_HIST: case B_F2I_STATS: return in;
+    case B_TOPK: case B_F2I_RAW: case B_GFC_SCAN: return 0;
+    case B_DELTA_ENC: case B_SCALE_SUB: case B_AFL_PACK: case B_F2I_ENC: return in + L(it.out[0]) + L(it.out[1]);
+    case B_SPLIT: return in + L(it.out[0]) + L(it.out[1]) + L(it.out[2]);
+    case B_RLE_HEADS: return in + L(it.out[0]) + L(it.out[2]) + L(it.out[1]);  // values, run starts
+    case B_RLE_LENGTHS: return 2 * L(it.out[1]);
+    case B_GFC_COMPRESS: return in + L(it.out[1]) + L(it.out[2]);
+    case B_GFC_COMPACT: return 2 * L(it.out[2]);
+    case B_NONE_COPY: return 2 * in;
+    case B_AFL_UNPACK: case B_DELTA_DEC: case B_SCALE_ADD: case B_F2I_DEC: return L(it.in[1]) + L(it.out[0]);
+    case B_MERGE: return in + L(it.in[1]) + L(it.in[2]) + L(it.out[0]);
+    case B_RLE_SCAN: return L(it.in[1]);
+    case B_RLE_EXPAND: return L(it.in[2]) + L(it.out[0]);
+    case B_GFC_SIZES: return L(it.in[1]);
+    case B_GFC_DEC: return L(it.in[2]) + L(it.out[0]);
+    default: return 0;
+    }
+}
+
+std::vector<BatchLaunchProfile> batch_profile(BatchEngine *e, bool compress, cudaStream_t s)
+{
+    std::vector<int> marks;
+    std::vector<cudaEvent_t> ev;
+    auto new_event = [&]() {
+        cudaEvent_t x;
+        GTSC_CUDA(cudaEventCreate(&x));
+        ev.push_back(x);
+        return x;
+    };
+    std::vector<BatchLaunchProfile> out;
+    try {
+        GTSC_CUDA(cudaEventRecord(new_event(), s));
+        auto mark = [&](int m) {
+            marks.push_back(m);
+            GTSC_CUDA(cudaEventRecord(new_event(), s));
+        };
+        if (compress) e->record_compress(s, mark);
+        else e->record_decompress(s, mark);
+        GTSC_CUDA(cudaStreamSynchronize(s));
+        std::vector<StreamDesc> S(e->streams.size());
+        d2h(S.data(), e->d_streams, S.size() * sizeof(StreamDesc), s);
+        unsigned long long total = 0;
+        d2h(&total, e->d_total, 8, s);
+        int li = 0;
+        for (size_t k = 0; k < marks.size(); k++) {
+            BatchLaunchProfile p{};
+            p.op = marks[k];
+            GTSC_CUDA(cudaEventElapsedTime(&p.ms, ev[k], ev[k + 1]));
+            if (marks[k] >= 0) {
+                const Launch &L = compress ? e->launch_c[li] : e->launch_d[li];
+                const BItem *items = compress ? &e->items_c[L.first] : &e->items_d[L.first];
+                for (int j = 0; j < L.count; j++) p.bytes += item_bytes(items[j], S);
+                p.blocks = L.tiles;
+                ++li;
+            } else if (marks[k] == M_FRAME_COPY) {
+                p.bytes = 2 * total;
+                p.blocks = e->copy_tiles;
+            }
+            out.push_back(p);
+        }
+    } catch (...) {
+        for (auto x : ev) cudaEventDestroy(x);
+        throw;
+    }
+    for (auto x : ev) cudaEventDestroy(x);
+    return out;
+}
+
 gtsc_status batch_status(BatchEngine *e, cudaStream_t s)
 {
     uint32_t w = 0;
@@ -785,7 +878,9 @@ gtsc_status batch_status(BatchEngine *e, cudaStream_t s)
 
 int batch_launches(BatchEngine *e, bool compress)
 {
-    return compress ? (int)e->launch_c.size() + 5 : (int)e->launch_d.size() + 3;
+    // compress: set streams, zero, stages, frame sizes / layout / copy; decompress: set streams,
+    // zero, parse directory + frames, stages
+    return compress ? (int)e->launch_c.size() + 5 : (int)e->launch_d.size() + 4;
 }
 
 }  // namespace gtsc

@@ -117,6 +117,15 @@ void batch_decompress(BatchEngine *e, const uint8_t *framed, uint64_t framed_byt
 gtsc_status batch_status(BatchEngine *e, cudaStream_t s);
 // number of kernel launches in one compress / decompress step
 int batch_launches(BatchEngine *e, bool compress);
+// one step run launch by launch with events between launches: per launch its pass kind (a BOp, or
+// a negative code for the fixed kernels), its time and the bytes it must move at least
+struct BatchLaunchProfile {
+    int op;
+    float ms;
+    uint64_t bytes;
+    uint64_t blocks;
+};
+std::vector<BatchLaunchProfile> batch_profile(BatchEngine *e, bool compress, cudaStream_t s);
 
 // stage launcher (batch_kernels.cu / batch_decode.cu): one launch of `total_tiles` blocks
 void launch_batch_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,

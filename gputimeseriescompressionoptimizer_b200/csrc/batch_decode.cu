@@ -143,7 +143,10 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     }
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     if (base >= n) return;
     unsigned long long acc = ld_unaligned<ES>(meta.ptr) + s_prefix + excl;
@@ -250,7 +253,10 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     const uint32_t bits = base < n ? ((uint32_t)stencil[1 + base / 8] & valid_mask) : 0u;
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(bits), ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     if (base >= n) return;
     uint64_t yes_pos = s_prefix + excl, no_pos = base - yes_pos;
@@ -318,7 +324,10 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
     if (neg) set_status(status, GTSC_ERR_FORMAT);
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     unsigned long long acc = s_prefix + excl;
 #pragma unroll

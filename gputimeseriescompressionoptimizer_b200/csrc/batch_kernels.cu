@@ -468,7 +468,10 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     const uint32_t yes_bits = bits & valid_mask;
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(yes_bits), ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     uint64_t yes_pos = s_prefix + excl;
     uint64_t no_pos = (base < n ? base : n) - yes_pos;
@@ -544,7 +547,10 @@ __device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
     }
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(heads), ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     uint64_t r = s_prefix + excl;
     uint8_t *values = S[it.out[2]].ptr;
@@ -846,7 +852,10 @@ __device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool d
     }
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     unsigned long long acc = s_prefix + excl;
 #pragma unroll

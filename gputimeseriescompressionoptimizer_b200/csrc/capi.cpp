@@ -294,6 +294,23 @@ gtsc_status gtsc_batch_status(gtsc_batch *b, void *stream)
 
 int32_t gtsc_batch_launches(gtsc_batch *b, int32_t compress) { return b ? batch_launches(b->e, compress != 0) : 0; }
 
+gtsc_status gtsc_batch_profile(gtsc_batch *b, int32_t compress, int32_t *ops, float *ms, uint64_t *bytes,
+                               uint64_t *blocks, int32_t cap, int32_t *n, void *stream)
+{
+    return guard([&] {
+        if (!b || !ops || !ms || !bytes || !blocks || !n) fail(GTSC_ERR_ARG, "null argument");
+        const auto p = batch_profile(b->e, compress != 0, S(stream));
+        if ((int64_t)p.size() > cap) fail(GTSC_ERR_CAPACITY, "profile: more launches than cap");
+        for (size_t i = 0; i < p.size(); i++) {
+            ops[i] = p[i].op;
+            ms[i] = p[i].ms;
+            bytes[i] = p[i].bytes;
+            blocks[i] = p[i].blocks;
+        }
+        *n = (int32_t)p.size();
+    });
+}
+
 gtsc_status gtsc_batch_destroy(gtsc_batch *b)
 {
     return guard([&] {

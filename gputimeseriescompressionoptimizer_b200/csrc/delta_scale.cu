@@ -80,7 +80,10 @@ k_delta_decode(const uint8_t *__restrict__ d, uint64_t n, const uint8_t *__restr
     unsigned long long total;
     unsigned long long excl = block_exclusive_scan<DD_THREADS>(local, ws, total);
     __shared__ unsigned long long s_prefix;
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     unsigned long long acc = ld_unaligned<ES>(first_p) + s_prefix + excl;
     uint64_t o[DD_PER];

@@ -23,7 +23,7 @@ namespace {
 // at most 2^24 decoded values per call: 8192 scan tiles of 2048 values
 constexpr uint64_t kNoAllocMaxValues = 1ull << 24;
 constexpr uint64_t kNoAllocTiles = kNoAllocMaxValues / 2048;
-constexpr uint64_t kNoAllocScratchBytes = 16 + 4 * kNoAllocTiles + 16 * kNoAllocTiles;
+constexpr uint64_t kNoAllocScratchBytes = lookback_bytes(kNoAllocTiles);
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -67,7 +67,7 @@ extern "C" gtsc_status gtsc_delta_decode_noalloc(int32_t dtype, const void *d_fi
             fail(GTSC_ERR_ARG, "deltas must be aligned to the element size and the output to 16 bytes");
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
         uint8_t *scratch = scratch_for_current_device();
-        // launch_delta_decode clears the counter, error word and tile flags before its kernel
+        // launch_delta_decode clears the counter, error word and tile descriptors before its kernel
         launch_delta_decode((const uint8_t *)d_deltas, n, (const uint8_t *)d_first, (uint8_t *)d_out, scratch, es, s);
         uint32_t err = 0;
         GTSC_CUDA(cudaMemcpyAsync(&err, lookback_at(scratch, delta_decode_tiles(n)).error, 4, cudaMemcpyDeviceToHost, s));

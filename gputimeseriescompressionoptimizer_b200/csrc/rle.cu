@@ -45,7 +45,10 @@ k_rle_heads(const uint8_t *__restrict__ in, uint64_t n, Order o, uint8_t *__rest
     }
     unsigned long long total;
     unsigned long long excl = block_exclusive_scan<R_THREADS>((unsigned long long)__popc(heads), ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     uint64_t r = s_prefix + excl;
     for (int j = 0; j < R_PER; j++)
@@ -88,7 +91,10 @@ k_scan_i32(const uint8_t *__restrict__ in, uint64_t n, unsigned long long *__res
     }
     unsigned long long total;
     unsigned long long excl = block_exclusive_scan<R_THREADS>(local, ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     unsigned long long acc = s_prefix + excl;
 #pragma unroll

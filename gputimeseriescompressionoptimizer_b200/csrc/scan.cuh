@@ -1,12 +1,13 @@
 // scan.cuh -- single-pass device-wide prefix scans by decoupled look-back, written for sm_100a.
 //
 // A kernel processes tiles in the order it claims them from a global counter (so every tile's
-// predecessors were claimed earlier and make progress).  Thread 0 of a tile publishes the tile's
-// aggregate (flag 1), walks back over the predecessors' flags, adds their aggregates until it finds
-// an inclusive prefix (flag 2), then publishes its own inclusive prefix.  Flags and values are
-// separate words ordered with st.release / ld.acquire at gpu scope.  Every wait is bounded: after
-// kSpinLimit polls the tile records GTSC_ERR_TIMEOUT in *error and proceeds with a wrong prefix,
-// so a broken predecessor can never hang the GPU; the host turns the error word into a status.
+// predecessors were claimed earlier and make progress).  One warp of a tile publishes the tile's
+// aggregate (flag 1), reads its predecessors' descriptors 32 at a time, adds their aggregates until
+// it finds an inclusive prefix (flag 2), then publishes its own inclusive prefix.  A descriptor is
+// two relaxed gpu-scope 64-bit words that both carry the flag, so a reader needs no acquire chain.
+// Every wait is bounded: after kSpinLimit polls, or as soon as another tile has recorded an error,
+// the tile records GTSC_ERR_TIMEOUT in *error and proceeds with a wrong prefix, so a broken
+// predecessor can never hang the GPU; the host turns the error word into a status.
 //
 // Values are 64-bit and combine by wrapping addition, which also serves 8/16/32-bit wrapping
 // arithmetic (the low bits of a 64-bit wrapping sum are the narrow wrapping sum).
@@ -20,41 +21,29 @@ constexpr uint32_t kSpinLimit = 1u << 22;  // ~0.3 s of polling with back-off
 
 struct Lookback {
     uint32_t *counter;             // tile claim counter (zeroed before launch)
-    uint32_t *flags;               // per tile: 0 none, 1 aggregate, 2 inclusive prefix (zeroed)
-    unsigned long long *agg;       // per tile aggregate
-    unsigned long long *pre;       // per tile inclusive prefix
     uint32_t *error;               // set to a gtsc_status on timeout (zeroed)
+    unsigned long long *desc;      // per tile two words: flag 0 none, 1 aggregate, 2 inclusive (zeroed)
 };
 
-// bytes of scratch for `tiles` tiles; layout: counter, error, pad, flags[tiles], agg[tiles], pre[tiles]
-__host__ __device__ inline uint64_t lookback_bytes(uint64_t tiles)
-{
-    return 16 + ((4 * tiles + 15) & ~15ull) + 16 * tiles;
-}
-// bytes that must be zeroed before each launch (counter, error and the flags)
-__host__ __device__ inline uint64_t lookback_zero_bytes(uint64_t tiles) { return 16 + 4 * tiles; }
+// bytes of scratch for `tiles` tiles; layout: counter, error, pad, then per tile two 64-bit
+// descriptor words (word 0 = flag << 32 | low half of the value, word 1 = flag << 32 | high half)
+__host__ __device__ constexpr uint64_t lookback_bytes(uint64_t tiles) { return 16 + 16 * tiles; }
+// bytes that must be zeroed before each launch (counter, error and the descriptors)
+__host__ __device__ constexpr uint64_t lookback_zero_bytes(uint64_t tiles) { return 16 + 16 * tiles; }
 
 __host__ __device__ inline Lookback lookback_at(uint8_t *scratch, uint64_t tiles)
 {
     Lookback l;
     l.counter = (uint32_t *)scratch;
     l.error = (uint32_t *)(scratch + 4);
-    l.flags = (uint32_t *)(scratch + 16);
-    uint8_t *v = scratch + 16 + ((4 * tiles + 15) & ~15ull);
-    l.agg = (unsigned long long *)v;
-    l.pre = (unsigned long long *)(v + 8 * tiles);
+    l.desc = (unsigned long long *)(scratch + 16);
+    (void)tiles;
     return l;
 }
 
-__device__ __forceinline__ void st_release_u32(uint32_t *p, uint32_t v)
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v)
 {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p)
-{
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
 {
@@ -66,39 +55,67 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 // Claims the next tile id (one thread per block; broadcast through shared memory by the caller).
 __device__ __forceinline__ uint32_t claim_tile(const Lookback &l) { return atomicAdd(l.counter, 1u); }
 
-// Called by ONE thread of the block that owns `tile`: publishes the tile aggregate and returns
-// the exclusive prefix (wrapping sum of all earlier tiles).
+// A descriptor is published as two words that each carry the flag, so a reader that sees the
+// same flag in both has a consistent value without any ordering between the stores.
+__device__ __forceinline__ void lookback_publish(const Lookback &l, uint32_t tile, uint32_t flag,
+                                                 unsigned long long v)
+{
+    const unsigned long long f = (unsigned long long)flag << 32;
+    st_relaxed_u64(l.desc + 2 * (uint64_t)tile, f | (v & 0xffffffffull));
+    st_relaxed_u64(l.desc + 2 * (uint64_t)tile + 1, f | (v >> 32));
+}
+
+// Called by all 32 lanes of ONE warp of the block that owns `tile` (the same tile_agg in every
+// lane): publishes the tile aggregate and returns the exclusive prefix (wrapping sum of all
+// earlier tiles) in every lane.  The warp inspects 32 predecessors per round trip: lane k reads
+// tile - 1 - k; the window is summed up to the nearest inclusive prefix, or wholly when it holds
+// only aggregates, and then moves 32 tiles back.
 __device__ inline unsigned long long lookback_exclusive(const Lookback &l, uint32_t tile, unsigned long long tile_agg)
 {
+    const int lane = threadIdx.x & 31;
     if (tile == 0) {
-        l.pre[0] = tile_agg;
-        st_release_u32(&l.flags[0], 2u);
+        if (lane == 0) lookback_publish(l, 0, 2u, tile_agg);
         return 0ull;
     }
-    l.agg[tile] = tile_agg;
-    st_release_u32(&l.flags[tile], 1u);
+    if (lane == 0) lookback_publish(l, tile, 1u, tile_agg);
     unsigned long long excl = 0;
-    int64_t t = (int64_t)tile - 1;
+    int64_t base = (int64_t)tile - 1;
     uint32_t spins = 0;
-    while (t >= 0) {
-        uint32_t f = ld_acquire_u32(&l.flags[t]);
-        if (f == 2u) {
-            excl += ld_relaxed_u64(&l.pre[t]);
-            break;
+    while (true) {
+        const int64_t idx = base - lane;
+        uint32_t flag = 2u;
+        unsigned long long v = 0;
+        if (idx >= 0) {
+            const unsigned long long w0 = ld_relaxed_u64(l.desc + 2 * idx);
+            const unsigned long long w1 = ld_relaxed_u64(l.desc + 2 * idx + 1);
+            const uint32_t f0 = (uint32_t)(w0 >> 32), f1 = (uint32_t)(w1 >> 32);
+            flag = f0 == f1 ? f0 : 0u;
+            v = (w0 & 0xffffffffull) | (w1 << 32);
         }
-        if (f == 1u) {
-            excl += ld_relaxed_u64(&l.agg[t]);
-            --t;
-            continue;
+        if (__any_sync(0xffffffffu, flag == 0u)) {
+            ++spins;
+            const bool gave_up = (spins & 63u) == 0 && *(volatile uint32_t *)l.error != 0u;
+            if (spins <= kSpinLimit && !__any_sync(0xffffffffu, gave_up)) {
+                __nanosleep(spins < 64 ? 32 : 256);
+                continue;
+            }
+            // bounded wait: record the timeout and stop at the unpublished tile (wrong prefix)
+            if (lane == 0) atomicExch(l.error, (uint32_t)(-GTSC_ERR_TIMEOUT));
+            if (flag == 0u) {
+                flag = 2u;
+                v = 0;
+            }
         }
-        if (++spins > kSpinLimit) {
-            atomicExch(l.error, (uint32_t)(-GTSC_ERR_TIMEOUT));
-            break;
-        }
-        __nanosleep(spins < 64 ? 32 : 256);
+        const unsigned incl = __ballot_sync(0xffffffffu, flag == 2u);
+        const int stop = incl ? __ffs(incl) - 1 : 31;
+        unsigned long long sum = lane <= stop ? v : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        excl += sum;
+        if (incl) break;
+        base -= 32;
     }
-    l.pre[tile] = excl + tile_agg;
-    st_release_u32(&l.flags[tile], 2u);
+    if (lane == 0) lookback_publish(l, tile, 2u, excl + tile_agg);
     return excl;
 }
 

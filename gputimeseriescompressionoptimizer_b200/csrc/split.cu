@@ -104,7 +104,10 @@ k_split(const uint8_t *__restrict__ in, uint64_t n, SplitArgs a, Lookback lb)
     const uint32_t yes_bits = bits & valid_mask;
     unsigned long long total;
     unsigned long long excl = block_exclusive_scan<SP_THREADS>((unsigned long long)__popc(yes_bits), ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     uint64_t yes_pos = s_prefix + excl;
     uint64_t no_pos = (base < n ? base : n) - yes_pos;
@@ -143,7 +146,10 @@ k_merge(const uint8_t *__restrict__ stencil, uint64_t n, MergeArgs a, uint8_t *_
     const uint32_t bits = base < n ? ((uint32_t)__ldg(stencil + base / 8) & valid_mask) : 0u;
     unsigned long long total;
     unsigned long long excl = block_exclusive_scan<SP_THREADS>((unsigned long long)__popc(bits), ws, total);
-    if (threadIdx.x == 0) s_prefix = lookback_exclusive(lb, tile, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
     __syncthreads();
     if (base >= n) return;
     uint64_t top[4] = {0, 0, 0, 0};

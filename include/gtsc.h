@@ -71,7 +71,9 @@ gtsc_status gtsc_stream_destroy(void *stream);
 /*
  * Encoding::Encode(SharedCudaPtr<char> data, DataType) (compression/encoding.hpp:28-47).
  * Writes out[0] = metadata, out[1..n_out-1] = encoded streams, byte-identical to the reference
- * encoder for the same input (see DESIGN.md for the documented exceptions).  Synchronises the
+ * encoder for the same input (bytes the reference leaves uninitialised -- AFL metadata bytes 2-3,
+ * unused dictionary slots, dictionary code bits past the last value -- are written as 0; the
+ * dictionary's top-4 ties are ordered by value).  Synchronises the
  * stream once to learn the data-dependent output sizes, as the reference does.
  */
 gtsc_status gtsc_encode(int32_t encoding, int32_t dtype, const void *d_in, uint64_t in_bytes,
@@ -182,6 +184,15 @@ gtsc_status gtsc_batch_decompress(gtsc_batch *b, const void *d_framed, uint64_t 
 gtsc_status gtsc_batch_status(gtsc_batch *b, void *stream);
 /* kernel launches in one step (compress != 0: compress step) */
 int32_t gtsc_batch_launches(gtsc_batch *b, int32_t compress);
+/*
+ * One step run launch by launch with CUDA events between the launches (not the graph): per launch
+ * its pass kind (ops[i] >= 0, or -1 stream setup, -2 scratch zeroing, -3/-4/-5 frame sizes / layout
+ * / copy, -6 frame parse), its time in ms, the bytes it must read and write at least (its input and
+ * output streams) and its blocks.  Writes at most cap entries and the count to *n.  Synchronises.
+ * No counterpart in the reference (its per-column calls are timed one by one).
+ */
+gtsc_status gtsc_batch_profile(gtsc_batch *b, int32_t compress, int32_t *ops, float *ms, uint64_t *bytes,
+                               uint64_t *blocks, int32_t cap, int32_t *n, void *stream);
 gtsc_status gtsc_batch_destroy(gtsc_batch *b);
 
 /* ------------------------------------------------------------------ kernel-level entry points */
