@@ -108,6 +108,22 @@ def lib():
         L.gtsc_batch_launches.argtypes = [vp, i32]
         L.gtsc_batch_destroy.argtypes = [vp]
         L.gtsc_batch_profile.argtypes = [vp, i32, i32p, ctypes.POINTER(ctypes.c_float), u64p, u64p, i32, i32p, vp]
+        f32p = ctypes.POINTER(ctypes.c_float)
+        L.gtsc_planner_features.argtypes = [ctypes.POINTER(Column), u32, vp, vp]
+        L.gtsc_planner_create.argtypes = [i16p, i32p, i32, u64, ctypes.POINTER(vp)]
+        L.gtsc_planner_load.argtypes = [vp, u64, ctypes.POINTER(vp)]
+        L.gtsc_planner_save.argtypes = [vp, vp, u64, u64p]
+        L.gtsc_planner_destroy.argtypes = [vp]
+        L.gtsc_planner_classes.argtypes = [vp]
+        L.gtsc_planner_param_count.argtypes = [vp]
+        L.gtsc_planner_param_count.restype = u64
+        L.gtsc_planner_get_params.argtypes = [vp, f32p, f32p, f32p]
+        L.gtsc_planner_set_params.argtypes = [vp, f32p, f32p, f32p]
+        L.gtsc_planner_valid.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8)]
+        L.gtsc_planner_gradient.argtypes = [vp, vp, i32p, u32, f32p, f32p, vp]
+        L.gtsc_planner_train.argtypes = [vp, vp, i32p, u32, i32, i32, ctypes.c_float, u64, f32p, vp]
+        L.gtsc_planner_predict.argtypes = [vp, vp, i32p, u32, i32p, f32p, vp]
+        L.gtsc_plan_learned.argtypes = [vp, ctypes.POINTER(Column), u32, ctypes.c_float, i16p, i32, i32p, i32p, vp]
         _lib = L
     return _lib
 
@@ -363,6 +379,129 @@ class Batch:
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:
             _lib.gtsc_batch_destroy(self.handle)
+            self.handle = None
+
+
+# ------------------------------------------------------------------------ learned planner
+N_FEATURES = 32
+MODEL_PATH = os.path.join(HERE, "planner_model.bin")
+
+
+def _columns(cols, dtypes):
+    arr = (Column * len(cols))()
+    for i, (c, dt) in enumerate(zip(cols, dtypes)):
+        arr[i] = Column(c.ptr, c.nbytes, dt, 0)
+    return arr
+
+
+def _f32(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _i32(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def planner_features(cols, dtypes, stream=None):
+    """Planner features of the columns' samples -> DeviceBuffer of len(cols) x 32 float32."""
+    out = alloc(4 * N_FEATURES * max(len(cols), 1), stream)
+    check(lib().gtsc_planner_features(_columns(cols, dtypes), len(cols), out.ptr, stream), "planner_features")
+    return out
+
+
+class Planner:
+    """The learned tree planner (an MLP over column features, exhaustive-planner fallback)."""
+
+    def __init__(self, classes=None, seed=0, model=None):
+        h = ctypes.c_void_p()
+        if model is not None:
+            b = np.frombuffer(bytes(model), np.uint8)
+            check(lib().gtsc_planner_load(b.ctypes.data, b.size, ctypes.byref(h)), "planner_load")
+        else:
+            lens = np.array([len(c) for c in classes], np.int32)
+            encs = np.ascontiguousarray(np.concatenate([np.asarray(c, np.int16) for c in classes]))
+            check(lib().gtsc_planner_create(encs.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)), _i32(lens),
+                                            len(classes), seed, ctypes.byref(h)), "planner_create")
+        self.handle = h.value
+        self.K = lib().gtsc_planner_classes(self.handle)
+
+    @classmethod
+    def load(cls, path=MODEL_PATH):
+        with open(path, "rb") as f:
+            return cls(model=f.read())
+
+    def save(self, path=None):
+        n = ctypes.c_uint64(0)
+        check(lib().gtsc_planner_save(self.handle, None, 0, ctypes.byref(n)), "planner_save")
+        buf = np.zeros(n.value, np.uint8)
+        check(lib().gtsc_planner_save(self.handle, buf.ctypes.data, buf.size, ctypes.byref(n)), "planner_save")
+        if path:
+            with open(path, "wb") as f:
+                f.write(buf.tobytes())
+        return buf.tobytes()
+
+    @property
+    def n_params(self):
+        return lib().gtsc_planner_param_count(self.handle)
+
+    def get_params(self):
+        p = np.zeros(self.n_params, np.float32)
+        mu = np.zeros(N_FEATURES, np.float32)
+        sd = np.zeros(N_FEATURES, np.float32)
+        check(lib().gtsc_planner_get_params(self.handle, _f32(p), _f32(mu), _f32(sd)), "planner_get_params")
+        return p, mu, sd
+
+    def set_params(self, params=None, mu=None, sd=None):
+        args = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (params, mu, sd)]
+        check(lib().gtsc_planner_set_params(self.handle, *[None if a is None else _f32(a) for a in args]),
+              "planner_set_params")
+
+    def valid(self):
+        v = np.zeros(self.K * 6, np.uint8)
+        check(lib().gtsc_planner_valid(self.handle, v.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))), "valid")
+        return v.reshape(self.K, 6)
+
+    def gradient(self, d_features, labels, stream=None):
+        labels = np.ascontiguousarray(labels, np.int32)
+        g = np.zeros(self.n_params, np.float32)
+        loss = ctypes.c_float(0)
+        check(lib().gtsc_planner_gradient(self.handle, d_features.ptr, _i32(labels), labels.size, _f32(g),
+                                          ctypes.byref(loss), stream), "planner_gradient")
+        return loss.value, g
+
+    def train(self, d_features, labels, epochs=100, batch=256, lr=2e-3, seed=1, stream=None):
+        labels = np.ascontiguousarray(labels, np.int32)
+        loss = ctypes.c_float(0)
+        check(lib().gtsc_planner_train(self.handle, d_features.ptr, _i32(labels), labels.size, epochs, batch, lr,
+                                       seed, ctypes.byref(loss), stream), "planner_train")
+        return loss.value
+
+    def predict(self, d_features, dtypes, stream=None):
+        dtypes = np.ascontiguousarray(dtypes, np.int32)
+        cls = np.zeros(dtypes.size, np.int32)
+        conf = np.zeros(dtypes.size, np.float32)
+        check(lib().gtsc_planner_predict(self.handle, d_features.ptr, _i32(dtypes), dtypes.size, _i32(cls),
+                                         _f32(conf), stream), "planner_predict")
+        return cls, conf
+
+    def plan(self, cols, dtypes, min_confidence=0.5, stream=None):
+        """Trees for the columns: [(nodes, fallback_used)]."""
+        cap = 64 * max(len(cols), 1)
+        nodes = np.zeros(2 * cap, np.int16)
+        counts = np.zeros(len(cols), np.int32)
+        fb = np.zeros(len(cols), np.int32)
+        check(lib().gtsc_plan_learned(self.handle, _columns(cols, dtypes), len(cols), min_confidence,
+                                      nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)), cap, _i32(counts),
+                                      _i32(fb), stream), "plan_learned")
+        out, pos = [], 0
+        for c, f in zip(counts, fb):
+            out.append((nodes[2 * pos: 2 * (pos + c)].copy(), bool(f)))
+            pos += c
+        return out
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.gtsc_planner_destroy(self.handle)
             self.handle = None
 
 

@@ -4,6 +4,7 @@
 #include "encodings.hpp"
 #include "kernels.hpp"
 #include "batch.hpp"
+#include "learned.hpp"
 #include "planner.hpp"
 #include "tree.hpp"
 
@@ -317,6 +318,172 @@ gtsc_status gtsc_batch_destroy(gtsc_batch *b)
         if (!b) return;
         batch_destroy(b->e);
         delete b;
+    });
+}
+
+// ------------------------------------------------------------------------------- learned planner
+struct gtsc_planner {
+    Planner *p;
+};
+
+gtsc_status gtsc_planner_features(const gtsc_column *cols, uint32_t n_cols, float *d_features, void *stream)
+{
+    return guard([&] {
+        if ((!cols && n_cols) || (!d_features && n_cols)) fail(GTSC_ERR_ARG, "null argument");
+        std::vector<FeatureColumn> fc(n_cols);
+        for (uint32_t c = 0; c < n_cols; c++) {
+            const int es = dtype_size(cols[c].dtype);
+            if (!es) fail(GTSC_ERR_ARG, "unknown data type");
+            fc[c] = FeatureColumn{cols[c].d_data, cols[c].bytes / es, cols[c].dtype};
+        }
+        compute_features(fc, d_features, S(stream));
+    });
+}
+
+gtsc_status gtsc_planner_create(const int16_t *class_encs, const int32_t *class_lens, int32_t n_classes,
+                                uint64_t seed, gtsc_planner **out)
+{
+    return guard([&] {
+        if (!class_encs || !class_lens || !out || n_classes <= 0) fail(GTSC_ERR_ARG, "null argument");
+        std::vector<std::vector<int16_t>> cls(n_classes);
+        size_t off = 0;
+        for (int c = 0; c < n_classes; c++) {
+            if (class_lens[c] <= 0 || class_lens[c] > 1024) fail(GTSC_ERR_ARG, "planner: bad class length");
+            cls[c].assign(class_encs + off, class_encs + off + class_lens[c]);
+            off += class_lens[c];
+        }
+        std::unique_ptr<Planner> p(new Planner(cls, seed));
+        *out = new gtsc_planner{p.release()};
+    });
+}
+
+gtsc_status gtsc_planner_load(const void *model, uint64_t bytes, gtsc_planner **out)
+{
+    return guard([&] {
+        if (!model || !out) fail(GTSC_ERR_ARG, "null argument");
+        *out = new gtsc_planner{Planner::load(model, bytes)};
+    });
+}
+
+gtsc_status gtsc_planner_save(gtsc_planner *p, void *buf, uint64_t cap, uint64_t *bytes)
+{
+    return guard([&] {
+        if (!p || !bytes) fail(GTSC_ERR_ARG, "null argument");
+        const std::vector<uint8_t> m = p->p->save();
+        *bytes = m.size();
+        if (buf) {
+            if (cap < m.size()) fail(GTSC_ERR_CAPACITY, "planner_save: buffer too small");
+            std::memcpy(buf, m.data(), m.size());
+        }
+    });
+}
+
+gtsc_status gtsc_planner_destroy(gtsc_planner *p)
+{
+    return guard([&] {
+        if (!p) return;
+        delete p->p;
+        delete p;
+    });
+}
+
+int32_t gtsc_planner_classes(gtsc_planner *p) { return p ? p->p->K : 0; }
+uint64_t gtsc_planner_param_count(gtsc_planner *p) { return p ? p->p->n_params() : 0; }
+
+gtsc_status gtsc_planner_get_params(gtsc_planner *p, float *params, float *mu, float *sd)
+{
+    return guard([&] {
+        if (!p) fail(GTSC_ERR_ARG, "null argument");
+        if (params) p->p->get_params(params, nullptr);
+        if (mu) std::memcpy(mu, p->p->mu.data(), 4 * kFeatures);
+        if (sd) std::memcpy(sd, p->p->sd.data(), 4 * kFeatures);
+    });
+}
+
+gtsc_status gtsc_planner_set_params(gtsc_planner *p, const float *params, const float *mu, const float *sd)
+{
+    return guard([&] {
+        if (!p) fail(GTSC_ERR_ARG, "null argument");
+        if (params) p->p->set_params(params, nullptr);
+        if (mu) std::memcpy(p->p->mu.data(), mu, 4 * kFeatures);
+        if (sd) std::memcpy(p->p->sd.data(), sd, 4 * kFeatures);
+    });
+}
+
+gtsc_status gtsc_planner_valid(gtsc_planner *p, uint8_t *valid)
+{
+    return guard([&] {
+        if (!p || !valid) fail(GTSC_ERR_ARG, "null argument");
+        std::memcpy(valid, p->p->valid.data(), p->p->valid.size());
+    });
+}
+
+gtsc_status gtsc_planner_gradient(gtsc_planner *p, const float *d_features, const int32_t *labels, uint32_t n_rows,
+                                  float *grad, float *loss, void *stream)
+{
+    return guard([&] {
+        if (!p || !d_features || !labels || !loss) fail(GTSC_ERR_ARG, "null argument");
+        *loss = p->p->gradient(d_features, labels, n_rows, grad, S(stream));
+    });
+}
+
+gtsc_status gtsc_planner_train(gtsc_planner *p, const float *d_features, const int32_t *labels, uint32_t n_rows,
+                               int32_t epochs, int32_t batch, float lr, uint64_t seed, float *final_loss,
+                               void *stream)
+{
+    return guard([&] {
+        if (!p || !d_features || !labels) fail(GTSC_ERR_ARG, "null argument");
+        const float l = p->p->train(d_features, labels, n_rows, epochs, batch, lr, seed, S(stream));
+        if (final_loss) *final_loss = l;
+    });
+}
+
+gtsc_status gtsc_planner_predict(gtsc_planner *p, const float *d_features, const int32_t *dtypes, uint32_t n_rows,
+                                 int32_t *classes, float *confidence, void *stream)
+{
+    return guard([&] {
+        if (!p || (!d_features && n_rows) || !dtypes || !classes || !confidence) fail(GTSC_ERR_ARG, "null argument");
+        p->p->predict(d_features, dtypes, n_rows, classes, confidence, S(stream));
+    });
+}
+
+gtsc_status gtsc_plan_learned(gtsc_planner *p, const gtsc_column *cols, uint32_t n_cols, float min_confidence,
+                              int16_t *nodes_out, int32_t nodes_cap, int32_t *node_counts, int32_t *fallback,
+                              void *stream)
+{
+    return guard([&] {
+        if (!p || (!cols && n_cols) || !nodes_out || !node_counts || !fallback) fail(GTSC_ERR_ARG, "null argument");
+        cudaStream_t s = S(stream);
+        if (!n_cols) return;
+        std::vector<FeatureColumn> fc(n_cols);
+        std::vector<int32_t> dts(n_cols);
+        for (uint32_t c = 0; c < n_cols; c++) {
+            const int es = dtype_size(cols[c].dtype);
+            if (!es) fail(GTSC_ERR_ARG, "unknown data type");
+            fc[c] = FeatureColumn{cols[c].d_data, cols[c].bytes / es, cols[c].dtype};
+            dts[c] = cols[c].dtype;
+        }
+        DevBuf feats = dev_alloc((size_t)n_cols * kFeatures * 4, s);
+        compute_features(fc, (float *)feats.get(), s);
+        std::vector<int32_t> cls(n_cols);
+        std::vector<float> conf(n_cols);
+        p->p->predict((const float *)feats.get(), dts.data(), n_cols, cls.data(), conf.data(), s);
+        int32_t used = 0;
+        for (uint32_t c = 0; c < n_cols; c++) {
+            Tree t;
+            fallback[c] = !(cls[c] >= 0 && conf[c] >= min_confidence);
+            if (!fallback[c]) {
+                t = p->p->class_tree(cls[c], dts[c]);
+            } else {
+                const uint64_t sb = sample_bytes(dts[c], cols[c].bytes);
+                uint64_t sz = 0;
+                t = plan_exhaustive(dts[c], View{cols[c].d_data, sb}, &sz, nullptr, s);
+            }
+            if (used + t.size() > nodes_cap) fail(GTSC_ERR_CAPACITY, "plan_learned: nodes_cap too small");
+            tree_to_nodes(t, nodes_out + 2 * used);
+            node_counts[c] = t.size();
+            used += t.size();
+        }
     });
 }
 

@@ -195,6 +195,55 @@ gtsc_status gtsc_batch_profile(gtsc_batch *b, int32_t compress, int32_t *ops, fl
                                uint64_t *blocks, int32_t cap, int32_t *n, void *stream);
 gtsc_status gtsc_batch_destroy(gtsc_batch *b);
 
+/* ------------------------------------------------------------------ learned planner */
+
+/*
+ * A small MLP over column features proposes the compression tree; the exhaustive planner above is
+ * its fallback.  No counterpart in the reference (its planners are FullStatisticsUpdate and
+ * OptimizeTree, optimizer/compression_optimizer.cpp:16-140); it stands beside gtsc_plan_exhaustive
+ * and returns trees in the same node-list form.
+ *
+ * Features: 32 floats per column from its first min(n, 10000) elements (the exhaustive planner's
+ * sample, GetSampleDataForFullUpdateSize): data-type one-hot, size, NaN / inf share, sortedness,
+ * runs, distinct values and the largest multiplicities, value / delta / second-delta bit widths,
+ * float precision and floatToInt feasibility.  d_features: device, n_cols x 32, row-major.
+ */
+#define GTSC_PLANNER_FEATURES 32
+typedef struct gtsc_planner gtsc_planner;
+gtsc_status gtsc_planner_features(const gtsc_column *cols, uint32_t n_cols, float *d_features, void *stream);
+/* A new network (He-uniform from `seed`) over n_classes tree classes: class c is the pre-order
+ * encoding list class_encs[off_c .. off_c + class_lens[c]) (the lists concatenated). */
+gtsc_status gtsc_planner_create(const int16_t *class_encs, const int32_t *class_lens, int32_t n_classes,
+                                uint64_t seed, gtsc_planner **out);
+/* Serialized model ("GTSCMLP1": shape, normalisation, parameters, class table). */
+gtsc_status gtsc_planner_load(const void *model, uint64_t bytes, gtsc_planner **out);
+gtsc_status gtsc_planner_save(gtsc_planner *p, void *buf, uint64_t cap, uint64_t *bytes);
+gtsc_status gtsc_planner_destroy(gtsc_planner *p);
+int32_t gtsc_planner_classes(gtsc_planner *p);
+/* parameters: W1[32x64] b1[64] W2[64x64] b2[64] W3[64xK] b3[K] (W row-major, in x out) */
+uint64_t gtsc_planner_param_count(gtsc_planner *p);
+gtsc_status gtsc_planner_get_params(gtsc_planner *p, float *params, float *mu, float *sd);
+gtsc_status gtsc_planner_set_params(gtsc_planner *p, const float *params, const float *mu, const float *sd);
+/* valid[c * 6 + dtype] = 1 when class c can encode a column of that data type */
+gtsc_status gtsc_planner_valid(gtsc_planner *p, uint8_t *valid);
+/* Mean cross-entropy over the rows (label < 0: skipped) and its gradient w.r.t. the parameters,
+ * by the library's forward and backward kernels (FP32, fixed summation order). */
+gtsc_status gtsc_planner_gradient(gtsc_planner *p, const float *d_features, const int32_t *labels, uint32_t n_rows,
+                                  float *grad, float *loss, void *stream);
+/* Adam over shuffled mini-batches on the device; sets the feature normalisation from the rows. */
+gtsc_status gtsc_planner_train(gtsc_planner *p, const float *d_features, const int32_t *labels, uint32_t n_rows,
+                               int32_t epochs, int32_t batch, float lr, uint64_t seed, float *final_loss,
+                               void *stream);
+/* Most probable valid class per row and its probability among the classes valid for the dtype. */
+gtsc_status gtsc_planner_predict(gtsc_planner *p, const float *d_features, const int32_t *dtypes, uint32_t n_rows,
+                                 int32_t *classes, float *confidence, void *stream);
+/* Trees for many columns: the network's class where its confidence >= min_confidence, else the
+ * exhaustive planner on the column's sample (fallback[c] = 1).  Node lists are written back to
+ * back into nodes_out (pairs), node_counts[c] nodes for column c. */
+gtsc_status gtsc_plan_learned(gtsc_planner *p, const gtsc_column *cols, uint32_t n_cols, float min_confidence,
+                              int16_t *nodes_out, int32_t nodes_cap, int32_t *node_counts, int32_t *fallback,
+                              void *stream);
+
 /* ------------------------------------------------------------------ kernel-level entry points */
 
 /*
