@@ -36,6 +36,8 @@ FALLBACK_HBM_GBS = 6650.0
 N_COLUMNS = int(os.environ.get("GTSC_BENCH_COLUMNS", "512"))
 MAX_LEN = 1 << int(os.environ.get("GTSC_BENCH_MAX_LOG2", "24"))
 CPU_SAMPLE_LEN = 1 << 18     # CPU legs: every column cut to its first 2^18 values
+MIN_CONFIDENCE = 0.5         # learned planner: below this softmax probability the exhaustive search decides
+TICK_CHUNKS = 4              # streaming tick table: 40 columns x 2^20 rows per chunk
 METRIC = "batched mixed-workload compress+decompress throughput (uncompressed GB/s)"
 WORKLOAD = (f"mixed {N_COLUMNS} columns, lengths log-uniform [4096, {MAX_LEN}], int32:float32:float64 = 2:1:1, "
             "generators walk/runs/zipf/const/outliers/price, seed 0xB204")
@@ -198,6 +200,65 @@ class DevView:
         self.nbytes = t.numel() * t.element_size()
 
 
+def tick_table(g, torch, planner, st, stream, sp):
+    """The streaming tick table (40 columns, 2^20-row chunks arriving one after another): per chunk
+    the learned planner against the exhaustive one (time, compressed bytes, fallbacks), and the
+    batched compress + decompress of the chunk with the learned trees (the engine is rebuilt only
+    when a column's tree changes)."""
+    from gputimeseriescompressionoptimizer_b200 import workloads as W
+    batch, prev, res = None, None, []
+    for ch in range(TICK_CHUNKS):
+        chunk = W.tick_chunk(40, 1 << 20, ch)
+        dts = [dt for _, dt, _ in chunk]
+        dev = [torch.from_numpy(x.view(np.uint8)).to("cuda") for _, _, x in chunk]
+        dv = [DevView(d) for d in dev]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        planned = planner.plan(dv, dts, MIN_CONFIDENCE, sp)
+        torch.cuda.synchronize()
+        t_ln = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ex = [g.plan_exhaustive(dt, g.DeviceBuffer(d.ptr, g.sample_bytes(dt, d.nbytes), owned=False), sp)[0]
+              for d, dt in zip(dv, dts)]
+        torch.cuda.synchronize()
+        t_ex = time.perf_counter() - t0
+        trees = [t for t, _ in planned]
+        key = [tuple(t) for t in trees]
+        if batch is None or key != prev:
+            batch = g.Batch(dv, dts, trees, st)
+            prev = key
+        else:
+            batch.set_inputs(dv)
+        outs = [torch.empty_like(d) for d in dev]
+        ov = [DevView(o) for o in outs]
+        batch.compress()
+        p, n = batch.output()
+        batch.decompress(p, n, ov)
+        batch.status()
+        assert all(torch.equal(a, b) for a, b in zip(outs, dev)), "tick chunk round trip differs"
+        sizes_ln = [b.size for b in g.split_framed(g.to_host(g.DeviceBuffer(p, n, owned=False)))]
+        sizes_ex = [g.tree_compress(t, d, sp).nbytes for t, d in zip(ex, dv)]
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(3):
+            batch.compress()
+            batch.decompress(p, n, ov)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t_step = ev0.elapsed_time(ev1) / 3e3
+        raw = sum(d.nbytes for d in dv)
+        res.append({"chunk": ch, "plan_learned_ms": round(1e3 * t_ln, 2), "plan_exhaustive_ms": round(1e3 * t_ex, 1),
+                    "fallbacks": int(sum(f for _, f in planned)),
+                    "ratio_learned": round(raw / sum(sizes_ln), 4), "ratio_exhaustive": round(raw / sum(sizes_ex), 4),
+                    "GBps": round(raw / t_step / 1e9, 2)})
+    gaps = [1 - r["ratio_learned"] / r["ratio_exhaustive"] for r in res]
+    return {"workload": "tick table: 40 columns (ts, price, volume, symbol, flags) x 2^20 rows per chunk",
+            "chunks": res, "ratio_gap": round(float(np.mean(gaps)), 4),
+            "fallback_rate": round(sum(r["fallbacks"] for r in res) / (40.0 * len(res)), 4),
+            "planning_speedup": round(sum(r["plan_exhaustive_ms"] for r in res) /
+                                      max(sum(r["plan_learned_ms"] for r in res), 1e-9), 1)}
+
+
 def run_ours(args, world, rank, local):
     import torch
     import gputimeseriescompressionoptimizer_b200 as g
@@ -226,13 +287,24 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     dv = [DevView(d) for d in dev]
 
-    # plain exhaustive planner on every column's sample (the reference's CompressData full update)
+    # the learned planner (features + MLP, exhaustive fallback below min confidence) for the batch
+    planner = g.Planner.load()
+    planner.plan(dv[:4], dts[:4], MIN_CONFIDENCE, sp)  # warm (kernel attributes, allocations)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    trees = []
+    planned = planner.plan(dv, dts, MIN_CONFIDENCE, sp)
+    torch.cuda.synchronize()
+    t_plan_learned = time.perf_counter() - t0
+    trees = [t for t, _ in planned]
+    fallback_rate = float(np.mean([f for _, f in planned]))
+
+    # the plain exhaustive planner on every column's sample (the reference's CompressData full update)
+    t0 = time.perf_counter()
+    ex_trees = []
     for d, dt in zip(dv, dts):
         sb = g.sample_bytes(dt, d.nbytes)
         nodes, _ = g.plan_exhaustive(dt, g.DeviceBuffer(d.ptr, sb, owned=False), sp)
-        trees.append(nodes)
+        ex_trees.append(nodes)
     torch.cuda.synchronize()
     t_plan_exh = time.perf_counter() - t0
 
@@ -298,14 +370,20 @@ def run_ours(args, world, rank, local):
     t_dec = timed(decompress, args.steps)
     batch.status()
 
-    # the plain path: one column at a time, planner excluded (trees as above)
+    # the plain path: one column at a time with the exhaustive planner's trees (planning timed above)
+    ex_sizes = [0] * len(cols)
+
     def plain():
         for i in range(len(cols)):
-            blob = g.tree_compress(trees[i], g.DeviceBuffer(dv[i].ptr, dv[i].nbytes, owned=False), sp)
+            blob = g.tree_compress(ex_trees[i], g.DeviceBuffer(dv[i].ptr, dv[i].nbytes, owned=False), sp)
+            ex_sizes[i] = blob.nbytes
             g.tree_decompress(blob, sp)
 
     plain()
     t_plain = timed(plain, 1)
+    ex_blob_bytes = sum(ex_sizes)
+    ratio_ln = [c.nbytes / b.size for c, b in zip(cols, blobs)]
+    ratio_ex = [c.nbytes / e for c, e in zip(cols, ex_sizes)]
 
     # end to end through the public API: pinned host columns in, framed output back to the host
     host_framed = torch.empty(framed["n"] + 4096, dtype=torch.uint8).pin_memory()
@@ -352,6 +430,7 @@ def run_ours(args, world, rank, local):
     ct, cin, _ = min((cpu_roundtrip(scols, trees, threads) for _ in range(2)), key=lambda r: r[0])
     cpu_gbs = cin / ct / 1e9
 
+    tick = tick_table(g, torch, planner, st, stream, sp) if rank == 0 else None
     tree_names = {}
     for t in trees:
         k = "-".join(g.tree_names(t))
@@ -363,14 +442,23 @@ def run_ours(args, world, rank, local):
         "config": {"workload": WORKLOAD, "columns": len(cols), "input_bytes": in_bytes, "blob_bytes": blob_bytes,
                    "compression_ratio": round(in_bytes / blob_bytes, 4),
                    "inputs": f"larger than L2 ({in_bytes / 1e9:.2f} GB), no flush needed",
-                   "planner": "plain exhaustive (FullStatisticsUpdate on each column's sample)",
+                   "planner": f"learned (MLP over 32 sample features, exhaustive fallback below confidence "
+                              f"{MIN_CONFIDENCE})",
+                   "plan_learned_ms": round(1e3 * t_plan_learned, 2), "fallback_rate": round(fallback_rate, 4),
+                   "ratio_learned": round(in_bytes / blob_bytes, 4),
+                   "ratio_exhaustive": round(in_bytes / ex_blob_bytes, 4),
+                   "ratio_gap": round(1 - ex_blob_bytes / blob_bytes, 4),
+                   "mean_column_ratio_learned": round(float(np.mean(ratio_ln)), 4),
+                   "mean_column_ratio_exhaustive": round(float(np.mean(ratio_ex)), 4),
+                   "blob_bytes_exhaustive": ex_blob_bytes,
                    "step": "gtsc_batch_compress + gtsc_batch_decompress (CUDA graphs), device-resident columns",
                    "compress_ms": round(1e3 * t_comp, 4), "decompress_ms": round(1e3 * t_dec, 4),
                    "hbm_frac_step": round(alg_step / t_step / 1e9 / peak, 4),
                    "algorithmic_bytes_per_step": alg_step,
                    "plain_path_ms": round(1e3 * t_plain, 2),
-                   "speedup_vs_plain": round(t_plain / t_step, 2),
                    "plan_exhaustive_ms": round(1e3 * t_plan_exh, 1),
+                   "speedup_vs_plain_step": round(t_plain / t_step, 2),
+                   "speedup_vs_plain_with_planning": round((t_plan_exh + t_plain) / (t_plan_learned + t_step), 2),
                    "batch_create_ms": round(1e3 * t_create, 1), "generate_s": round(t_gen, 1),
                    "trees": dict(sorted(tree_names.items(), key=lambda kv: -kv[1]))},
         "roofline": {"bound": "hbm", "kernel": f"{top[0]}:{top[1]}", "achieved": round(top_ach, 1), "peak": peak,
@@ -385,6 +473,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": round(world * in_bytes / t_e2e / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": in_bytes,
                 "d2h_bytes_per_step": e2e_step.d2h},
         "gpu_launches": (batch.launches(True) + batch.launches(False)) * args.steps,
+        "tick_table": tick,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

@@ -77,7 +77,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--columns", type=int, default=10000)
     ap.add_argument("--min-count", type=int, default=3)
-    ap.add_argument("--max-classes", type=int, default=64)
+    ap.add_argument("--max-classes", type=int, default=96)
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--lr", type=float, default=2e-3)

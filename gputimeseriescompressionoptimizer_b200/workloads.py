@@ -152,12 +152,22 @@ TRAIN_KINDS = KINDS + ["ts", "tick_price", "volume", "flags", "uniform", "sawtoo
 
 def training_column(seed, m=10000):
     """One seeded training column for the learned planner: (kind, dtype, nominal length, the first
-    min(m, length) values).  Generator parameters are drawn per column so the family covers the
-    benchmark generators and the tick table without repeating their exact settings."""
+    min(m, length) values).  Four in ten come from the benchmark generators (column(), fresh seeds),
+    fifteen in a hundred from the tick-table generators, the rest from the family below whose
+    parameters are drawn per column."""
     rng = np.random.default_rng([0x7EA1, seed])
-    kind = TRAIN_KINDS[rng.integers(0, len(TRAIN_KINDS))]
     n_total = int(np.floor(np.exp(rng.uniform(np.log(1024), np.log(1 << 24)))))
     n = min(m, n_total)
+    u = rng.random()
+    if u < 0.40:
+        kind = KINDS[rng.integers(0, len(KINDS))]
+        dtype = [INT, INT, FLOAT, DOUBLE, TIME, SHORT][rng.integers(0, 6)]
+        return kind, dtype, n_total, column(kind, dtype, n, (0x7EA1 << 20) + seed)
+    if u < 0.55:
+        chunk = tick_chunk(n_cols=5, rows=n, chunk=int(rng.integers(0, 1000)), seed=int(rng.integers(1 << 30)))
+        kind, dtype, x = chunk[rng.integers(0, 5)]
+        return "tick_" + kind, dtype, n_total, x
+    kind = TRAIN_KINDS[rng.integers(0, len(TRAIN_KINDS))]
     dtype = [INT, INT, FLOAT, DOUBLE, TIME, SHORT, CHAR][rng.integers(0, 7)]
     v = None
     if kind == "walk":
