@@ -64,6 +64,7 @@ struct Launch {
     int op;
     int first, count;
     uint64_t tiles;
+    uint64_t map_off;  // this launch's tile -> item table in the item_of array
 };
 
 uint64_t gfc_warps_for(bool dbl, uint64_t n)
@@ -87,6 +88,9 @@ public:
     std::vector<Pass> pass_c, pass_d;
     std::vector<BItem> items_c, items_d, items_copy;
     std::vector<Launch> launch_c, launch_d;
+    std::vector<uint32_t> item_of;           // tile -> item tables of every launch, back to back
+    uint64_t copy_map_off = 0;
+    uint32_t *d_item_of = nullptr;
     uint64_t copy_tiles = 0, framed_cap = 0;
     std::vector<unsigned long long> zero_c, zero_d;  // (ptr, bytes) pairs
     std::vector<std::pair<uint64_t, uint64_t>> hist_tables;  // (offset, cap) to initialise
@@ -296,7 +300,7 @@ void BatchEngine::plan_passes()
             add(h);
             BItem tk = h;
             tk.op = B_TOPK;
-            tk.tiles = 1;
+            tk.tiles = (uint32_t)nd.hist_tiles;  // one block per histogram tile
             add(tk);
             BItem sp = base_item(nd, B_SPLIT, nd.split_tiles);
             sp.order = (int16_t)native_order(nd.dt);
@@ -500,6 +504,8 @@ void BatchEngine::layout(cudaStream_t s)
                 j++;
             }
             L.count = (int)items.size() - L.first;
+            L.map_off = item_of.size();
+            for (int k = 0; k < L.count; k++) item_of.insert(item_of.end(), items[L.first + k].tiles, (uint32_t)k);
             launches.push_back(L);
             i = j;
         }
@@ -564,6 +570,8 @@ void BatchEngine::layout(cudaStream_t s)
             items_copy.push_back(it);
         }
     }
+    copy_map_off = item_of.size();
+    for (size_t k = 0; k < items_copy.size(); k++) item_of.insert(item_of.end(), items_copy[k].tiles, (uint32_t)k);
     // counters: one per launch
     n_counters = (int)(launch_c.size() + launch_d.size()) + 4;
 
@@ -588,6 +596,7 @@ void BatchEngine::layout(cudaStream_t s)
     const uint64_t o_frame = t_off; t_off += 256;
     const uint64_t o_status = t_off; t_off += 256;
     const uint64_t o_counters = t_off; t_off += sz(n_counters, 4);
+    const uint64_t o_item_of = t_off; t_off += sz(item_of.size(), 4);
     tables = dev_alloc(t_off, s);
     uint8_t *T = tables.get();
     GTSC_CUDA(cudaMemsetAsync(T, 0, t_off, s));
@@ -609,6 +618,7 @@ void BatchEngine::layout(cudaStream_t s)
     d_frame_len = (unsigned long long *)(T + o_frame + 8);
     d_status = (uint32_t *)(T + o_status);
     d_counters = (uint32_t *)(T + o_counters);
+    d_item_of = (uint32_t *)(T + o_item_of);
     // the status word and the counters are zeroed with the other ranges at each step
     zr(zero_c, (uint8_t *)d_status, 8);   // [0] error code, [1] decode: the frames did not parse
     zr(zero_d, (uint8_t *)d_status, 8);
@@ -626,6 +636,7 @@ void BatchEngine::layout(cudaStream_t s)
     h2d(d_nodes_d, nodes_d.data(), nodes_d.size() * sizeof(BNodeDev));
     h2d(d_zero_c, zero_c.data(), zero_c.size() * 8);
     h2d(d_zero_d, zero_d.data(), zero_d.size() * 8);
+    h2d(d_item_of, item_of.data(), item_of.size() * 4);
     GTSC_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -642,14 +653,16 @@ void BatchEngine::record_compress(cudaStream_t s, const std::function<void(int)>
     mark(M_ZERO);
     int ctr = 0;
     for (auto &L : launch_c) {
-        launch_batch_stage(L.op, d_items_c + L.first, L.count, L.tiles, d_streams, d_counters + ctr++, d_status, s);
+        launch_batch_stage(L.op, d_items_c + L.first, d_item_of + L.map_off, L.count, L.tiles, d_streams,
+                           d_counters + ctr++, d_status, s);
         mark(L.op);
     }
     launch_frame_sizes(d_cols, nc, d_nodes_c, d_streams, d_col_off, d_total, d_framed, s);
     mark(M_FRAME_SIZES);
     launch_frame_layout(d_cols, nc, d_nodes_c, d_streams, d_col_off, d_framed, s);
     mark(M_FRAME_LAYOUT);
-    launch_frame_copy(d_items_copy, (int)items_copy.size(), copy_tiles, d_nodes_c, d_streams, d_framed, s);
+    launch_frame_copy(d_items_copy, d_item_of + copy_map_off, (int)items_copy.size(), copy_tiles, d_nodes_c, d_streams,
+                      d_framed, s);
     mark(M_FRAME_COPY);
 }
 
@@ -666,7 +679,8 @@ void BatchEngine::record_decompress(cudaStream_t s, const std::function<void(int
     mark(M_PARSE);
     int ctr = (int)launch_c.size();
     for (auto &L : launch_d) {
-        launch_batch_stage(L.op, d_items_d + L.first, L.count, L.tiles, d_streams, d_counters + ctr++, d_status, s);
+        launch_batch_stage(L.op, d_items_d + L.first, d_item_of + L.map_off, L.count, L.tiles, d_streams,
+                           d_counters + ctr++, d_status, s);
         mark(L.op);
     }
 }

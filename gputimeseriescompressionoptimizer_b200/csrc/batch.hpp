@@ -81,8 +81,8 @@ void launch_frame_sizes(const BColumnDev *cols, int ncols, const BNodeDev *nodes
                         unsigned long long *col_off, unsigned long long *total, uint8_t *framed, cudaStream_t s);
 void launch_frame_layout(const BColumnDev *cols, int ncols, BNodeDev *nodes, const StreamDesc *S,
                          const unsigned long long *col_off, uint8_t *framed, cudaStream_t s);
-void launch_frame_copy(const BItem *items, int n_items, uint64_t total_tiles, const BNodeDev *nodes,
-                       const StreamDesc *S, uint8_t *framed, cudaStream_t s);
+void launch_frame_copy(const BItem *items, const uint32_t *item_of, int n_items, uint64_t total_tiles,
+                       const BNodeDev *nodes, const StreamDesc *S, uint8_t *framed, cudaStream_t s);
 void launch_parse_frames(const BColumnDev *cols, int ncols, const BNodeDev *nodes, StreamDesc *S,
                          unsigned long long *col_off, const uint8_t *const *framed_p,
                          const unsigned long long *framed_bytes_p, uint32_t *status, cudaStream_t s);
@@ -127,12 +127,14 @@ struct BatchLaunchProfile {
 };
 std::vector<BatchLaunchProfile> batch_profile(BatchEngine *e, bool compress, cudaStream_t s);
 
-// stage launcher (batch_kernels.cu / batch_decode.cu): one launch of `total_tiles` blocks
-void launch_batch_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,
-                        uint32_t *d_counter, uint32_t *d_status, cudaStream_t s);
+// stage launcher (batch_kernels.cu / batch_decode.cu): one launch of `total_tiles` blocks;
+// d_item_of[t] = the item (index into d_items) of tile t
+void launch_batch_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items, uint64_t total_tiles,
+                        StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status, cudaStream_t s);
 
 // tile sizes (elements) of the batched passes
-constexpr uint32_t kBTile = 2048;       // element-wise, look-back and pack passes
+constexpr uint32_t kBVPT = 16;         // values per thread of the element-wise and look-back passes
+constexpr uint32_t kBTile = 256 * kBVPT; // elements per tile of those passes (256 threads per block)
 constexpr uint32_t kBMinMaxTile = 8192;
 constexpr uint32_t kBHistTile = 16384;
 constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
@@ -143,11 +145,13 @@ struct BHistHdr {
     unsigned int used;      // slots taken in the global table
     unsigned int special;   // occurrences of the all-ones value
     unsigned int overflow;
-    unsigned int pad;
+    unsigned int pad;       // top-k: blocks finished
 };
+// header | keys (8 cap) | counts (4 cap) | used slots (4 cap) | NaN lists (32 per tile) | top-k
+// partials (96 per tile)
 inline uint64_t bhist_bytes(uint64_t cap, uint64_t tiles)
 {
-    return 16 + 8 * cap + 4 * cap + 4 * cap + 32 * tiles + 64;
+    return 16 + 8 * cap + 4 * cap + 4 * cap + 32 * tiles + 96 * tiles + 64;
 }
 
 }  // namespace gtsc

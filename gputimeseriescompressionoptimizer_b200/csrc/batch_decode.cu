@@ -83,11 +83,11 @@ __device__ void p_afl_unpack(const BItem &it, uint32_t tile, StreamDesc *S, uint
     const StreamReader rd{(const uint32_t *)(data.ptr - mis), data.len + mis};
     const uint64_t off_bits = 8 * mis;
     const uint64_t mask = b >= 64 ? ~0ull : ((1ull << b) - 1);
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     if (base >= n) return;
-    uint64_t v[8];
+    uint64_t v[kBVPT];
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         v[j] = 0;
         const uint64_t i = base + j;
         if (i >= n) continue;
@@ -105,16 +105,7 @@ __device__ void p_afl_unpack(const BItem &it, uint32_t tile, StreamDesc *S, uint
             v[j] = x & mask;
         }
     }
-    uint8_t *o = out.ptr;
-    if (base + 8 <= n && (8 * ES) % 16 == 0) {
-        constexpr int PER = 16 / ES;
-#pragma unroll
-        for (int c = 0; c < 8 / PER; c++)
-            reinterpret_cast<uint4 *>(o + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
-    } else {
-        for (int j = 0; j < 8; j++)
-            if (base + j < n) st_elem<ES>(o, base + j, v[j]);
-    }
+    store_run<ES, kBVPT>(out.ptr, base, n, v);
 }
 
 // ------------------------------------------------------------------------------- delta decode
@@ -133,14 +124,12 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     const uint64_t m = n ? n - 1 : 0;
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
-    uint64_t v[8];
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    uint64_t v[kBVPT];
+    load_run<ES, kBVPT>(d.ptr, base, m, v);
     unsigned long long local = 0;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-        v[j] = base + j < m ? ld_unaligned<ES>(d.ptr + (base + j) * ES) : 0;
-        local += v[j];
-    }
+    for (int j = 0; j < (int)kBVPT; j++) local += v[j];
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
     if (threadIdx.x < 32) {
@@ -150,21 +139,13 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     __syncthreads();
     if (base >= n) return;
     unsigned long long acc = ld_unaligned<ES>(meta.ptr) + s_prefix + excl;
-    uint64_t o[8];
+    uint64_t o[kBVPT];
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         o[j] = wrap_es(acc, ES);
         acc += v[j];
     }
-    if (base + 8 <= n && (8 * ES) % 16 == 0) {
-        constexpr int PER = 16 / ES;
-#pragma unroll
-        for (int c = 0; c < 8 / PER; c++)
-            reinterpret_cast<uint4 *>(out.ptr + (base + c * PER) * ES)[0] = make_chunk<ES>(o + c * PER);
-    } else {
-        for (int j = 0; j < 8; j++)
-            if (base + j < n) st_elem<ES>(out.ptr, base + j, o[j]);
-    }
+    store_run<ES, kBVPT>(out.ptr, base, n, o);
 }
 
 // ------------------------------------------------------------------------------- scale add
@@ -179,26 +160,19 @@ __device__ void p_scale_add(const BItem &it, uint32_t tile, StreamDesc *S, uint3
         return;
     }
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     if (base >= n) return;
     const uint64_t mn = ld_unaligned<ES>(meta.ptr);
-    uint64_t v[8];
+    uint64_t v[kBVPT];
+    load_run<ES, kBVPT>(d.ptr, base, n, v);
 #pragma unroll
-    for (int j = 0; j < 8; j++) v[j] = base + j < n ? wrap_es(ld_unaligned<ES>(d.ptr + (base + j) * ES) + mn, ES) : 0;
-    if (base + 8 <= n && (8 * ES) % 16 == 0) {
-        constexpr int PER = 16 / ES;
-#pragma unroll
-        for (int c = 0; c < 8 / PER; c++)
-            reinterpret_cast<uint4 *>(out.ptr + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
-    } else {
-        for (int j = 0; j < 8; j++)
-            if (base + j < n) st_elem<ES>(out.ptr, base + j, v[j]);
-    }
+    for (int j = 0; j < (int)kBVPT; j++) v[j] = wrap_es(v[j] + mn, ES);
+    store_run<ES, kBVPT>(out.ptr, base, n, v);
 }
 
 // ------------------------------------------------------------------------------- merge
 template <int ES>
-__device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+__device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, uint8_t *sm)
 {
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
@@ -248,9 +222,13 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
         yes_cap = in1.len / ES;
     }
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
-    const uint32_t valid_mask = base >= n ? 0u : (n - base >= 8 ? 0xffu : ((1u << (n - base)) - 1));
-    const uint32_t bits = base < n ? ((uint32_t)stencil[1 + base / 8] & valid_mask) : 0u;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    const uint32_t valid_mask = base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
+    uint32_t bits = 0;
+#pragma unroll
+    for (int q = 0; q < (int)kBVPT / 8; q++)
+        if (base + 8 * q < n) bits |= (uint32_t)stencil[1 + base / 8 + q] << (8 * q);
+    bits &= valid_mask;
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(bits), ws, total);
     if (threadIdx.x < 32) {
@@ -258,40 +236,57 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
         if (threadIdx.x == 0) s_prefix = e;
     }
     __syncthreads();
-    if (base >= n) return;
-    uint64_t yes_pos = s_prefix + excl, no_pos = base - yes_pos;
-    uint64_t v[8];
+    // the tile's runs of both streams are staged in shared memory with coalesced loads (matches
+    // first, then the rest), then every thread assembles its values from there
+    const uint64_t tile_base = (uint64_t)tile * kBTile;
+    const uint64_t tile_n = tile_base < n ? (n - tile_base < kBTile ? n - tile_base : kBTile) : 0;
+    const uint64_t ny = total, nn = tile_n - ny;
+    const uint64_t yes0 = s_prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
     bool bad = false;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-        v[j] = 0;
-        if (!((valid_mask >> j) & 1u)) continue;
-        if ((bits >> j) & 1u) {
-            if (yes_pos >= yes_cap) bad = true;
-            else if (mode == SPLIT_DICT) {
-                const uint32_t w = (uint32_t)ld_unaligned<4>(codes + 4 * (yes_pos >> 4));
-                v[j] = top[(w >> (2 * (yes_pos & 15))) & 3u];
-            } else {
-                v[j] = ld_unaligned<ES>(in1.ptr + yes_pos * ES);
-            }
-            ++yes_pos;
-        } else {
-            if (mode == SPLIT_NOT_CONST) v[j] = top[0];
-            else if (no_pos >= no_cap) bad = true;
-            else v[j] = ld_unaligned<ES>(in2.ptr + no_pos * ES);
-            ++no_pos;
+    if (mode != SPLIT_DICT) {
+        const bool al = ((uintptr_t)in1.ptr & (ES - 1)) == 0;
+        for (uint64_t i = threadIdx.x; i < ny; i += kBThreads) {
+            if (yes0 + i < yes_cap) st_elem<ES>(sm, i, ld_elem_any<ES>(in1.ptr, yes0 + i, al));
+            else bad = true;
         }
     }
-    if (bad) set_status(status, GTSC_ERR_FORMAT);
-    if (base + 8 <= n && (8 * ES) % 16 == 0) {
-        constexpr int PER = 16 / ES;
-#pragma unroll
-        for (int c = 0; c < 8 / PER; c++)
-            reinterpret_cast<uint4 *>(out.ptr + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
-    } else {
-        for (int j = 0; j < 8; j++)
-            if (base + j < n) st_elem<ES>(out.ptr, base + j, v[j]);
+    if (mode != SPLIT_NOT_CONST) {
+        const bool al = ((uintptr_t)in2.ptr & (ES - 1)) == 0;
+        for (uint64_t i = threadIdx.x; i < nn; i += kBThreads) {
+            if (no0 + i < no_cap) st_elem<ES>(sm, ny + i, ld_elem_any<ES>(in2.ptr, no0 + i, al));
+            else bad = true;
+        }
     }
+    __syncthreads();
+    if (base < n) {
+        uint64_t ly = excl, ln = (uint64_t)threadIdx.x * kBVPT - excl;
+        uint64_t v[kBVPT];
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++) {
+            v[j] = 0;
+            if (!((valid_mask >> j) & 1u)) continue;
+            if ((bits >> j) & 1u) {
+                if (mode == SPLIT_DICT) {
+                    const uint64_t y = yes0 + ly;
+                    if (y >= yes_cap) {
+                        bad = true;
+                    } else {
+                        const uint32_t w = (uint32_t)ld_unaligned<4>(codes + 4 * (y >> 4));
+                        v[j] = top[(w >> (2 * (y & 15))) & 3u];
+                    }
+                } else if (ly < ny) {
+                    v[j] = ld_elem_sm<ES>(sm, ly);
+                }
+                ++ly;
+            } else {
+                if (mode == SPLIT_NOT_CONST) v[j] = top[0];
+                else v[j] = ld_elem_sm<ES>(sm, ny + ln);
+                ++ln;
+            }
+        }
+        store_run<ES, kBVPT>(out.ptr, base, n, v);
+    }
+    if (bad) set_status(status, GTSC_ERR_FORMAT);
 }
 
 // ------------------------------------------------------------------------------- RLE decode
@@ -311,12 +306,12 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
     }
     unsigned long long *ends = (unsigned long long *)(it.scratch + it.p[1]);
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
-    long long v[8];
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    long long v[kBVPT];
     unsigned long long local = 0;
     bool neg = false;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         v[j] = base + j < (uint64_t)runs ? (long long)(int32_t)ld_unaligned<4>(lengths.ptr + 4 * (base + j)) : 0;
         neg |= v[j] < 0;
         local += (unsigned long long)v[j];
@@ -331,7 +326,7 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
     __syncthreads();
     unsigned long long acc = s_prefix + excl;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         acc += (unsigned long long)v[j];
         if (base + j < (uint64_t)runs) ends[base + j] = acc;
     }
@@ -370,25 +365,18 @@ __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint
         s_hi = hi < runs ? hi + 1 : runs;
     }
     __syncthreads();
-    const uint64_t base = t0 + (uint64_t)threadIdx.x * 8;
+    const uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT;
     if (base >= n) return;
+    const bool val_al = ((uintptr_t)values.ptr & (ES - 1)) == 0;
     uint64_t r = ub(s_lo, s_hi, base);
-    uint64_t v[8];
+    uint64_t v[kBVPT];
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         const uint64_t i = base + j;
         while (r < runs && ends[r] <= i) ++r;
-        v[j] = (i < n && r < runs) ? ld_unaligned<ES>(values.ptr + r * ES) : 0;
+        v[j] = (i < n && r < runs) ? ld_elem_any<ES>(values.ptr, r, val_al) : 0;
     }
-    if (base + 8 <= n && (8 * ES) % 16 == 0) {
-        constexpr int PER = 16 / ES;
-#pragma unroll
-        for (int c = 0; c < 8 / PER; c++)
-            reinterpret_cast<uint4 *>(out.ptr + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
-    } else {
-        for (int j = 0; j < 8; j++)
-            if (base + j < n) st_elem<ES>(out.ptr, base + j, v[j]);
-    }
+    store_run<ES, kBVPT>(out.ptr, base, n, v);
     (void)status;
 }
 
@@ -420,18 +408,19 @@ __device__ void p_f2i_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
         return;
     }
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     const Order o = (Order)it.order;
-    for (int j = 0; j < 8 && base + j < n; j++) {
+    const bool d_al = ((uintptr_t)d.ptr & 3) == 0;
+    for (int j = 0; j < (int)kBVPT && base + j < n; j++) {
         uint64_t v;
         if (p < 10) {
-            const int k = (int32_t)ld_unaligned<4>(d.ptr + 4 * (base + j));
+            const int k = (int32_t)ld_elem_any<4>(d.ptr, base + j, d_al);
             if (o == ORD_F32) v = __float_as_uint(__double2float_rn(__ddiv_rn((double)__int2float_rn(k), p10[p])));
             else if (o == ORD_F64) v = (uint64_t)__double_as_longlong(__ddiv_rn((double)k, p10[p]));
             else if (ES == 8) v = (uint64_t)__double2ll_rz(__ddiv_rn((double)k, p10[p]));
             else v = (uint64_t)(long long)__double2int_rz(__ddiv_rn((double)sext((uint64_t)(long long)k, ES), p10[p]));
         } else {
-            v = ld_unaligned<ES>(d.ptr + (base + j) * ES);
+            v = ld_elem_any<ES>(d.ptr, base + j, ((uintptr_t)d.ptr & (ES - 1)) == 0);
         }
         st_elem<ES>(out.ptr, base + j, v);
     }
@@ -550,14 +539,15 @@ __device__ __forceinline__ void parse_fail(uint32_t *status)
 }
 
 template <int OP>
-__global__ void __launch_bounds__(kBThreads)
-k_bdec(const BItem *items, int n_items, StreamDesc *S, uint32_t *counter, uint32_t *status)
+__global__ void __launch_bounds__(kBThreads, 3)
+k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status)
 {
     constexpr bool DYN = OP == B_DELTA_DEC || OP == B_MERGE || OP == B_RLE_SCAN;
+    __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : 16];
     if (*(volatile uint32_t *)(status + 1)) return;
     BItem it;
     uint32_t tile;
-    locate<DYN>(items, n_items, counter, it, tile);
+    locate<DYN>(items, item_of, counter, it, tile);
     if (tile >= it.tiles) return;
 #define GTSC_ES_SWITCH(CALL)                       \
     switch (it.es) {                               \
@@ -570,7 +560,7 @@ k_bdec(const BItem *items, int n_items, StreamDesc *S, uint32_t *counter, uint32
     else if constexpr (OP == B_AFL_UNPACK) { GTSC_ES_SWITCH(p_afl_unpack<E>(it, tile, S, status)) }
     else if constexpr (OP == B_DELTA_DEC) { GTSC_ES_SWITCH(p_delta_dec<E>(it, tile, S, status)) }
     else if constexpr (OP == B_SCALE_ADD) { GTSC_ES_SWITCH(p_scale_add<E>(it, tile, S, status)) }
-    else if constexpr (OP == B_MERGE) { GTSC_ES_SWITCH(p_merge<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_MERGE) { GTSC_ES_SWITCH(p_merge<E>(it, tile, S, status, smem)) }
     else if constexpr (OP == B_RLE_SCAN) p_rle_scan(it, tile, S, status);
     else if constexpr (OP == B_RLE_EXPAND) { GTSC_ES_SWITCH(p_rle_expand<E>(it, tile, S, status)) }
     else if constexpr (OP == B_F2I_DEC) { GTSC_ES_SWITCH(p_f2i_dec<E>(it, tile, S, status)) }
@@ -650,11 +640,11 @@ __global__ void k_frame_layout(const BColumnDev *cols, int ncols, BNodeDev *node
 
 // copy items: p[0] = node table index, p[1] = 0 copy the node's metadata, 1 its data
 __global__ void __launch_bounds__(kBThreads)
-k_frame_copy(const BItem *items, int n_items, const BNodeDev *nodes, const StreamDesc *S, uint8_t *framed)
+k_frame_copy(const BItem *items, const uint32_t *item_of, const BNodeDev *nodes, const StreamDesc *S, uint8_t *framed)
 {
     BItem it;
     uint32_t tile;
-    locate<false>(items, n_items, nullptr, it, tile);
+    locate<false>(items, item_of, nullptr, it, tile);
     const BNodeDev &nd = nodes[it.p[0]];
     const StreamDesc src = S[it.p[1] ? nd.data : nd.meta];
     const uint64_t dst = it.p[1] ? nd.data_dst : nd.meta_dst;
@@ -749,15 +739,16 @@ __global__ void k_zero_ranges(const unsigned long long *ranges, int n)
 
 }  // namespace
 
-void launch_batch_decode_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,
-                               uint32_t *d_counter, uint32_t *d_status, cudaStream_t s)
+void launch_batch_decode_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items,
+                               uint64_t total_tiles, StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status,
+                               cudaStream_t s)
 {
     if (n_items == 0 || total_tiles == 0) return;
     if (total_tiles > 0x7fffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles in one stage");
     const unsigned g = (unsigned)total_tiles;
     switch (op) {
 #define GTSC_STAGE(OPC) \
-    case OPC: k_bdec<OPC><<<g, kBThreads, 0, s>>>(d_items, n_items, d_streams, d_counter, d_status); break;
+    case OPC: k_bdec<OPC><<<g, kBThreads, 0, s>>>(d_items, d_item_of, d_streams, d_counter, d_status); break;
         GTSC_STAGE(B_NONE_COPY)
         GTSC_STAGE(B_AFL_UNPACK)
         GTSC_STAGE(B_DELTA_DEC)
@@ -790,11 +781,11 @@ void launch_frame_layout(const BColumnDev *cols, int ncols, BNodeDev *nodes, con
     GTSC_CUDA(cudaGetLastError());
 }
 
-void launch_frame_copy(const BItem *items, int n_items, uint64_t total_tiles, const BNodeDev *nodes,
-                       const StreamDesc *S, uint8_t *framed, cudaStream_t s)
+void launch_frame_copy(const BItem *items, const uint32_t *item_of, int n_items, uint64_t total_tiles,
+                       const BNodeDev *nodes, const StreamDesc *S, uint8_t *framed, cudaStream_t s)
 {
     if (!n_items || !total_tiles) return;
-    k_frame_copy<<<(unsigned)total_tiles, kBThreads, 0, s>>>(items, n_items, nodes, S, framed);
+    k_frame_copy<<<(unsigned)total_tiles, kBThreads, 0, s>>>(items, item_of, nodes, S, framed);
     GTSC_CUDA(cudaGetLastError());
 }
 

@@ -9,6 +9,65 @@
 namespace gtsc {
 
 constexpr int kBThreads = 256;
+static_assert(kBTile == kBThreads * kBVPT, "tile = threads x values per thread");
+
+// Loads elements [base, base + VPT) of a stream (zeros past n): 16-byte vector loads when the
+// whole run is in range and the stream is 16-byte aligned, else element loads (byte loads when
+// the stream is not even element aligned, as streams inside a blob may be).
+template <int ES, int VPT>
+__device__ __forceinline__ void load_run(const uint8_t *p, uint64_t base, uint64_t n, uint64_t (&v)[VPT])
+{
+    if (base + VPT <= n && ((uintptr_t)p & 15) == 0) {
+        constexpr int PER = 16 / ES;
+        static_assert(VPT % PER == 0, "a run is whole 16-byte chunks");
+#pragma unroll
+        for (int c = 0; c < VPT / PER; c++) {
+            const uint4 q = ld_chunk(p + (base + (uint64_t)c * PER) * ES);
+#pragma unroll
+            for (int j = 0; j < PER; j++) v[c * PER + j] = chunk_elem<ES>(q, j);
+        }
+    } else if (((uintptr_t)p & (ES - 1)) == 0) {
+#pragma unroll
+        for (int j = 0; j < VPT; j++) v[j] = base + j < n ? ld_elem<ES>(p, base + j) : 0;
+    } else {
+#pragma unroll
+        for (int j = 0; j < VPT; j++) v[j] = base + j < n ? ld_unaligned<ES>(p + (base + j) * ES) : 0;
+    }
+}
+
+// element i of a shared-memory array of ES-byte elements
+template <int ES>
+__device__ __forceinline__ uint64_t ld_elem_sm(const uint8_t *sm, uint64_t i)
+{
+    if (ES == 1) return sm[i];
+    if (ES == 2) return ((const uint16_t *)sm)[i];
+    if (ES == 4) return ((const uint32_t *)sm)[i];
+    return ((const unsigned long long *)sm)[i];
+}
+
+// element i of a stream that may not be element aligned (streams inside a blob)
+template <int ES>
+__device__ __forceinline__ uint64_t ld_elem_any(const uint8_t *p, uint64_t i, bool aligned)
+{
+    return aligned ? ld_elem<ES>(p, i) : ld_unaligned<ES>(p + i * ES);
+}
+
+// Stores elements [base, min(base + VPT, n)) to an element-aligned stream (16-byte stores when the
+// whole run is in range and the stream is 16-byte aligned).
+template <int ES, int VPT>
+__device__ __forceinline__ void store_run(uint8_t *p, uint64_t base, uint64_t n, const uint64_t (&v)[VPT])
+{
+    if (base + VPT <= n && ((uintptr_t)p & 15) == 0) {
+        constexpr int PER = 16 / ES;
+#pragma unroll
+        for (int c = 0; c < VPT / PER; c++)
+            reinterpret_cast<uint4 *>(p + (base + (uint64_t)c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
+    } else {
+#pragma unroll
+        for (int j = 0; j < VPT; j++)
+            if (base + j < n) st_elem<ES>(p, base + j, v[j]);
+    }
+}
 
 __device__ __forceinline__ void set_status(uint32_t *status, gtsc_status code)
 {
@@ -155,22 +214,20 @@ __device__ __forceinline__ uint64_t d_gfc_cut(const DGfc &g, int64_t i)
 __device__ __forceinline__ uint64_t d_gfc_begin(const DGfc &g, int64_t w) { return w ? d_gfc_cut(g, w - 1) : 0; }
 __device__ __forceinline__ uint64_t d_gfc_start(const DGfc &g, int64_t w) { return (d_gfc_begin(g, w) + 1) / 2 * (uint64_t)g.unit; }
 
-// the stage kernel skeleton: finds this block's (item, tile)
+// the stage kernel skeleton: finds this block's (item, tile).  DYN passes take tiles in claim
+// order from a counter (look-back needs every predecessor claimed first), the others use the
+// block index; item_of[t] is the item of global tile t (one table per launch).
 template <bool DYN>
-__device__ __forceinline__ void locate(const BItem *items, int n_items, uint32_t *counter, BItem &it, uint32_t &tile)
+__device__ __forceinline__ void locate(const BItem *items, const uint32_t *item_of, uint32_t *counter, BItem &it,
+                                       uint32_t &tile)
 {
     __shared__ uint32_t s_tile;
-    __shared__ int s_idx;
+    __shared__ uint32_t s_idx;
     if (threadIdx.x == 0) {
-        const uint64_t t = DYN ? (uint64_t)atomicAdd(counter, 1u) : (uint64_t)blockIdx.x;
-        int lo = 0, hi = n_items - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (items[mid].tile_base <= t) lo = mid;
-            else hi = mid - 1;
-        }
-        s_idx = lo;
-        s_tile = (uint32_t)(t - items[lo].tile_base);
+        const uint32_t t = DYN ? atomicAdd(counter, 1u) : blockIdx.x;
+        const uint32_t idx = item_of[t];
+        s_idx = idx;
+        s_tile = (uint32_t)(t - items[idx].tile_base);
     }
     __syncthreads();
     it = items[s_idx];

@@ -73,24 +73,16 @@ __device__ void p_delta_enc(const BItem &it, uint32_t tile, StreamDesc *S)
         }
     }
     const uint64_t m = n ? n - 1 : 0;
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     if (base >= m) return;
-    uint8_t *out = S[it.out[1]].ptr;
-    uint64_t v[9];
+    uint64_t v[kBVPT];
+    load_run<ES, kBVPT>(in.ptr, base, n, v);
+    const uint64_t next = base + kBVPT < n ? ld_elem<ES>(in.ptr, base + kBVPT) : 0;
+    uint64_t d[kBVPT];
 #pragma unroll
-    for (int j = 0; j < 9; j++) v[j] = base + j < n ? ld_elem<ES>(in.ptr, base + j) : 0;
-    uint64_t d[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) d[j] = wrap_es(v[j + 1] - v[j], ES);
-    if (base + 8 <= m && (8 * ES) % 16 == 0) {
-        constexpr int PER = 16 / ES;
-#pragma unroll
-        for (int c = 0; c < 8 / PER; c++)
-            reinterpret_cast<uint4 *>(out + (base + c * PER) * ES)[0] = make_chunk<ES>(d + c * PER);
-    } else {
-        for (int j = 0; j < 8; j++)
-            if (base + j < m) st_elem<ES>(out, base + j, d[j]);
-    }
+    for (int j = 0; j + 1 < (int)kBVPT; j++) d[j] = wrap_es(v[j + 1] - v[j], ES);
+    d[kBVPT - 1] = wrap_es(next - v[kBVPT - 1], ES);
+    store_run<ES, kBVPT>(S[it.out[1]].ptr, base, m, d);
 }
 
 // ------------------------------------------------------------------------------- scale
@@ -111,21 +103,13 @@ __device__ void p_scale_sub(const BItem &it, uint32_t tile, StreamDesc *S)
         }
         S[it.out[1]].len = n * ES;
     }
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     if (base >= n) return;
-    uint8_t *out = S[it.out[1]].ptr;
-    uint64_t v[8];
+    uint64_t v[kBVPT];
+    load_run<ES, kBVPT>(in.ptr, base, n, v);
 #pragma unroll
-    for (int j = 0; j < 8; j++) v[j] = base + j < n ? wrap_es(ld_elem<ES>(in.ptr, base + j) - mn, ES) : 0;
-    if (base + 8 <= n && (8 * ES) % 16 == 0) {
-        constexpr int PER = 16 / ES;
-#pragma unroll
-        for (int c = 0; c < 8 / PER; c++)
-            reinterpret_cast<uint4 *>(out + (base + c * PER) * ES)[0] = make_chunk<ES>(v + c * PER);
-    } else {
-        for (int j = 0; j < 8; j++)
-            if (base + j < n) st_elem<ES>(out, base + j, v[j]);
-    }
+    for (int j = 0; j < (int)kBVPT; j++) v[j] = wrap_es(v[j] - mn, ES);
+    store_run<ES, kBVPT>(S[it.out[1]].ptr, base, n, v);
 }
 
 // ------------------------------------------------------------------------------- AFL pack
@@ -213,7 +197,8 @@ struct HTab {
     unsigned long long *keys;
     unsigned int *counts;
     unsigned int *used;
-    unsigned long long *nan;
+    unsigned long long *nan;   // 4 per histogram tile
+    unsigned long long *part;  // top-k partials: 4 x (key, bits, count) per histogram tile
     uint64_t cap;
 };
 __device__ __forceinline__ HTab htab(const BItem &it)
@@ -227,6 +212,7 @@ __device__ __forceinline__ HTab htab(const BItem &it)
     t.counts = (unsigned int *)(b + 16 + 8 * t.cap);
     t.used = (unsigned int *)(b + 16 + 12 * t.cap);
     t.nan = (unsigned long long *)(b + 16 + 16 * t.cap);
+    t.part = t.nan + 4 * it.p[1];
     return t;
 }
 
@@ -355,27 +341,12 @@ __device__ __forceinline__ void cpush(Cand *l, const Cand &c)
         if (cbetter(l[i], l[i - 1])) { const Cand x = l[i]; l[i] = l[i - 1]; l[i - 1] = x; }
 }
 
-// one block per item: the k most frequent values, then the table is cleared for the next step
-template <int ES>
-__device__ void p_topk(const BItem &it, StreamDesc *S, unsigned char *smem)
+// The k most frequent values of an item, then the table is cleared for the next step.  The item's
+// blocks (one per histogram tile) each take a slice of the used-slot list (and of the NaN lists),
+// reduce it to a top-4, clear their slots and write the top-4 to the partial list; the last block
+// to finish (threadfence + counter) merges the partials, writes the result and resets the header.
+__device__ __forceinline__ void topk_block_reduce(Cand *l, Cand *sc)
 {
-    constexpr unsigned long long EMPTY = ~0ull;
-    Cand *sc = (Cand *)smem;
-    const HTab t = htab(it);
-    const Order o = (Order)it.order;
-    const unsigned int used = t.hdr->used;
-    Cand l[4];
-    for (int j = 0; j < 4; j++) l[j] = Cand{EMPTY, 0, 0};
-    for (unsigned int i = threadIdx.x; i < used; i += kBThreads) {
-        const unsigned int h = t.used[i];
-        const unsigned long long k = t.keys[h];
-        cpush(l, Cand{order_key(k, ES, o), k, t.counts[h]});
-    }
-    if (threadIdx.x == 0 && t.hdr->special) cpush(l, Cand{order_key(EMPTY, ES, o), EMPTY, t.hdr->special});
-    for (uint64_t i = threadIdx.x; i < 4 * it.p[1]; i += kBThreads) {
-        const unsigned long long k = t.nan[i];
-        if (k != EMPTY) cpush(l, Cand{k, order_unkey(k, ES, o), 1u});
-    }
     for (int j = 0; j < 4; j++) sc[threadIdx.x * 4 + j] = l[j];
     __syncthreads();
     for (int width = kBThreads / 2; width > 0; width >>= 1) {
@@ -386,27 +357,74 @@ __device__ void p_topk(const BItem &it, StreamDesc *S, unsigned char *smem)
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        const int k = it.mode;  // 1: const -> meta[0..es), 4: dict -> out1[16 ..)
-        uint8_t *dst = k == 1 ? S[it.out[0]].ptr : S[it.out[1]].ptr + 16;
-        for (int j = 0; j < k; j++) st_elem<ES>(dst, j, sc[j].count ? sc[j].bits : 0ull);
+}
+
+template <int ES>
+__device__ void p_topk(const BItem &it, uint32_t tile, StreamDesc *S, unsigned char *smem)
+{
+    constexpr unsigned long long EMPTY = ~0ull;
+    __shared__ bool s_last;
+    Cand *sc = (Cand *)smem;
+    const HTab t = htab(it);
+    const Order o = (Order)it.order;
+    const uint32_t T = it.tiles;
+    const unsigned int used = t.hdr->used;
+    const uint64_t slice = (used + T - 1) / T;
+    const uint64_t lo = (uint64_t)tile * slice, hi = lo + slice < used ? lo + slice : used;
+    const uint64_t nan_n = 4 * it.p[1], nslice = (nan_n + T - 1) / T;
+    const uint64_t nlo = (uint64_t)tile * nslice, nhi = nlo + nslice < nan_n ? nlo + nslice : nan_n;
+    Cand l[4];
+    for (int j = 0; j < 4; j++) l[j] = Cand{EMPTY, 0, 0};
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += kBThreads) {
+        const unsigned int h = t.used[i];
+        const unsigned long long k = t.keys[h];
+        cpush(l, Cand{order_key(k, ES, o), k, t.counts[h]});
     }
-    __syncthreads();
-    for (unsigned int i = threadIdx.x; i < used; i += kBThreads) {
+    if (tile == 0 && threadIdx.x == 0 && t.hdr->special) cpush(l, Cand{order_key(EMPTY, ES, o), EMPTY, t.hdr->special});
+    for (uint64_t i = nlo + threadIdx.x; i < nhi; i += kBThreads) {
+        const unsigned long long k = t.nan[i];
+        if (k != EMPTY) cpush(l, Cand{k, order_unkey(k, ES, o), 1u});
+    }
+    topk_block_reduce(l, sc);
+    // clear this slice of the table for the next step
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += kBThreads) {
         const unsigned int h = t.used[i];
         t.keys[h] = EMPTY;
         t.counts[h] = 0;
     }
+    unsigned long long *part = t.part + (uint64_t)tile * 12;
+    if (threadIdx.x < 4) {
+        part[3 * threadIdx.x] = sc[threadIdx.x].key;
+        part[3 * threadIdx.x + 1] = sc[threadIdx.x].bits;
+        part[3 * threadIdx.x + 2] = sc[threadIdx.x].count;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&t.hdr->pad, 1u) == T - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int j = 0; j < 4; j++) l[j] = Cand{EMPTY, 0, 0};
+    for (uint64_t i = threadIdx.x; i < 4ull * T; i += kBThreads) {
+        const volatile unsigned long long *q = t.part + 3 * i;
+        cpush(l, Cand{q[0], q[1], (unsigned int)q[2]});
+    }
+    __syncthreads();
+    topk_block_reduce(l, sc);
     if (threadIdx.x == 0) {
+        const int k = it.mode;  // 1: const -> meta[0..es), 4: dict -> out1[16 ..)
+        uint8_t *dst = k == 1 ? S[it.out[0]].ptr : S[it.out[1]].ptr + 16;
+        for (int j = 0; j < k; j++) st_elem<ES>(dst, j, sc[j].count ? sc[j].bits : 0ull);
         t.hdr->used = 0;
         t.hdr->special = 0;
         t.hdr->overflow = 0;
+        t.hdr->pad = 0;
     }
 }
 
 // ------------------------------------------------------------------------------- split
 template <int ES>
-__device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+__device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, unsigned char *sm)
 {
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
@@ -437,13 +455,12 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
             if (mode != SPLIT_NOT_CONST) S[it.out[2]].len = 0;
         }
     }
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
-    uint64_t v[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) v[j] = base + j < n ? ld_elem<ES>(in.ptr, base + j) : 0;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    uint64_t v[kBVPT];
+    load_run<ES, kBVPT>(in.ptr, base, n, v);
     uint32_t bits = 0, codes = 0;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         bool f = false;
         uint32_t code = 0;
         if (mode == SPLIT_LOWER) f = lt_native(v[j], thr, ES, o);
@@ -458,13 +475,15 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     }
     if (base < n) {
         const uint64_t valid = n - base;
-        if (valid < 8) {
+        if (valid < kBVPT) {  // Stencil::pack's index clamp: the last element fills the last byte
             const uint32_t last = (bits >> (valid - 1)) & 1u;
-            for (int j = (int)valid; j < 8; j++) bits = (bits & ~(1u << j)) | (last << j);
+            for (int j = (int)valid; j < (int)kBVPT; j++) bits = (bits & ~(1u << j)) | (last << j);
         }
-        stencil[base / 8] = (uint8_t)bits;
+#pragma unroll
+        for (int q = 0; q < (int)kBVPT / 8; q++)
+            if (base + 8 * q < n) stencil[base / 8 + q] = (uint8_t)(bits >> (8 * q));
     }
-    const uint32_t valid_mask = base >= n ? 0u : (n - base >= 8 ? 0xffu : ((1u << (n - base)) - 1));
+    const uint32_t valid_mask = base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
     const uint32_t yes_bits = bits & valid_mask;
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(yes_bits), ws, total);
@@ -473,28 +492,57 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
         if (threadIdx.x == 0) s_prefix = e;
     }
     __syncthreads();
-    uint64_t yes_pos = s_prefix + excl;
-    uint64_t no_pos = (base < n ? base : n) - yes_pos;
-    uint8_t *yes = S[it.out[1]].ptr;
-    uint8_t *no = mode == SPLIT_NOT_CONST ? nullptr : S[it.out[2]].ptr;
-    uint32_t *words = mode == SPLIT_DICT ? (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES) : nullptr;
-    for (int j = 0; j < 8; j++) {
+    // the tile's values go to shared memory in output order (matches first, then the rest), then
+    // the block writes both runs with coalesced stores
+    const uint64_t tile_base = (uint64_t)tile * kBTile;
+    const uint64_t tile_n = tile_base < n ? (n - tile_base < kBTile ? n - tile_base : kBTile) : 0;
+    const uint64_t ny = total, nn = tile_n - ny;
+    const uint64_t yes0 = s_prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
+    uint64_t ly = excl, ln = (uint64_t)threadIdx.x * kBVPT - excl;
+#pragma unroll
+    for (int j = 0; j < (int)kBVPT; j++) {
         if (!((valid_mask >> j) & 1u)) break;
         if ((yes_bits >> j) & 1u) {
-            if (mode == SPLIT_DICT) {
-                const uint32_t c = (codes >> (2 * j)) & 3u;
-                if (c) atomicOr(words + (yes_pos >> 4), c << (2 * (yes_pos & 15)));
-            } else {
-                st_elem<ES>(yes, yes_pos, v[j]);
-            }
-            ++yes_pos;
+            if (mode != SPLIT_DICT) st_elem<ES>(sm, ly, v[j]);
+            ++ly;
         } else {
-            if (mode != SPLIT_NOT_CONST) st_elem<ES>(no, no_pos, v[j]);
-            ++no_pos;
+            st_elem<ES>(sm, ny + ln, v[j]);
+            ++ln;
         }
     }
-    if (base < n && base + 8 >= n) {  // the thread holding the last element: lengths and headers
-        const uint64_t m = yes_pos;
+    if (mode == SPLIT_DICT) {
+        // 2-bit codes of this thread's matches: at most two code words; a word wholly inside the
+        // thread's range is stored, a shared one is merged with atomicOr (the words start zeroed)
+        uint32_t *words = (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES);
+        const uint64_t y0 = yes0 + excl, y1 = y0 + __popc(yes_bits);
+        uint32_t acc[2] = {0u, 0u};
+        uint64_t y = y0;
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++)
+            if ((yes_bits >> j) & 1u) {
+                acc[(y >> 4) - (y0 >> 4)] |= ((codes >> (2 * j)) & 3u) << (2 * (y & 15));
+                ++y;
+            }
+        if (y1 > y0) {
+            for (uint64_t w = y0 >> 4; w <= (y1 - 1) >> 4; w++) {
+                const uint32_t a = acc[w - (y0 >> 4)];
+                if (16 * w >= y0 && 16 * w + 16 <= y1) words[w] = a;
+                else if (a) atomicOr(words + w, a);
+            }
+        }
+    }
+    __syncthreads();
+    if (mode != SPLIT_DICT) {
+        uint8_t *yes = S[it.out[1]].ptr;
+        for (uint64_t i = threadIdx.x; i < ny; i += kBThreads) st_elem<ES>(yes, yes0 + i, ld_elem_sm<ES>(sm, i));
+    }
+    if (mode != SPLIT_NOT_CONST) {
+        uint8_t *no = S[it.out[2]].ptr;
+        for (uint64_t i = threadIdx.x; i < nn; i += kBThreads) st_elem<ES>(no, no0 + i, ld_elem_sm<ES>(sm, ny + i));
+    }
+    const uint64_t yes_pos = yes0 + ny;
+    if (base < n && base + kBVPT >= n) {  // the thread holding the last element: lengths and headers
+        const uint64_t m = yes_pos;  // this is the last tile: its matches end the match stream
         if (mode == SPLIT_LOWER) {
             S[it.out[0]].len = 1 + (n + 7) / 8;
             S[it.out[1]].len = m * ES;
@@ -534,16 +582,15 @@ __device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
         }
         return;
     }
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
-    uint64_t v[9];
-    v[0] = base > 0 && base - 1 < n ? ld_elem<ES>(in.ptr, base - 1) : 0;
-#pragma unroll
-    for (int j = 0; j < 8; j++) v[j + 1] = base + j < n ? ld_elem<ES>(in.ptr, base + j) : 0;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    uint64_t v[kBVPT];
+    load_run<ES, kBVPT>(in.ptr, base, n, v);
+    const uint64_t prev = base > 0 && base - 1 < n ? ld_elem<ES>(in.ptr, base - 1) : 0;
     uint32_t heads = 0;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         const uint64_t i = base + j;
-        if (i < n && (i == 0 || !bsame(v[j + 1], v[j], o))) heads |= 1u << j;
+        if (i < n && (i == 0 || !bsame(v[j], j ? v[j - 1] : prev, o))) heads |= 1u << j;
     }
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(heads), ws, total);
@@ -554,13 +601,14 @@ __device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
     __syncthreads();
     uint64_t r = s_prefix + excl;
     uint8_t *values = S[it.out[2]].ptr;
-    for (int j = 0; j < 8; j++)
+#pragma unroll
+    for (int j = 0; j < (int)kBVPT; j++)
         if ((heads >> j) & 1u) {
-            st_elem<ES>(values, r, v[j + 1]);
+            st_elem<ES>(values, r, v[j]);
             starts[r] = (uint32_t)(base + j);
             ++r;
         }
-    if (base < n && base + 8 >= n) {
+    if (base < n && base + kBVPT >= n) {
         *(int32_t *)S[it.out[0]].ptr = (int32_t)r;
         S[it.out[0]].len = 4;
         S[it.out[1]].len = 4 * r;
@@ -710,14 +758,14 @@ __device__ void p_f2i_enc(const BItem &it, uint32_t tile, StreamDesc *S)
             S[it.out[1]].len = 0;
         }
     }
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     if (base >= n) return;
     uint8_t *out = S[it.out[1]].ptr;
     if (transform) {
         const Order o = (Order)it.order;
         const uint64_t wm = ES == 8 ? ~0ull : ((1ull << (8 * ES)) - 1);
         bool bad = false;
-        for (int j = 0; j < 8 && base + j < n; j++) {
+        for (int j = 0; j < (int)kBVPT && base + j < n; j++) {
             const uint64_t u = ld_elem<ES>(in.ptr, base + j);
             const int k = (int)(long long)__double2ll_rn(__dmul_rn(as_double<ES>(u, o), p10[p]));
             ((int32_t *)out)[base + j] = k;
@@ -726,7 +774,7 @@ __device__ void p_f2i_enc(const BItem &it, uint32_t tile, StreamDesc *S)
         if (bad) atomicExch((unsigned int *)(it.scratch + 64), 1u);
     } else {
         const uint64_t bytes = (n * ES) / 4 * 4;
-        for (uint64_t b = base * ES; b < (base + 8) * ES && b < bytes; b++) out[b] = in.ptr[b];
+        for (uint64_t b = base * ES; b < (base + kBVPT) * ES && b < bytes; b++) out[b] = in.ptr[b];
     }
 }
 
@@ -742,9 +790,9 @@ __device__ void p_f2i_raw(const BItem &it, uint32_t tile, StreamDesc *S)
         *(int32_t *)S[it.out[0]].ptr = 10;
         S[it.out[1]].len = bytes;
     }
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     uint8_t *out = S[it.out[1]].ptr;
-    for (uint64_t b = base * ES; b < (base + 8) * ES && b < bytes; b++) out[b] = in.ptr[b];
+    for (uint64_t b = base * ES; b < (base + kBVPT) * ES && b < bytes; b++) out[b] = in.ptr[b];
 }
 
 // ------------------------------------------------------------------------------- GFC
@@ -843,10 +891,10 @@ __device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool d
     const int32_t *sizes = (const int32_t *)(it.scratch + it.p[1]);
     unsigned long long *incl = (unsigned long long *)(it.scratch + it.p[2]);
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * 8;
-    unsigned long long v[8], local = 0;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    unsigned long long v[kBVPT], local = 0;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         v[j] = base + j < (uint64_t)g.warps ? (unsigned long long)(uint32_t)sizes[base + j] : 0ull;
         local += v[j];
     }
@@ -859,7 +907,7 @@ __device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool d
     __syncthreads();
     unsigned long long acc = s_prefix + excl;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
         acc += v[j];
         if (base + j < (uint64_t)g.warps) incl[base + j] = acc;
     }
@@ -890,18 +938,19 @@ constexpr size_t stage_smem(int op)
     return op == B_AFL_PACK ? 8 * (kBTile + 4)
          : op == B_HIST     ? 12 * kBHistSmem + 8 * 4 * (kBThreads / 32)
          : op == B_TOPK     ? sizeof(Cand) * kBThreads * 4
+         : op == B_SPLIT    ? 8 * kBTile
                             : 16;
 }
 
 template <int OP>
-__global__ void __launch_bounds__(kBThreads)
-k_bstage(const BItem *items, int n_items, StreamDesc *S, uint32_t *counter, uint32_t *status)
+__global__ void __launch_bounds__(kBThreads, 3)
+k_bstage(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status)
 {
     constexpr bool DYN = OP == B_SPLIT || OP == B_RLE_HEADS || OP == B_GFC_SCAN;
     __shared__ __align__(16) unsigned char smem[stage_smem(OP)];
     BItem it;
     uint32_t tile;
-    locate<DYN>(items, n_items, counter, it, tile);
+    locate<DYN>(items, item_of, counter, it, tile);
     if (tile >= it.tiles) return;
 #define GTSC_ES_SWITCH(CALL)                       \
     switch (it.es) {                               \
@@ -915,8 +964,8 @@ k_bstage(const BItem *items, int n_items, StreamDesc *S, uint32_t *counter, uint
     else if constexpr (OP == B_SCALE_SUB) { GTSC_ES_SWITCH(p_scale_sub<E>(it, tile, S)) }
     else if constexpr (OP == B_AFL_PACK) { GTSC_ES_SWITCH(p_afl_pack<E>(it, tile, S, (unsigned long long *)smem)) }
     else if constexpr (OP == B_HIST) { GTSC_ES_SWITCH(p_hist<E>(it, tile, S, status, smem)) }
-    else if constexpr (OP == B_TOPK) { GTSC_ES_SWITCH(p_topk<E>(it, S, smem)) }
-    else if constexpr (OP == B_SPLIT) { GTSC_ES_SWITCH(p_split<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_TOPK) { GTSC_ES_SWITCH(p_topk<E>(it, tile, S, smem)) }
+    else if constexpr (OP == B_SPLIT) { GTSC_ES_SWITCH(p_split<E>(it, tile, S, status, smem)) }
     else if constexpr (OP == B_RLE_HEADS) { GTSC_ES_SWITCH(p_rle_heads<E>(it, tile, S)) }
     else if constexpr (OP == B_RLE_LENGTHS) { p_rle_lengths(it, tile, S); }
     else if constexpr (OP == B_F2I_STATS) { GTSC_ES_SWITCH(p_f2i_stats<E>(it, tile, S)) }
@@ -936,18 +985,19 @@ k_bstage(const BItem *items, int n_items, StreamDesc *S, uint32_t *counter, uint
 
 }  // namespace
 
-void launch_batch_decode_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,
-                               uint32_t *d_counter, uint32_t *d_status, cudaStream_t s);
+void launch_batch_decode_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items,
+                               uint64_t total_tiles, StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status,
+                               cudaStream_t s);
 
-void launch_batch_stage(int op, const BItem *d_items, int n_items, uint64_t total_tiles, StreamDesc *d_streams,
-                        uint32_t *d_counter, uint32_t *d_status, cudaStream_t s)
+void launch_batch_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items, uint64_t total_tiles,
+                        StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status, cudaStream_t s)
 {
     if (n_items == 0 || total_tiles == 0) return;
     if (total_tiles > 0x7fffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles in one stage");
     const unsigned g = (unsigned)total_tiles;
     switch (op) {
 #define GTSC_STAGE(OPC) \
-    case OPC: k_bstage<OPC><<<g, kBThreads, 0, s>>>(d_items, n_items, d_streams, d_counter, d_status); break;
+    case OPC: k_bstage<OPC><<<g, kBThreads, 0, s>>>(d_items, d_item_of, d_streams, d_counter, d_status); break;
         GTSC_STAGE(B_MINMAX)
         GTSC_STAGE(B_DELTA_ENC)
         GTSC_STAGE(B_SCALE_SUB)
@@ -965,7 +1015,7 @@ void launch_batch_stage(int op, const BItem *d_items, int n_items, uint64_t tota
         GTSC_STAGE(B_GFC_COMPACT)
 #undef GTSC_STAGE
     default:
-        launch_batch_decode_stage(op, d_items, n_items, total_tiles, d_streams, d_counter, d_status, s);
+        launch_batch_decode_stage(op, d_items, d_item_of, n_items, total_tiles, d_streams, d_counter, d_status, s);
         return;
     }
     GTSC_CUDA(cudaGetLastError());

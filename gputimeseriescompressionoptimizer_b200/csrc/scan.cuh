@@ -2,8 +2,8 @@
 //
 // A kernel processes tiles in the order it claims them from a global counter (so every tile's
 // predecessors were claimed earlier and make progress).  One warp of a tile publishes the tile's
-// aggregate (flag 1), reads its predecessors' descriptors 32 at a time, adds their aggregates until
-// it finds an inclusive prefix (flag 2), then publishes its own inclusive prefix.  A descriptor is
+// aggregate (flag 1), reads its predecessors' descriptors 128 at a time, adds their aggregates
+// until it finds an inclusive prefix (flag 2), then publishes its own inclusive prefix.  A descriptor is
 // two relaxed gpu-scope 64-bit words that both carry the flag, so a reader needs no acquire chain.
 // Every wait is bounded: after kSpinLimit polls, or as soon as another tile has recorded an error,
 // the tile records GTSC_ERR_TIMEOUT in *error and proceeds with a wrong prefix, so a broken
@@ -65,13 +65,17 @@ __device__ __forceinline__ void lookback_publish(const Lookback &l, uint32_t til
     st_relaxed_u64(l.desc + 2 * (uint64_t)tile + 1, f | (v >> 32));
 }
 
+constexpr int kLookbackPerLane = 4;  // descriptors read by each lane per round trip (window 128)
+
 // Called by all 32 lanes of ONE warp of the block that owns `tile` (the same tile_agg in every
 // lane): publishes the tile aggregate and returns the exclusive prefix (wrapping sum of all
-// earlier tiles) in every lane.  The warp inspects 32 predecessors per round trip: lane k reads
-// tile - 1 - k; the window is summed up to the nearest inclusive prefix, or wholly when it holds
-// only aggregates, and then moves 32 tiles back.
+// earlier tiles) in every lane.  The warp reads a window of 128 predecessors per round trip (lane
+// k reads tiles base - 4k .. base - 4k - 3, nearest first), sums the window up to its nearest
+// inclusive prefix (or wholly when it holds only aggregates, then moves 128 tiles back), and waits
+// only while a tile nearer than that prefix has published nothing.
 __device__ inline unsigned long long lookback_exclusive(const Lookback &l, uint32_t tile, unsigned long long tile_agg)
 {
+    constexpr int PL = kLookbackPerLane;
     const int lane = threadIdx.x & 31;
     if (tile == 0) {
         if (lane == 0) lookback_publish(l, 0, 2u, tile_agg);
@@ -81,39 +85,60 @@ __device__ inline unsigned long long lookback_exclusive(const Lookback &l, uint3
     unsigned long long excl = 0;
     int64_t base = (int64_t)tile - 1;
     uint32_t spins = 0;
+    bool gave_up = false;
     while (true) {
-        const int64_t idx = base - lane;
-        uint32_t flag = 2u;
-        unsigned long long v = 0;
-        if (idx >= 0) {
-            const unsigned long long w0 = ld_relaxed_u64(l.desc + 2 * idx);
-            const unsigned long long w1 = ld_relaxed_u64(l.desc + 2 * idx + 1);
-            const uint32_t f0 = (uint32_t)(w0 >> 32), f1 = (uint32_t)(w1 >> 32);
-            flag = f0 == f1 ? f0 : 0u;
-            v = (w0 & 0xffffffffull) | (w1 << 32);
+        uint32_t flag[PL];
+        unsigned long long v[PL];
+#pragma unroll
+        for (int j = 0; j < PL; j++) {
+            const int64_t idx = base - (int64_t)(PL * lane + j);
+            flag[j] = 2u;
+            v[j] = 0;
+            if (idx >= 0) {
+                const unsigned long long w0 = ld_relaxed_u64(l.desc + 2 * idx);
+                const unsigned long long w1 = ld_relaxed_u64(l.desc + 2 * idx + 1);
+                const uint32_t f0 = (uint32_t)(w0 >> 32), f1 = (uint32_t)(w1 >> 32);
+                flag[j] = f0 == f1 ? f0 : 0u;
+                v[j] = (w0 & 0xffffffffull) | (w1 << 32);
+            }
+            if (gave_up && flag[j] == 0u) {  // bounded wait ran out: treat as an empty prefix
+                flag[j] = 2u;
+                v[j] = 0;
+            }
         }
-        if (__any_sync(0xffffffffu, flag == 0u)) {
+        // this lane's nearest inclusive and nearest unpublished slot (PL = none)
+        int inc = PL, inv = PL;
+#pragma unroll
+        for (int j = PL - 1; j >= 0; j--) {
+            if (flag[j] == 2u) inc = j;
+            if (flag[j] == 0u) inv = j;
+        }
+        const unsigned inc_lanes = __ballot_sync(0xffffffffu, inc < PL);
+        const unsigned inv_lanes = __ballot_sync(0xffffffffu, inv < PL);
+        const int L_inc = inc_lanes ? __ffs(inc_lanes) - 1 : 32;
+        const int inc_pos = L_inc < 32 ? PL * L_inc + __shfl_sync(0xffffffffu, inc, L_inc & 31) : 32 * PL;
+        const int L_inv = inv_lanes ? __ffs(inv_lanes) - 1 : 32;
+        const int inv_pos = L_inv < 32 ? PL * L_inv + __shfl_sync(0xffffffffu, inv, L_inv & 31) : 32 * PL;
+        if (inv_pos < inc_pos) {  // a nearer tile has not published yet
             ++spins;
-            const bool gave_up = (spins & 63u) == 0 && *(volatile uint32_t *)l.error != 0u;
-            if (spins <= kSpinLimit && !__any_sync(0xffffffffu, gave_up)) {
+            const bool err = (spins & 63u) == 0 && *(volatile uint32_t *)l.error != 0u;
+            if (spins > kSpinLimit || __any_sync(0xffffffffu, err)) {
+                if (lane == 0) atomicExch(l.error, (uint32_t)(-GTSC_ERR_TIMEOUT));
+                gave_up = true;
+            } else {
                 __nanosleep(spins < 64 ? 32 : 256);
-                continue;
             }
-            // bounded wait: record the timeout and stop at the unpublished tile (wrong prefix)
-            if (lane == 0) atomicExch(l.error, (uint32_t)(-GTSC_ERR_TIMEOUT));
-            if (flag == 0u) {
-                flag = 2u;
-                v = 0;
-            }
+            continue;
         }
-        const unsigned incl = __ballot_sync(0xffffffffu, flag == 2u);
-        const int stop = incl ? __ffs(incl) - 1 : 31;
-        unsigned long long sum = lane <= stop ? v : 0ull;
+        unsigned long long sum = 0;
+#pragma unroll
+        for (int j = 0; j < PL; j++)
+            if (PL * lane + j <= inc_pos) sum += v[j];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         excl += sum;
-        if (incl) break;
-        base -= 32;
+        if (inc_pos < 32 * PL) break;
+        base -= 32 * PL;
     }
     if (lane == 0) lookback_publish(l, tile, 2u, excl + tile_agg);
     return excl;
