@@ -67,6 +67,13 @@ struct Launch {
     uint64_t map_off;  // this launch's tile -> item table in the item_of array
 };
 
+// passes whose tiles chain through a decoupled look-back (claimed in order from a counter)
+bool dyn_pass(int op)
+{
+    return op == B_SPLIT || op == B_RLE_HEADS || op == B_GFC_SCAN || op == B_DELTA_DEC || op == B_MERGE ||
+           op == B_RLE_SCAN;
+}
+
 uint64_t gfc_warps_for(bool dbl, uint64_t n)
 {
     const uint64_t wpb = dbl ? 16 : 32;
@@ -506,6 +513,23 @@ void BatchEngine::layout(cudaStream_t s)
             L.count = (int)items.size() - L.first;
             L.map_off = item_of.size();
             for (int k = 0; k < L.count; k++) item_of.insert(item_of.end(), items[L.first + k].tiles, (uint32_t)k);
+            if (dyn_pass(L.op)) {
+                // claim order: tile j of every item before tile j + 1 of any, so the tiles in flight
+                // spread over the items' look-back chains instead of queueing on one
+                std::vector<int> live(L.count);
+                for (int k = 0; k < L.count; k++) live[k] = k;
+                for (uint32_t j = 0; !live.empty(); j++) {
+                    size_t w = 0;
+                    for (int k : live) {
+                        const BItem &b = items[L.first + k];
+                        if (j < b.tiles) {
+                            item_of.push_back((uint32_t)(b.tile_base + j));
+                            live[w++] = k;
+                        }
+                    }
+                    live.resize(w);
+                }
+            }
             launches.push_back(L);
             i = j;
         }

@@ -216,7 +216,8 @@ __device__ __forceinline__ uint64_t d_gfc_start(const DGfc &g, int64_t w) { retu
 
 // the stage kernel skeleton: finds this block's (item, tile).  DYN passes take tiles in claim
 // order from a counter (look-back needs every predecessor claimed first), the others use the
-// block index; item_of[t] is the item of global tile t (one table per launch).
+// block index; item_of[t] is the item of global tile t (one table per launch), and for DYN launches
+// item_of[grid + c] is the tile taken by the c-th claim.
 template <bool DYN>
 __device__ __forceinline__ void locate(const BItem *items, const uint32_t *item_of, uint32_t *counter, BItem &it,
                                        uint32_t &tile)
@@ -224,7 +225,9 @@ __device__ __forceinline__ void locate(const BItem *items, const uint32_t *item_
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_idx;
     if (threadIdx.x == 0) {
-        const uint32_t t = DYN ? atomicAdd(counter, 1u) : blockIdx.x;
+        // DYN launches: the claim order (items interleaved round-robin, each item's tiles in order)
+        // follows the launch's tile -> item table
+        const uint32_t t = DYN ? item_of[gridDim.x + atomicAdd(counter, 1u)] : blockIdx.x;
         const uint32_t idx = item_of[t];
         s_idx = idx;
         s_tile = (uint32_t)(t - items[idx].tile_base);
