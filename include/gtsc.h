@@ -262,7 +262,7 @@ gtsc_status gtsc_afl_decompress_gpu(int32_t dtype, uint32_t bit_length, const vo
  * cannot call cudaMalloc -- e.g. code whose device memory is all owned by a host framework's pool.
  * Decodes the delta stream (d_first = the metadata, the column's first value; d_deltas = n_deltas
  * deltas) into d_out, which the caller provides with room for n_deltas + 1 values (16-byte aligned;
- * d_deltas aligned to the element size).  The scan's scratch is a static device array of ~160 KB,
+ * d_deltas aligned to the element size).  The scan's scratch is a static device array of ~128 KB,
  * reserved on every GPU that loads the library until exit, so at most 2^24 values are decoded per
  * call (GTSC_ERR_CAPACITY beyond).  The first call on a device looks up that array's address and
  * should come before any stream capture.  Calls share the array: calls whose GPU work overlaps race.
