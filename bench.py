@@ -38,6 +38,7 @@ MAX_LEN = 1 << int(os.environ.get("GTSC_BENCH_MAX_LOG2", "24"))
 CPU_SAMPLE_LEN = 1 << 18     # CPU legs: every column cut to its first 2^18 values
 MIN_CONFIDENCE = 0.5         # learned planner: below this softmax probability the exhaustive search decides
 TICK_CHUNKS = 4              # streaming tick table: 40 columns x 2^20 rows per chunk
+E2E_GROUPS = 8               # end to end: column groups pipelined over their own streams
 METRIC = "batched mixed-workload compress+decompress throughput (uncompressed GB/s)"
 WORKLOAD = (f"mixed {N_COLUMNS} columns, lengths log-uniform [4096, {MAX_LEN}], int32:float32:float64 = 2:1:1, "
             "generators walk/runs/zipf/const/outliers/price, seed 0xB204")
@@ -385,23 +386,6 @@ def run_ours(args, world, rank, local):
     ratio_ln = [c.nbytes / b.size for c, b in zip(cols, blobs)]
     ratio_ex = [c.nbytes / e for c, e in zip(cols, ex_sizes)]
 
-    # end to end through the public API: pinned host columns in, framed output back to the host
-    host_framed = torch.empty(framed["n"] + 4096, dtype=torch.uint8).pin_memory()
-
-    def e2e_step():
-        for d, h in zip(dv, host):
-            g.check(L.gtsc_memcpy(d.ptr, h.data_ptr(), d.nbytes, 1, sp), "h2d")
-        batch.compress()
-        p, n = batch.output()
-        g.check(L.gtsc_memcpy(host_framed.data_ptr(), p, n, 2, sp), "d2h")
-        batch.decompress(p, n, ov)
-        batch.status()
-        e2e_step.d2h = n + 4
-
-    e2e_step()
-    t_e2e = timed(e2e_step, max(2, args.steps // 2))
-    clk = clocks.stop()
-
     # launch-by-launch profile (events between launches, outside the graphs), a few repeats
     prof = {}
     for name, comp in (("compress", True), ("decompress", False)):
@@ -409,6 +393,34 @@ def run_ours(args, world, rank, local):
         prof[name] = [(runs[0][j][0], min(r[j][1] for r in runs), runs[0][j][2], runs[0][j][3])
                       for j in range(len(runs[0]))]
     batch.status()
+    n_launch = batch.launches(True) + batch.launches(False)
+    del batch, outs, ov
+
+    # end to end through the public API: the column-chunk pipeline (8 column groups, each with its
+    # batch engine and stream) from pinned host columns to pinned host framed output, then the
+    # device decode of that chunk; the call is synchronous, timed by CUDA events around it
+    pipe = g.Pipeline([c.nbytes for c in cols], dts, trees, groups=E2E_GROUPS)
+    cap = blob_bytes + 8 * len(cols) + 8 * E2E_GROUPS + (1 << 20)
+    host_framed = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    host_ptrs = [h.data_ptr() for h in host]
+    e2e_bytes = {}
+
+    def e2e_step():
+        sizes = pipe.compress_host(host_ptrs, host_framed.data_ptr(), cap)
+        pipe.decompress()
+        e2e_bytes["d2h"] = int(sizes.sum()) + 4
+
+    e2e_step()
+    for i in range(len(cols)):  # the first end-to-end step restores every column
+        _, d_out = pipe.column(i)
+        chk = torch.empty_like(dev[i])
+        g.check(L.gtsc_memcpy(chk.data_ptr(), d_out, dev[i].numel(), 3, sp), "d2d")
+        torch.cuda.synchronize()
+        assert torch.equal(chk, dev[i]), f"column {i}: end-to-end round trip differs"
+        del chk
+    t_e2e = timed(e2e_step, max(2, args.steps // 2))
+    clk = clocks.stop()
+    del pipe
 
     if rank != 0:
         if dist is not None:
@@ -471,8 +483,10 @@ def run_ours(args, world, rank, local):
                          "sample": f"all {len(scols)} columns cut to their first 2^18 values ({cin} B), same trees, "
                                    "oracle tree compress + decompress"},
         "e2e": {"value": round(world * in_bytes / t_e2e / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": in_bytes,
-                "d2h_bytes_per_step": e2e_step.d2h},
-        "gpu_launches": (batch.launches(True) + batch.launches(False)) * args.steps,
+                "d2h_bytes_per_step": e2e_bytes["d2h"],
+                "path": f"gtsc_pipeline_compress_host + gtsc_pipeline_decompress, {E2E_GROUPS} column groups, "
+                        "pinned host buffers"},
+        "gpu_launches": n_launch * args.steps,
         "tick_table": tick,
         "clocks": clk,
     }

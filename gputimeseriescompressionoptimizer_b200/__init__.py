@@ -78,6 +78,7 @@ def lib():
         L.gtsc_malloc.argtypes = [ctypes.POINTER(vp), u64, vp]
         L.gtsc_free.argtypes = [vp, vp]
         L.gtsc_memcpy.argtypes = [vp, vp, u64, i32, vp]
+        L.gtsc_memcpy_async.argtypes = [vp, vp, u64, i32, vp]
         L.gtsc_stream_synchronize.argtypes = [vp]
         L.gtsc_encode.argtypes = [i32, i32, vp, u64, ctypes.POINTER(Buffer), ctypes.POINTER(ctypes.c_uint32), vp]
         L.gtsc_decode.argtypes = [i32, i32, ctypes.POINTER(Buffer), ctypes.c_uint32, ctypes.POINTER(Buffer), vp]
@@ -108,6 +109,13 @@ def lib():
         L.gtsc_batch_launches.argtypes = [vp, i32]
         L.gtsc_batch_destroy.argtypes = [vp]
         L.gtsc_batch_profile.argtypes = [vp, i32, i32p, ctypes.POINTER(ctypes.c_float), u64p, u64p, i32, i32p, vp]
+        L.gtsc_pipeline_create.argtypes = [ctypes.POINTER(Column), u32, i16p, i32p, i32, ctypes.POINTER(vp)]
+        L.gtsc_pipeline_groups.argtypes = [vp]
+        L.gtsc_pipeline_group_columns.argtypes = [vp, i32, i32p, i32, i32p]
+        L.gtsc_pipeline_compress_host.argtypes = [vp, ctypes.POINTER(vp), vp, u64, u64p]
+        L.gtsc_pipeline_decompress.argtypes = [vp]
+        L.gtsc_pipeline_column.argtypes = [vp, i32, ctypes.POINTER(vp), ctypes.POINTER(vp)]
+        L.gtsc_pipeline_destroy.argtypes = [vp]
         f32p = ctypes.POINTER(ctypes.c_float)
         L.gtsc_planner_features.argtypes = [ctypes.POINTER(Column), u32, vp, vp]
         L.gtsc_planner_create.argtypes = [i16p, i32p, i32, u64, ctypes.POINTER(vp)]
@@ -301,7 +309,7 @@ class Stream:
 PASS_NAMES = dict(enumerate(
     ["minmax", "delta_enc", "scale_sub", "afl_pack", "hist", "topk", "split", "rle_heads", "rle_lengths",
      "f2i_stats", "f2i_enc", "f2i_raw", "gfc_compress", "gfc_scan", "gfc_compact", "none_copy", "afl_unpack",
-     "delta_dec", "scale_add", "merge", "rle_scan", "rle_expand", "f2i_dec", "gfc_sizes", "gfc_dec"]))
+     "delta_dec", "scale_add", "merge", "rle_scan", "rle_expand", "f2i_dec", "gfc_sizes", "gfc_dec", "vmeta"]))
 PASS_NAMES.update({-1: "set_streams", -2: "zero", -3: "frame_sizes", -4: "frame_layout", -5: "frame_copy",
                    -6: "parse_frames"})
 
@@ -379,6 +387,56 @@ class Batch:
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:
             _lib.gtsc_batch_destroy(self.handle)
+            self.handle = None
+
+
+# ------------------------------------------------------------------------ column-chunk pipeline
+class Pipeline:
+    """Column chunks from host memory (pinned for overlap) to host framed output, column groups
+    pipelined over their own batch engines and streams (gtsc_pipeline_*)."""
+
+    def __init__(self, sizes, dtypes, trees, groups=8):
+        self.n = len(sizes)
+        cols = (Column * self.n)()
+        for i, (b, dt) in enumerate(zip(sizes, dtypes)):
+            cols[i] = Column(None, int(b), dt, 0)
+        counts = np.array([len(t) // 2 for t in trees], np.int32)
+        nodes = np.ascontiguousarray(np.concatenate([np.asarray(t, np.int16) for t in trees]))
+        h = ctypes.c_void_p()
+        check(lib().gtsc_pipeline_create(cols, self.n, nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
+                                         _i32(counts), groups, ctypes.byref(h)), "pipeline_create")
+        self.handle = h.value
+        self.groups = lib().gtsc_pipeline_groups(self.handle)
+
+    def compress_host(self, host_ptrs, framed_ptr, cap):
+        """host_ptrs: addresses of the host columns; framed_ptr: host buffer of cap bytes.
+        Returns the bytes of every group's framed output (written back to back)."""
+        arr = (ctypes.c_void_p * self.n)(*host_ptrs)
+        sizes = np.zeros(self.groups, np.uint64)
+        check(lib().gtsc_pipeline_compress_host(self.handle, arr, framed_ptr, cap,
+                                                sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))),
+              "pipeline_compress_host")
+        return sizes
+
+    def decompress(self):
+        check(lib().gtsc_pipeline_decompress(self.handle), "pipeline_decompress")
+
+    def group_columns(self, g):
+        out = np.zeros(self.n, np.int32)
+        k = ctypes.c_int32(0)
+        check(lib().gtsc_pipeline_group_columns(self.handle, g, _i32(out), self.n, ctypes.byref(k)),
+              "pipeline_group_columns")
+        return out[:k.value].tolist()
+
+    def column(self, c):
+        """(device input, device output) addresses of column c."""
+        a, b = ctypes.c_void_p(), ctypes.c_void_p()
+        check(lib().gtsc_pipeline_column(self.handle, c, ctypes.byref(a), ctypes.byref(b)), "pipeline_column")
+        return a.value, b.value
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.gtsc_pipeline_destroy(self.handle)
             self.handle = None
 
 

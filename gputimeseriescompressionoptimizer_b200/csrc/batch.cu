@@ -51,6 +51,12 @@ struct HNode {
     // decode scratch layout (relative to scratch)
     uint64_t dlb_off = 0, dends_off = 0, druns_off = 0, dsizes_off = 0, dincl_off = 0;
     int last_c_level = 0, last_d_level = 0;
+    // compress input view: the node reads stream in_sid through vop[] (V_SCALE ops take their
+    // constant from scale node vnode[k]); a virtual node's own output is never written, its child
+    // reads it as this node's view plus this node's operation
+    int8_t vop[kMaxViewOps] = {V_NONE, V_NONE, V_NONE};
+    int vnode[kMaxViewOps] = {-1, -1, -1};
+    bool virt = false;
 };
 
 struct Pass {
@@ -59,6 +65,20 @@ struct Pass {
     int node;
     BItem item;
 };
+
+int view_ops(const int8_t *vop)
+{
+    int k = 0;
+    while (k < kMaxViewOps && vop[k] != V_NONE) ++k;
+    return k;
+}
+
+// encodings whose compress passes read their input through a view
+bool view_consumer(int enc)
+{
+    return enc == GTSC_AFL || enc == GTSC_GFC || enc == GTSC_DICT || enc == GTSC_CONST || enc == GTSC_PATCH ||
+           enc == GTSC_RLE || enc == GTSC_DELTA || enc == GTSC_SCALE;
+}
 
 struct Launch {
     int op;
@@ -123,7 +143,8 @@ public:
         return (int)streams.size() - 1;
     }
 
-    void build_node(const Tree &t, int &k, int col, int parent, int in_sid, uint64_t in_cap, int depth);
+    void build_node(const Tree &t, int &k, int col, int parent, int in_sid, uint64_t in_cap, int depth,
+                    const int8_t *in_vop, const int *in_vnode);
     void plan_passes();
     void layout(cudaStream_t s);
     void capture(cudaStream_t s);
@@ -133,7 +154,8 @@ public:
 
 // ---------------------------------------------------------------------------------- compile
 
-void BatchEngine::build_node(const Tree &t, int &k, int col, int parent, int in_sid, uint64_t in_cap, int depth)
+void BatchEngine::build_node(const Tree &t, int &k, int col, int parent, int in_sid, uint64_t in_cap, int depth,
+                             const int8_t *in_vop, const int *in_vnode)
 {
     if (k >= t.size() || depth > 64) fail(GTSC_ERR_ARG, "batch: incomplete tree");
     HNode nd;
@@ -144,7 +166,15 @@ void BatchEngine::build_node(const Tree &t, int &k, int col, int parent, int in_
     nd.parent = parent;
     nd.in_sid = in_sid;
     nd.in_cap = in_cap;
+    for (int j = 0; j < kMaxViewOps; j++) {
+        nd.vop[j] = in_vop ? in_vop[j] : (int8_t)V_NONE;
+        nd.vnode[j] = in_vnode ? in_vnode[j] : -1;
+    }
     ++k;
+    // a delta / scale whose one child reads through views is not materialised
+    const int nops = view_ops(nd.vop);
+    nd.virt = (nd.enc == GTSC_DELTA || nd.enc == GTSC_SCALE) && k < t.size() && view_consumer(t.enc[k]) &&
+              nops < kMaxViewOps;
     const int id = (int)nodes.size();
     nodes.push_back(nd);
     if (parent >= 0) nodes[parent].kids.push_back(id);
@@ -173,13 +203,28 @@ void BatchEngine::build_node(const Tree &t, int &k, int col, int parent, int in_
     default: fail(GTSC_ERR_ARG, "batch: unsupported encoding in tree");
     }
     const int r = n_results(me.enc);
+    if (me.virt) cap[1] = 0;  // read through the child's view, never written
     if (me.enc != GTSC_NONE)
         for (int j = 0; j <= r; j++) nodes[id].out_sid[j] = new_stream(cap[j]);
     // decode-side streams
     if (nodes[id].enc == GTSC_NONE) nodes[id].dec_data_sid = new_stream(0);
     else nodes[id].dec_meta_sid = new_stream(0);
     if (parent >= 0) nodes[id].dec_out_sid = new_stream(in_cap);
-    for (int j = 0; j < r; j++) build_node(t, k, col, id, nodes[id].out_sid[j + 1], cap[j + 1], depth + 1);
+    if (nodes[id].virt) {
+        int8_t cv[kMaxViewOps];
+        int cn[kMaxViewOps];
+        for (int j = 0; j < kMaxViewOps; j++) {
+            cv[j] = nodes[id].vop[j];
+            cn[j] = nodes[id].vnode[j];
+        }
+        const int nops2 = view_ops(cv);
+        cv[nops2] = nodes[id].enc == GTSC_DELTA ? (int8_t)V_DELTA : (int8_t)V_SCALE;
+        cn[nops2] = nodes[id].enc == GTSC_SCALE ? id : -1;
+        const uint64_t child_cap = nodes[id].in_cap;
+        build_node(t, k, col, id, nodes[id].in_sid, child_cap, depth + 1, cv, cn);
+        return;
+    }
+    for (int j = 0; j < r; j++) build_node(t, k, col, id, nodes[id].out_sid[j + 1], cap[j + 1], depth + 1, nullptr, nullptr);
 }
 
 void BatchEngine::plan_passes()
@@ -263,6 +308,7 @@ void BatchEngine::plan_passes()
             it.out[j] = nd.out_sid[j];
         }
         it.in[0] = nd.in_sid;
+        for (int j = 0; j < kMaxViewOps; j++) it.vop[j] = nd.vop[j];
         return it;
     };
 
@@ -274,6 +320,24 @@ void BatchEngine::plan_passes()
         const uint64_t t2k = cdiv(n, kBTile);
         std::vector<BItem> ps;
         auto add = [&](BItem it) { ps.push_back(it); };
+        const int nops = view_ops(nd.vop);
+        const bool scale_view = nops > 0 && nd.vop[nops - 1] == V_SCALE;
+        if (nd.virt) {
+            // delta: metadata only, the child can start at once; scale: min/max, then metadata
+            BItem vm = base_item(nd, B_VMETA, 1);
+            vm.mode = (int16_t)nd.enc;
+            if (nd.enc == GTSC_SCALE) {
+                add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+                add(vm);
+            } else {
+                add(vm);
+            }
+            int lvl = start;
+            for (auto &it : ps) pass_c.push_back(Pass{lvl++, it.op, (int)id, it});
+            // children start with the last pass (the metadata pass has no consumer)
+            nd.last_c_level = start + (int)ps.size() - 2;
+            continue;
+        }
         switch (nd.enc) {
         case GTSC_NONE: break;
         case GTSC_DELTA: add(base_item(nd, B_DELTA_ENC, t2k)); break;
@@ -281,10 +345,13 @@ void BatchEngine::plan_passes()
             add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
             add(base_item(nd, B_SCALE_SUB, t2k));
             break;
-        case GTSC_AFL:
-            add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
-            add(base_item(nd, B_AFL_PACK, t2k));
+        case GTSC_AFL: {
+            BItem pk = base_item(nd, B_AFL_PACK, t2k);
+            if (scale_view) pk.vflags |= 1;  // width from the scale's min / max: no min/max pass
+            else add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+            add(pk);
             break;
+        }
         case GTSC_PATCH: {
             BItem mm = base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile));
             mm.order = (int16_t)native_order(nd.dt);
@@ -356,8 +423,10 @@ void BatchEngine::plan_passes()
                 cp.op = B_GFC_COMPACT;
                 add(cp);
             } else {
-                add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
-                add(base_item(nd, B_AFL_PACK, t2k));
+                BItem pk = base_item(nd, B_AFL_PACK, t2k);
+                if (scale_view) pk.vflags |= 1;
+                else add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+                add(pk);
             }
             break;
         default: break;
@@ -505,6 +574,11 @@ void BatchEngine::layout(cudaStream_t s)
             while (j < ps.size() && ps[j].level == ps[i].level && ps[j].op == ps[i].op) {
                 BItem it = ps[j].item;
                 it.scratch = A + nodes[ps[j].node].scratch;
+                if (ps[j].op < B_NONE_COPY || ps[j].op == B_VMETA)  // compress passes: the view's scale nodes
+                    for (int v = 0; v < kMaxViewOps; v++) {
+                        const int sn = nodes[ps[j].node].vnode[v];
+                        it.vscr[v] = sn >= 0 ? A + nodes[sn].scratch : nullptr;
+                    }
                 it.tile_base = L.tiles;
                 L.tiles += it.tiles;
                 items.push_back(it);
@@ -751,7 +825,7 @@ BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vecto
         e->col_bytes.push_back(cols[c].bytes);
         e->col_root.push_back((int)e->nodes.size());
         int k = 0;
-        e->build_node(t, k, (int)c, -1, in_sid, cols[c].bytes, 0);
+        e->build_node(t, k, (int)c, -1, in_sid, cols[c].bytes, 0, nullptr, nullptr);
         if (k != t.size()) fail(GTSC_ERR_ARG, "batch: extra nodes in tree");
         e->nodes[e->col_root.back()].dec_out_sid = out_sid;
     }
@@ -776,6 +850,11 @@ BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vecto
 void batch_destroy(BatchEngine *e)
 {
     if (!e) return;
+    // the arena was allocated on the caller's stream, which may already be gone: finish all work,
+    // then release on the legacy stream
+    cudaDeviceSynchronize();
+    e->arena.release_on_default_stream();
+    e->tables.release_on_default_stream();
     if (e->graph_c) cudaGraphExecDestroy(e->graph_c);
     if (e->graph_d) cudaGraphExecDestroy(e->graph_d);
     delete e;

@@ -41,8 +41,16 @@ enum BOp : int {
     B_F2I_DEC,
     B_GFC_SIZES,
     B_GFC_DEC,
+    B_VMETA,           // compress: metadata of a node whose output is read through a view
     B_NUM_OPS
 };
+
+// Elementwise operations a pass applies to its input stream on the fly (the input "view"), so that
+// delta and scale nodes feeding another encoding never write their output: in order,
+//   V_DELTA  y[i] = x[i + 1] - x[i]            (one element shorter)
+//   V_SCALE  y[i] = x[i] - c                   (c from the scale node's min/max, scale_min)
+enum VOp : int8_t { V_NONE = 0, V_DELTA = 1, V_SCALE = 2 };
+constexpr int kMaxViewOps = 3;
 
 // A stream: device bytes and their length.  The table lives in device memory; compress passes
 // write lengths, the decode parser writes the pointers of streams that sit inside a blob.
@@ -64,6 +72,9 @@ struct BItem {
     int32_t out[3];              // output stream ids (compress: meta, out1, out2; decode: out[0])
     uint8_t *scratch;            // the node's scratch: accumulators, look-back state, tables
     uint64_t p[4];               // pass parameters (scratch offsets, capacities)
+    int8_t vop[kMaxViewOps];     // the input view: ops applied to in[0] (compress passes)
+    int8_t vflags;               // bit 0: AFL width from the view's last scale (no own min/max pass)
+    uint8_t *vscr[kMaxViewOps];  // V_SCALE: that scale node's scratch (its MinMaxAcc)
 };
 
 // A tree node as the framing / parse kernels see it.
@@ -126,6 +137,19 @@ struct BatchLaunchProfile {
     uint64_t blocks;
 };
 std::vector<BatchLaunchProfile> batch_profile(BatchEngine *e, bool compress, cudaStream_t s);
+
+// column chunks from host memory through per-group batch engines with overlapped copies
+struct Pipeline;
+Pipeline *pipeline_create(const std::vector<uint64_t> &bytes, const std::vector<int> &dtypes,
+                          const std::vector<Tree> &trees, int groups);
+void pipeline_destroy(Pipeline *p);
+int pipeline_groups(const Pipeline *p);
+const std::vector<int> &pipeline_group_columns(const Pipeline *p, int g);  // ascending column indices
+void pipeline_compress_host(Pipeline *p, const void *const *host_cols, uint8_t *host_framed, uint64_t cap,
+                            uint64_t *sizes);
+gtsc_status pipeline_decompress(Pipeline *p);
+const void *pipeline_column_input(Pipeline *p, int c);
+const void *pipeline_column_output(Pipeline *p, int c);
 
 // stage launcher (batch_kernels.cu / batch_decode.cu): one launch of `total_tiles` blocks;
 // d_item_of[t] = the item (index into d_items) of tile t

@@ -214,6 +214,90 @@ __device__ __forceinline__ uint64_t d_gfc_cut(const DGfc &g, int64_t i)
 __device__ __forceinline__ uint64_t d_gfc_begin(const DGfc &g, int64_t w) { return w ? d_gfc_cut(g, w - 1) : 0; }
 __device__ __forceinline__ uint64_t d_gfc_start(const DGfc &g, int64_t w) { return (d_gfc_begin(g, w) + 1) / 2 * (uint64_t)g.unit; }
 
+// ------------------------------------------------------------------------------- input views
+// A pass's input is S[it.in[0]] seen through it.vop[]: the constants of the scale ops and the
+// view's length, computed once per block.
+struct ViewCtx {
+    uint64_t c[kMaxViewOps];
+    uint64_t n;      // view elements
+    uint64_t n_src;  // source elements
+    int nd;          // delta ops (source elements read past the view's end)
+    bool plain;
+};
+
+template <int ES>
+__device__ __forceinline__ ViewCtx view_ctx(const BItem &it, const StreamDesc &src)
+{
+    ViewCtx v;
+    v.n_src = src.len / ES;
+    v.nd = 0;
+    v.plain = it.vop[0] == V_NONE;
+#pragma unroll
+    for (int k = 0; k < kMaxViewOps; k++) {
+        v.c[k] = 0;
+        if (it.vop[k] == V_DELTA) ++v.nd;
+        else if (it.vop[k] == V_SCALE) {
+            uint64_t mnb = 0, mxb = 0;
+            acc_minmax((const MinMaxAcc *)it.vscr[k], ES, ORD_INT, mnb, mxb);
+            v.c[k] = scale_min(mnb, mxb, ES);
+        }
+    }
+    v.n = v.n_src > (uint64_t)v.nd ? v.n_src - v.nd : 0;
+    return v;
+}
+
+// view elements [base, base + VPT) (garbage at and past the view's end)
+template <int ES, int VPT>
+__device__ __forceinline__ void load_view(const BItem &it, const ViewCtx &vc, const uint8_t *src, uint64_t base,
+                                          uint64_t (&v)[VPT])
+{
+    if (vc.plain) {
+        load_run<ES, VPT>(src, base, vc.n_src, v);
+        return;
+    }
+    uint64_t x[VPT + kMaxViewOps];
+    uint64_t head[VPT];
+    load_run<ES, VPT>(src, base, vc.n_src, head);
+#pragma unroll
+    for (int j = 0; j < VPT; j++) x[j] = head[j];
+#pragma unroll
+    for (int j = 0; j < kMaxViewOps; j++)
+        x[VPT + j] = j < vc.nd && base + VPT + j < vc.n_src ? ld_elem<ES>(src, base + VPT + j) : 0;
+#pragma unroll
+    for (int k = 0; k < kMaxViewOps; k++) {
+        if (it.vop[k] == V_DELTA) {
+#pragma unroll
+            for (int j = 0; j + 1 < VPT + kMaxViewOps; j++) x[j] = wrap_es(x[j + 1] - x[j], ES);
+        } else if (it.vop[k] == V_SCALE) {
+#pragma unroll
+            for (int j = 0; j < VPT + kMaxViewOps; j++) x[j] = wrap_es(x[j] - vc.c[k], ES);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < VPT; j++) v[j] = x[j];
+}
+
+// view element i (i < vc.n)
+template <int ES>
+__device__ __forceinline__ uint64_t view_elem(const BItem &it, const ViewCtx &vc, const uint8_t *src, uint64_t i)
+{
+    if (vc.plain) return ld_elem<ES>(src, i);
+    uint64_t x[kMaxViewOps + 1];
+#pragma unroll
+    for (int j = 0; j <= kMaxViewOps; j++) x[j] = j <= vc.nd && i + j < vc.n_src ? ld_elem<ES>(src, i + j) : 0;
+#pragma unroll
+    for (int k = 0; k < kMaxViewOps; k++) {
+        if (it.vop[k] == V_DELTA) {
+#pragma unroll
+            for (int j = 0; j < kMaxViewOps; j++) x[j] = wrap_es(x[j + 1] - x[j], ES);
+        } else if (it.vop[k] == V_SCALE) {
+#pragma unroll
+            for (int j = 0; j <= kMaxViewOps; j++) x[j] = wrap_es(x[j] - vc.c[k], ES);
+        }
+    }
+    return x[0];
+}
+
 // the stage kernel skeleton: finds this block's (item, tile).  DYN passes take tiles in claim
 // order from a counter (look-back needs every predecessor claimed first), the others use the
 // block index; item_of[t] is the item of global tile t (one table per launch), and for DYN launches

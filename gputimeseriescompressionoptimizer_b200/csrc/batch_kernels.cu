@@ -19,32 +19,22 @@ template <int ES>
 __device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
 {
     const StreamDesc in = S[it.in[0]];
-    const uint64_t n = in.len / ES;
+    const ViewCtx vc = view_ctx<ES>(it, in);
+    const uint64_t n = vc.n;
     const uint64_t t0 = (uint64_t)tile * kBMinMaxTile;
     if (t0 >= n) return;
     const uint64_t end = n < t0 + kBMinMaxTile ? n : t0 + kBMinMaxTile;
     const Order o = (Order)it.order;
-    constexpr int PER = 16 / ES;
     uint64_t kmin = ~0ull, kmax = 0;
-    for (uint64_t i = t0 + (uint64_t)threadIdx.x * PER; i < end; i += (uint64_t)kBThreads * PER) {
-        if (i + PER <= end) {
-            const uint4 c = ld_chunk(in.ptr + i * ES);
+    for (uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT; base < end; base += (uint64_t)kBThreads * kBVPT) {
+        uint64_t v[kBVPT];
+        load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
 #pragma unroll
-            for (int j = 0; j < PER; j++) {
-                const uint64_t u = chunk_elem<ES>(c, j);
-                if (is_nan_bits(u, o)) continue;
-                const uint64_t k = order_key(u, ES, o);
-                kmin = k < kmin ? k : kmin;
-                kmax = k > kmax ? k : kmax;
-            }
-        } else {
-            for (uint64_t j = i; j < end; j++) {
-                const uint64_t u = ld_elem<ES>(in.ptr, j);
-                if (is_nan_bits(u, o)) continue;
-                const uint64_t k = order_key(u, ES, o);
-                kmin = k < kmin ? k : kmin;
-                kmax = k > kmax ? k : kmax;
-            }
+        for (int j = 0; j < (int)kBVPT; j++) {
+            if (base + j >= end || is_nan_bits(v[j], o)) continue;
+            const uint64_t k = order_key(v[j], ES, o);
+            kmin = k < kmin ? k : kmin;
+            kmax = k > kmax ? k : kmax;
         }
     }
     block_minmax(kmin, kmax);
@@ -60,11 +50,12 @@ template <int ES>
 __device__ void p_delta_enc(const BItem &it, uint32_t tile, StreamDesc *S)
 {
     const StreamDesc in = S[it.in[0]];
-    const uint64_t n = in.len / ES;
+    const ViewCtx vc = view_ctx<ES>(it, in);
+    const uint64_t n = vc.n;
     if (tile == 0 && threadIdx.x == 0) {
         StreamDesc &m = S[it.out[0]];
         if (n) {
-            st_elem<ES>(m.ptr, 0, ld_elem<ES>(in.ptr, 0));
+            st_elem<ES>(m.ptr, 0, view_elem<ES>(it, vc, in.ptr, 0));
             m.len = ES;
             S[it.out[1]].len = (n - 1) * ES;
         } else {
@@ -76,8 +67,8 @@ __device__ void p_delta_enc(const BItem &it, uint32_t tile, StreamDesc *S)
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     if (base >= m) return;
     uint64_t v[kBVPT];
-    load_run<ES, kBVPT>(in.ptr, base, n, v);
-    const uint64_t next = base + kBVPT < n ? ld_elem<ES>(in.ptr, base + kBVPT) : 0;
+    load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+    const uint64_t next = base + kBVPT < n ? view_elem<ES>(it, vc, in.ptr, base + kBVPT) : 0;
     uint64_t d[kBVPT];
 #pragma unroll
     for (int j = 0; j + 1 < (int)kBVPT; j++) d[j] = wrap_es(v[j + 1] - v[j], ES);
@@ -90,7 +81,8 @@ template <int ES>
 __device__ void p_scale_sub(const BItem &it, uint32_t tile, StreamDesc *S)
 {
     const StreamDesc in = S[it.in[0]];
-    const uint64_t n = in.len / ES;
+    const ViewCtx vc = view_ctx<ES>(it, in);
+    const uint64_t n = vc.n;
     uint64_t mnb = 0, mxb = 0;
     acc_minmax((const MinMaxAcc *)it.scratch, ES, ORD_INT, mnb, mxb);
     const uint64_t mn = scale_min(mnb, mxb, ES);
@@ -106,21 +98,43 @@ __device__ void p_scale_sub(const BItem &it, uint32_t tile, StreamDesc *S)
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     if (base >= n) return;
     uint64_t v[kBVPT];
-    load_run<ES, kBVPT>(in.ptr, base, n, v);
+    load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) v[j] = wrap_es(v[j] - mn, ES);
     store_run<ES, kBVPT>(S[it.out[1]].ptr, base, n, v);
 }
 
 // ------------------------------------------------------------------------------- AFL pack
+__device__ __forceinline__ uint32_t afl_slot(uint32_t i) { return i + (i >> 4); }
 template <int ES>
 __device__ void p_afl_pack(const BItem &it, uint32_t tile, StreamDesc *S, unsigned long long *sv)
 {
     const StreamDesc in = S[it.in[0]];
-    const uint64_t n = in.len / ES;
+    const ViewCtx vc = view_ctx<ES>(it, in);
+    const uint64_t n = vc.n;
     uint64_t mnb = 0, mxb = 0;
-    acc_minmax((const MinMaxAcc *)it.scratch, ES, ORD_INT, mnb, mxb);
-    const int b = bitlen_signed(sext(mnb, ES), sext(mxb, ES), ES);
+    int b;
+    if (it.vflags & 1) {
+        // the view ends with a scale by c = scale_min(min, max) of the scale's input: c = 0 leaves
+        // [min, max]; c = min maps onto [0, max - min], unless max - min passes the type's largest
+        // value (scale_min keeps c = min for the most negative min): then values wrap negative
+        // and the width is the full word, as BITLEN gives for any negative minimum
+        int last = 0;
+        for (int k = 0; k < kMaxViewOps; k++)
+            if (it.vop[k] == V_SCALE) last = k;
+        acc_minmax((const MinMaxAcc *)it.vscr[last], ES, ORD_INT, mnb, mxb);
+        const uint64_t c = vc.c[last];
+        if (c == 0) {
+            b = bitlen_signed(sext(mnb, ES), sext(mxb, ES), ES);
+        } else {
+            const uint64_t span = (uint64_t)sext(mxb, ES) - (uint64_t)sext(mnb, ES);
+            const uint64_t tmax = (ES == 8 ? ~0ull : ((1ull << (8 * ES)) - 1)) >> 1;
+            b = span > tmax ? 8 * ES : bitlen_signed(0, (int64_t)span, ES);
+        }
+    } else {
+        acc_minmax((const MinMaxAcc *)it.scratch, ES, ORD_INT, mnb, mxb);
+        b = bitlen_signed(sext(mnb, ES), sext(mxb, ES), ES);
+    }
     const uint64_t W = 8ull * ES;
     const uint64_t out_bytes = n ? (b * n + W - 1) / W * ES : 0;
     if (tile == 0 && threadIdx.x == 0) {
@@ -141,19 +155,27 @@ __device__ void p_afl_pack(const BItem &it, uint32_t tile, StreamDesc *S, unsign
     uint8_t *out = S[it.out[1]].ptr;
     const uint64_t vmask = b >= 64 ? ~0ull : ((1ull << b) - 1);
     const uint64_t cnt = n - t0 < kBTile ? n - t0 : kBTile;
-    const uint8_t *src = in.ptr + t0 * ES;
-    if (cnt == kBTile) {
+    // the tile's values in shared memory, skewed by one slot per 16 values (afl_slot) so that a
+    // thread's run of 16 and the word gather below both spread over the banks
+    if (vc.plain && cnt == kBTile && ((uintptr_t)in.ptr & 15) == 0) {
+        const uint8_t *src = in.ptr + t0 * ES;
         constexpr int PER = 16 / ES;
         for (int c = threadIdx.x; c < (int)kBTile / PER; c += kBThreads) {
             const uint4 v = ld_chunk(src + 16 * c);
 #pragma unroll
-            for (int j = 0; j < PER; j++) sv[c * PER + j] = chunk_elem<ES>(v, j) & vmask;
+            for (int j = 0; j < PER; j++) sv[afl_slot(c * PER + j)] = chunk_elem<ES>(v, j) & vmask;
         }
     } else {
-        for (int i = threadIdx.x; i < (int)kBTile; i += kBThreads)
-            sv[i] = (uint64_t)i < cnt ? (ld_elem<ES>(src, i) & vmask) : 0ull;
+        uint64_t v[kBVPT];
+        const uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT;
+        load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++) {
+            const uint32_t i = threadIdx.x * kBVPT + j;
+            sv[afl_slot(i)] = base + j < n ? (v[j] & vmask) : 0ull;
+        }
     }
-    if (threadIdx.x < 4) sv[kBTile + threadIdx.x] = 0;
+    if (threadIdx.x < 4) sv[afl_slot(kBTile + threadIdx.x)] = 0;
     __syncthreads();
     const uint64_t total_words = (out_bytes + 3) / 4;
     const uint64_t w0 = t0 * (uint64_t)b / 32;
@@ -163,11 +185,11 @@ __device__ void p_afl_pack(const BItem &it, uint32_t tile, StreamDesc *S, unsign
         const uint32_t p = (uint32_t)(w - w0) * 32u;
         uint32_t a = p / (uint32_t)b;
         const uint32_t s = p - a * (uint32_t)b;
-        uint64_t acc = sv[a] >> s;
+        uint64_t acc = sv[afl_slot(a)] >> s;
         int filled = b - (int)s;
         ++a;
         while (filled < 32) {
-            acc |= sv[a] << filled;
+            acc |= sv[afl_slot(a)] << filled;
             filled += b;
             ++a;
         }
@@ -251,7 +273,8 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
     unsigned int *scounts = (unsigned int *)(smem + 8 * kBHistSmem);
     unsigned long long(*snan)[4] = (unsigned long long(*)[4])(smem + 12 * kBHistSmem);
     const StreamDesc in = S[it.in[0]];
-    const uint64_t n = in.len / ES;
+    const ViewCtx vc = view_ctx<ES>(it, in);
+    const uint64_t n = vc.n;
     const uint64_t t0 = (uint64_t)tile * kBHistTile;
     const HTab t = htab(it);
     const Order o = (Order)it.order;
@@ -270,7 +293,7 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         __syncthreads();
         const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
         for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
-            const unsigned long long key = ld_elem<ES>(in.ptr, i);
+            const unsigned long long key = view_elem<ES>(it, vc, in.ptr, i);
             if (is_nan_bits(key, o)) {
                 unsigned long long k = order_key(key, ES, o);
 #pragma unroll
@@ -430,7 +453,8 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     __shared__ unsigned long long s_prefix;
     const int mode = it.mode;
     const StreamDesc in = S[it.in[0]];
-    const uint64_t n = in.len / ES;
+    const ViewCtx vc = view_ctx<ES>(it, in);
+    const uint64_t n = vc.n;
     const Order o = (Order)it.order;
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     // stencil location and the values matched against
@@ -439,7 +463,7 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     uint64_t top[4] = {0, 0, 0, 0}, thr = 0;
     if (mode == SPLIT_LOWER) {
         uint64_t mnb = 0, mxb = 0;
-        if (!acc_minmax((const MinMaxAcc *)it.scratch, ES, o, mnb, mxb) && n) mnb = mxb = ld_elem<ES>(in.ptr, 0);
+        if (!acc_minmax((const MinMaxAcc *)it.scratch, ES, o, mnb, mxb) && n) mnb = mxb = view_elem<ES>(it, vc, in.ptr, 0);
         thr = d_patch_threshold(mnb, mxb, it.dt, ES);
     } else if (mode == SPLIT_NOT_CONST) {
         top[0] = ld_elem<ES>(meta, 0);
@@ -457,7 +481,7 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     }
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     uint64_t v[kBVPT];
-    load_run<ES, kBVPT>(in.ptr, base, n, v);
+    load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
     uint32_t bits = 0, codes = 0;
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) {
@@ -569,7 +593,8 @@ __device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
     const StreamDesc in = S[it.in[0]];
-    const uint64_t n = in.len / ES;
+    const ViewCtx vc = view_ctx<ES>(it, in);
+    const uint64_t n = vc.n;
     const Order o = (Order)it.order;
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     uint32_t *starts = (uint32_t *)(it.scratch + it.p[1]);
@@ -584,8 +609,8 @@ __device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
     }
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     uint64_t v[kBVPT];
-    load_run<ES, kBVPT>(in.ptr, base, n, v);
-    const uint64_t prev = base > 0 && base - 1 < n ? ld_elem<ES>(in.ptr, base - 1) : 0;
+    load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+    const uint64_t prev = base > 0 && base - 1 < n ? view_elem<ES>(it, vc, in.ptr, base - 1) : 0;
     uint32_t heads = 0;
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) {
@@ -618,7 +643,10 @@ __device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
 
 __device__ void p_rle_lengths(const BItem &it, uint32_t tile, StreamDesc *S)
 {
-    const uint64_t n = S[it.in[0]].len / it.es;
+    int nd = 0;
+    for (int k = 0; k < kMaxViewOps; k++) nd += it.vop[k] == V_DELTA;
+    const uint64_t n_src = S[it.in[0]].len / it.es;
+    const uint64_t n = n_src > (uint64_t)nd ? n_src - nd : 0;
     const uint64_t runs = S[it.out[1]].len / 4;
     const uint32_t *starts = (const uint32_t *)(it.scratch + it.p[1]);
     int32_t *lengths = (int32_t *)S[it.out[1]].ptr;
@@ -801,7 +829,8 @@ template <bool DBL>
 __device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S)
 {
     const StreamDesc in = S[it.in[0]];
-    const uint64_t n = in.len / (DBL ? 8 : 4);
+    const ViewCtx vc = view_ctx<DBL ? 8 : 4>(it, in);
+    const uint64_t n = vc.n;
     const DGfc g = d_gfc_geom(DBL, n, 0, 0);
     if (tile == 0 && threadIdx.x == 0) {
         if (n) {
@@ -829,7 +858,7 @@ __device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S)
     for (uint64_t s = cb; s < ce; s += 32) {
         const uint64_t i = s + lane;
         uint64_t x = 0;
-        if (i < n) x = DBL ? ld_elem<8>(in.ptr, i) : ld_elem<4>(in.ptr, i);
+        if (i < n) x = view_elem<DBL ? 8 : 4>(it, vc, in.ptr, i);
         uint64_t diff;
         uint32_t sign, mb, code;
         if (DBL) {
@@ -883,7 +912,10 @@ __device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool d
         n = (uint64_t)(int32_t)ld_unaligned<4>(m.ptr + 8);
         if (blocks <= 0 || wpb <= 0) return;
     } else {
-        n = S[it.in[0]].len / (dbl ? 8 : 4);
+        int nd = 0;
+        for (int k = 0; k < kMaxViewOps; k++) nd += it.vop[k] == V_DELTA;
+        const uint64_t n_src = S[it.in[0]].len / (dbl ? 8 : 4);
+        n = n_src > (uint64_t)nd ? n_src - nd : 0;
     }
     const DGfc g = d_gfc_geom(dbl, n, blocks, wpb);
     // decode: p[3] = the chunks the scratch holds (a larger count is reported by the sizes pass)
@@ -916,7 +948,10 @@ __device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool d
 template <bool DBL>
 __device__ void p_gfc_compact(const BItem &it, uint32_t tile, StreamDesc *S)
 {
-    const uint64_t n = S[it.in[0]].len / (DBL ? 8 : 4);
+    int nd = 0;
+    for (int k = 0; k < kMaxViewOps; k++) nd += it.vop[k] == V_DELTA;
+    const uint64_t n_src = S[it.in[0]].len / (DBL ? 8 : 4);
+    const uint64_t n = n_src > (uint64_t)nd ? n_src - nd : 0;
     const DGfc g = d_gfc_geom(DBL, n, 0, 0);
     const int lane = threadIdx.x & 31;
     const int64_t w = (int64_t)tile * kBGfcChunks + (threadIdx.x >> 5);
@@ -932,10 +967,36 @@ __device__ void p_gfc_compact(const BItem &it, uint32_t tile, StreamDesc *S)
     if (w == g.warps - 1 && lane == 0) S[it.out[2]].len = incl[w];
 }
 
+// ------------------------------------------------------------------------------- view nodes
+// Metadata of a delta / scale node whose output is only read through its child's view: delta's
+// first value, scale's minimum (scale_min of its min / max).  One thread per item.
+template <int ES>
+__device__ void p_vmeta(const BItem &it, StreamDesc *S)
+{
+    if (threadIdx.x != 0) return;
+    const StreamDesc in = S[it.in[0]];
+    const ViewCtx vc = view_ctx<ES>(it, in);
+    StreamDesc &m = S[it.out[0]];
+    if (vc.n == 0) {
+        m.len = 0;
+        return;
+    }
+    uint64_t v;
+    if (it.mode == GTSC_DELTA) {
+        v = view_elem<ES>(it, vc, in.ptr, 0);
+    } else {
+        uint64_t mnb = 0, mxb = 0;
+        acc_minmax((const MinMaxAcc *)it.scratch, ES, ORD_INT, mnb, mxb);
+        v = scale_min(mnb, mxb, ES);
+    }
+    st_elem<ES>(m.ptr, 0, v);
+    m.len = ES;
+}
+
 // ------------------------------------------------------------------------------- dispatch
 constexpr size_t stage_smem(int op)
 {
-    return op == B_AFL_PACK ? 8 * (kBTile + 4)
+    return op == B_AFL_PACK ? 8 * (kBTile + kBTile / 16 + 8)
          : op == B_HIST     ? 12 * kBHistSmem + 8 * 4 * (kBThreads / 32)
          : op == B_TOPK     ? sizeof(Cand) * kBThreads * 4
          : op == B_SPLIT    ? 8 * kBTile
@@ -965,6 +1026,7 @@ k_bstage(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *c
     else if constexpr (OP == B_AFL_PACK) { GTSC_ES_SWITCH(p_afl_pack<E>(it, tile, S, (unsigned long long *)smem)) }
     else if constexpr (OP == B_HIST) { GTSC_ES_SWITCH(p_hist<E>(it, tile, S, status, smem)) }
     else if constexpr (OP == B_TOPK) { GTSC_ES_SWITCH(p_topk<E>(it, tile, S, smem)) }
+    else if constexpr (OP == B_VMETA) { GTSC_ES_SWITCH(p_vmeta<E>(it, S)) }
     else if constexpr (OP == B_SPLIT) { GTSC_ES_SWITCH(p_split<E>(it, tile, S, status, smem)) }
     else if constexpr (OP == B_RLE_HEADS) { GTSC_ES_SWITCH(p_rle_heads<E>(it, tile, S)) }
     else if constexpr (OP == B_RLE_LENGTHS) { p_rle_lengths(it, tile, S); }
@@ -1013,6 +1075,7 @@ void launch_batch_stage(int op, const BItem *d_items, const uint32_t *d_item_of,
         GTSC_STAGE(B_GFC_COMPRESS)
         GTSC_STAGE(B_GFC_SCAN)
         GTSC_STAGE(B_GFC_COMPACT)
+        GTSC_STAGE(B_VMETA)
 #undef GTSC_STAGE
     default:
         launch_batch_decode_stage(op, d_items, d_item_of, n_items, total_tiles, d_streams, d_counter, d_status, s);

@@ -83,6 +83,14 @@ gtsc_status gtsc_memcpy(void *dst, const void *src, uint64_t bytes, int32_t kind
     });
 }
 
+gtsc_status gtsc_memcpy_async(void *dst, const void *src, uint64_t bytes, int32_t kind, void *stream)
+{
+    return guard([&] {
+        if (kind < 1 || kind > 3) fail(GTSC_ERR_ARG, "bad copy kind");
+        if (bytes) GTSC_CUDA(cudaMemcpyAsync(dst, src, bytes, (cudaMemcpyKind)kind, S(stream)));
+    });
+}
+
 gtsc_status gtsc_stream_synchronize(void *stream)
 {
     return guard([&] { GTSC_CUDA(cudaStreamSynchronize(S(stream))); });
@@ -318,6 +326,80 @@ gtsc_status gtsc_batch_destroy(gtsc_batch *b)
         if (!b) return;
         batch_destroy(b->e);
         delete b;
+    });
+}
+
+// ------------------------------------------------------------------------------- pipeline
+struct gtsc_pipeline {
+    Pipeline *p;
+    uint32_t n_cols;
+};
+
+gtsc_status gtsc_pipeline_create(const gtsc_column *cols, uint32_t n_cols, const int16_t *nodes,
+                                 const int32_t *node_counts, int32_t groups, gtsc_pipeline **out)
+{
+    return guard([&] {
+        if (!cols || !nodes || !node_counts || !out || !n_cols) fail(GTSC_ERR_ARG, "null argument");
+        std::vector<uint64_t> bytes;
+        std::vector<int> dts;
+        std::vector<Tree> t;
+        const int16_t *p = nodes;
+        for (uint32_t i = 0; i < n_cols; i++) {
+            bytes.push_back(cols[i].bytes);
+            dts.push_back(cols[i].dtype);
+            t.push_back(tree_from_nodes(p, node_counts[i]));
+            p += 2 * node_counts[i];
+        }
+        *out = new gtsc_pipeline{pipeline_create(bytes, dts, t, groups), n_cols};
+    });
+}
+
+int32_t gtsc_pipeline_groups(gtsc_pipeline *p) { return p ? pipeline_groups(p->p) : 0; }
+
+gtsc_status gtsc_pipeline_group_columns(gtsc_pipeline *p, int32_t g, int32_t *cols, int32_t cap, int32_t *n)
+{
+    return guard([&] {
+        if (!p || !cols || !n || g < 0 || g >= pipeline_groups(p->p)) fail(GTSC_ERR_ARG, "bad argument");
+        const auto &m = pipeline_group_columns(p->p, g);
+        if ((int64_t)m.size() > cap) fail(GTSC_ERR_CAPACITY, "pipeline_group_columns: cap too small");
+        for (size_t i = 0; i < m.size(); i++) cols[i] = m[i];
+        *n = (int32_t)m.size();
+    });
+}
+
+gtsc_status gtsc_pipeline_compress_host(gtsc_pipeline *p, const void *const *host_cols, void *host_framed,
+                                        uint64_t cap, uint64_t *group_bytes)
+{
+    return guard([&] {
+        if (!p || !host_cols || !host_framed || !group_bytes) fail(GTSC_ERR_ARG, "null argument");
+        pipeline_compress_host(p->p, host_cols, (uint8_t *)host_framed, cap, group_bytes);
+    });
+}
+
+gtsc_status gtsc_pipeline_decompress(gtsc_pipeline *p)
+{
+    return guard([&] {
+        if (!p) fail(GTSC_ERR_ARG, "null argument");
+        const gtsc_status st = pipeline_decompress(p->p);
+        if (st != GTSC_OK) fail(st, "pipeline: a decode step reported an error");
+    });
+}
+
+gtsc_status gtsc_pipeline_column(gtsc_pipeline *p, int32_t c, const void **d_input, const void **d_output)
+{
+    return guard([&] {
+        if (!p || c < 0 || (uint32_t)c >= p->n_cols) fail(GTSC_ERR_ARG, "bad column");
+        if (d_input) *d_input = pipeline_column_input(p->p, c);
+        if (d_output) *d_output = pipeline_column_output(p->p, c);
+    });
+}
+
+gtsc_status gtsc_pipeline_destroy(gtsc_pipeline *p)
+{
+    return guard([&] {
+        if (!p) return;
+        pipeline_destroy(p->p);
+        delete p;
     });
 }
 

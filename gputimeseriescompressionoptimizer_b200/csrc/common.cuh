@@ -66,6 +66,12 @@ struct DevBuf {
     std::shared_ptr<DevMem> m;
     uint64_t bytes = 0;
     uint8_t *get() const { return m ? m->p : nullptr; }
+    // free on the legacy stream instead of the allocating one (for buffers that may outlive that
+    // stream; the owner synchronises the device before releasing them)
+    void release_on_default_stream()
+    {
+        if (m) m->s = nullptr;
+    }
     // give up ownership (the caller frees the pointer); returns it
     uint8_t *disown()
     {

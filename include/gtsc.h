@@ -61,6 +61,8 @@ gtsc_status gtsc_malloc(void **d_ptr, uint64_t bytes, void *stream);
 gtsc_status gtsc_free(void *d_ptr, void *stream);
 /* Copies; `kind` 1 = host->device, 2 = device->host, 3 = device->device (cudaMemcpyKind). */
 gtsc_status gtsc_memcpy(void *dst, const void *src, uint64_t bytes, int32_t kind, void *stream);
+/* The same copy, never synchronising (host memory must be pinned for it to overlap). */
+gtsc_status gtsc_memcpy_async(void *dst, const void *src, uint64_t bytes, int32_t kind, void *stream);
 gtsc_status gtsc_stream_synchronize(void *stream);
 /* A non-blocking CUDA stream (the batched steps need one they can capture on). */
 gtsc_status gtsc_stream_create(void **stream);
@@ -194,6 +196,33 @@ int32_t gtsc_batch_launches(gtsc_batch *b, int32_t compress);
 gtsc_status gtsc_batch_profile(gtsc_batch *b, int32_t compress, int32_t *ops, float *ms, uint64_t *bytes,
                                uint64_t *blocks, int32_t cap, int32_t *n, void *stream);
 gtsc_status gtsc_batch_destroy(gtsc_batch *b);
+
+/* ------------------------------------------------------------------ column-chunk pipeline */
+
+/*
+ * Column chunks from host memory to host framed output: ParallelTSCompressor::Compress's chunk loop
+ * (parallel_ts_compressor.cpp:39-63, a CompressionTask per column chunk writing size_t len + blob,
+ * optimizer/compression_task.cpp:35-77) on the batched engine.  The columns are split into `groups`
+ * of about equal bytes, each with its own batch engine and stream, so that one group's host <->
+ * device copies overlap the others' compression.  The pipeline owns the device copies of the
+ * columns (cols[].d_data is ignored; bytes and dtype fix the chunk shape).
+ */
+typedef struct gtsc_pipeline gtsc_pipeline;
+gtsc_status gtsc_pipeline_create(const gtsc_column *cols, uint32_t n_cols, const int16_t *nodes,
+                                 const int32_t *node_counts, int32_t groups, gtsc_pipeline **out);
+int32_t gtsc_pipeline_groups(gtsc_pipeline *p);
+/* The columns of group g in the order of its framed output (ascending column index). */
+gtsc_status gtsc_pipeline_group_columns(gtsc_pipeline *p, int32_t g, int32_t *cols, int32_t cap, int32_t *n);
+/* One chunk: host_cols[c] (pinned for overlap) -> host_framed = every group's framed output
+ * (column count, blob sizes, blobs) back to back, group_bytes[g] their sizes.  Synchronises. */
+gtsc_status gtsc_pipeline_compress_host(gtsc_pipeline *p, const void *const *host_cols, void *host_framed,
+                                        uint64_t cap, uint64_t *group_bytes);
+/* Decodes the last compressed chunk on the device (every group's step in flight together) into
+ * the pipeline's per-column output buffers; the first failing status is returned. */
+gtsc_status gtsc_pipeline_decompress(gtsc_pipeline *p);
+/* Device buffers of column c: its last input chunk and its last decoded output. */
+gtsc_status gtsc_pipeline_column(gtsc_pipeline *p, int32_t c, const void **d_input, const void **d_output);
+gtsc_status gtsc_pipeline_destroy(gtsc_pipeline *p);
 
 /* ------------------------------------------------------------------ learned planner */
 

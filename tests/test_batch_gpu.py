@@ -176,3 +176,62 @@ def test_batch_corrupt_frames_fail_cleanly(G, O, rng):
     b.status()
     for i, x in enumerate(cols):
         assert G.to_host(outs[i]).tobytes() == x.tobytes()
+
+
+VIEW_TREES = [
+    [OR.DELTA, OR.SCALE, OR.AFL, OR.NONE],
+    [OR.SCALE, OR.AFL, OR.NONE],
+    [OR.DELTA, OR.AFL, OR.NONE],
+    [OR.DELTA, OR.DELTA, OR.SCALE, OR.AFL, OR.NONE],
+    [OR.DELTA, OR.SCALE, OR.DELTA, OR.SCALE, OR.AFL, OR.NONE],  # one more than a view holds
+    [OR.SCALE, OR.DELTA, OR.SCALE, OR.DELTA, OR.AFL, OR.NONE],
+    [OR.DELTA, OR.RLE, OR.AFL, OR.NONE, OR.AFL, OR.NONE],
+    [OR.SCALE, OR.DICT, OR.NONE, OR.AFL, OR.NONE],
+    [OR.DELTA, OR.PATCH, OR.SCALE, OR.AFL, OR.NONE, OR.SCALE, OR.AFL, OR.NONE],
+    [OR.DELTA, OR.CONST, OR.AFL, OR.NONE],
+    [OR.DELTA, OR.SCALE, OR.NONE],
+    [OR.DELTA, OR.GFC, OR.NONE, OR.NONE],
+    [OR.SCALE, OR.SCALE, OR.AFL, OR.NONE],
+]
+
+
+def view_columns(rng, dt, n):
+    npt = OR.NP_TYPES[dt]
+    info = np.iinfo(npt)
+    walk = np.cumsum(rng.integers(-50, 51, n)).astype(np.int64)
+    yield np.clip(walk, info.min, info.max).astype(npt)
+    x = rng.integers(0, 100, n).astype(npt)  # the most negative value among small positives:
+    x[n // 3] = info.min                      # scale keeps c = min and the values wrap
+    yield x
+    y = rng.integers(info.min // 2, info.max // 2, n, dtype=np.int64).astype(npt)
+    yield y
+    yield np.repeat(rng.integers(-5, 5, n // 7 + 1), 7)[:n].astype(npt)
+
+
+@pytest.mark.parametrize("dt", [OR.CHAR, OR.SHORT, OR.INT, OR.TIME], ids=["char", "short", "int", "time"])
+def test_batch_view_chains(G, O, rng, dt):
+    """delta / scale nodes read through their child's view: the blobs stay identical to the
+    per-column trees, for chains up to the view depth and past it, and when scaling wraps"""
+    cols, dts, trees = [], [], []
+    for path in VIEW_TREES:
+        for n in [1, 2, 3, 4097, 50001]:
+            for x in view_columns(rng, dt, n):
+                cols.append(x)
+                dts.append(dt)
+                trees.append(G.tree_from_path(path, dt))
+    run_batch(G, O, cols, dts, trees)
+
+
+@pytest.mark.parametrize("dt", [OR.FLOAT, OR.DOUBLE], ids=["float", "double"])
+def test_batch_view_chains_float(G, O, rng, dt):
+    paths = [[OR.DELTA, OR.GFC, OR.NONE, OR.NONE], [OR.SCALE, OR.DELTA, OR.GFC, OR.NONE, OR.NONE],
+             [OR.DELTA, OR.DICT, OR.NONE, OR.GFC, OR.NONE, OR.NONE],
+             [OR.DELTA, OR.PATCH, OR.GFC, OR.NONE, OR.NONE, OR.GFC, OR.NONE, OR.NONE]]
+    cols, dts, trees = [], [], []
+    for path in paths:
+        for n in [1, 5, 33000]:
+            x = W.column("price", dt, n, int(rng.integers(1 << 30)))
+            cols.append(x)
+            dts.append(dt)
+            trees.append(G.tree_from_path(path, dt))
+    run_batch(G, O, cols, dts, trees)
