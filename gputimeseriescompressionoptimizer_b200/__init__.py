@@ -114,6 +114,7 @@ def lib():
         L.gtsc_pipeline_group_columns.argtypes = [vp, i32, i32p, i32, i32p]
         L.gtsc_pipeline_compress_host.argtypes = [vp, ctypes.POINTER(vp), vp, u64, u64p]
         L.gtsc_pipeline_decompress.argtypes = [vp]
+        L.gtsc_pipeline_roundtrip_host.argtypes = [vp, ctypes.POINTER(vp), vp, u64, u64p]
         L.gtsc_pipeline_column.argtypes = [vp, i32, ctypes.POINTER(vp), ctypes.POINTER(vp)]
         L.gtsc_pipeline_destroy.argtypes = [vp]
         f32p = ctypes.POINTER(ctypes.c_float)
@@ -416,6 +417,15 @@ class Pipeline:
         check(lib().gtsc_pipeline_compress_host(self.handle, arr, framed_ptr, cap,
                                                 sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))),
               "pipeline_compress_host")
+        return sizes
+
+    def roundtrip_host(self, host_ptrs, framed_ptr, cap):
+        """compress_host plus each group's device decode right after its read-back."""
+        arr = (ctypes.c_void_p * self.n)(*host_ptrs)
+        sizes = np.zeros(self.groups, np.uint64)
+        check(lib().gtsc_pipeline_roundtrip_host(self.handle, arr, framed_ptr, cap,
+                                                 sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))),
+              "pipeline_roundtrip_host")
         return sizes
 
     def decompress(self):

@@ -57,6 +57,11 @@ struct HNode {
     int8_t vop[kMaxViewOps] = {V_NONE, V_NONE, V_NONE};
     int vnode[kMaxViewOps] = {-1, -1, -1};
     bool virt = false;
+    // decode: a node whose decoded output its parent reads through a DView (an AFL node over its
+    // packed bits, a scale node as an addition) has no decode pass and no output stream
+    bool dvirt = false;
+    DView dview;        // how the parent reads this node's decoded output
+    int d_ready = 0;    // decode level from which that output can be read
 };
 
 struct Pass {
@@ -444,8 +449,32 @@ void BatchEngine::plan_passes()
     for (int id : order) {
         HNode &nd = nodes[id];
         int start = 0;
-        for (int kid : nd.kids)
-            if (nodes[kid].enc != GTSC_NONE) start = std::max(start, nodes[kid].last_d_level + 1);
+        for (int kid : nd.kids) start = std::max(start, nodes[kid].d_ready);
+        // how the parent will read this node's decoded output
+        nd.dview = DView{};
+        nd.dview.data = nd.enc == GTSC_NONE ? nd.dec_data_sid : nd.dec_out_sid;
+        if (nd.parent >= 0) {
+            const HNode &par = nodes[nd.parent];
+            const int slot = (int)(std::find(par.kids.begin(), par.kids.end(), id) - par.kids.begin()) + 1;
+            const bool consumer = par.enc == GTSC_DELTA || par.enc == GTSC_SCALE || par.enc == GTSC_PATCH ||
+                                  par.enc == GTSC_CONST || par.enc == GTSC_RLE || par.enc == GTSC_FLOAT_TO_INT ||
+                                  (par.enc == GTSC_DICT && slot == 2);
+            if (consumer && nd.enc == GTSC_AFL && nd.kids.size() == 1 && nodes[nd.kids[0]].enc == GTSC_NONE) {
+                nd.dvirt = true;
+                nd.dview.data = nodes[nd.kids[0]].dec_data_sid;
+                nd.dview.afl_meta = nd.dec_meta_sid;
+            } else if (consumer && nd.enc == GTSC_SCALE && nd.kids.size() == 1 && nodes[nd.kids[0]].dview.add[1] < 0) {
+                nd.dvirt = true;
+                nd.dview = nodes[nd.kids[0]].dview;
+                nd.dview.add[nd.dview.add[0] < 0 ? 0 : 1] = nd.dec_meta_sid;
+            }
+        }
+        if (nd.dvirt) {
+            streams[nd.dec_out_sid].cap = 0;  // never written
+            nd.d_ready = start;
+            nd.last_d_level = start - 1;
+            continue;
+        }
         const uint64_t n = nd.in_cap / nd.es;
         const uint64_t t2k = std::max<uint64_t>(1, cdiv(n, kBTile));
         auto child_out = [&](int j) {
@@ -463,6 +492,10 @@ void BatchEngine::plan_passes()
             it.in[0] = nd.dec_meta_sid;
             for (size_t j = 0; j < nd.kids.size() && j < 2; j++) it.in[j + 1] = child_out((int)j);
             it.out[0] = nd.dec_out_sid;
+            // the passes that read their children element-wise take them through DViews
+            if (op == B_DELTA_DEC || op == B_SCALE_ADD || op == B_MERGE || op == B_RLE_SCAN || op == B_RLE_EXPAND ||
+                op == B_F2I_DEC)
+                for (size_t j = 0; j < nd.kids.size() && j < 2; j++) it.dv[j] = nodes[nd.kids[j]].dview;
             return it;
         };
         std::vector<BItem> ps;
@@ -522,6 +555,7 @@ void BatchEngine::plan_passes()
         int lvl = start;
         for (auto &it : ps) pass_d.push_back(Pass{lvl++, it.op, id, it});
         nd.last_d_level = ps.empty() ? start - 1 : lvl - 1;
+        nd.d_ready = nd.enc == GTSC_NONE ? 0 : nd.last_d_level + 1;
     }
 }
 
@@ -916,6 +950,10 @@ void batch_decompress(BatchEngine *e, const uint8_t *framed, uint64_t framed_byt
 static uint64_t item_bytes(const BItem &it, const std::vector<StreamDesc> &S)
 {
     auto L = [&](int sid) -> uint64_t { return sid >= 0 ? S[sid].len : 0; };
+    auto D = [&](int slot) -> uint64_t {  // a decode input: its view's source, else the stream
+        const DView &d = it.dv[slot - 1];
+        return d.data >= 0 ? S[d.data].len : L(it.in[slot]);
+    };
     const uint64_t in = L(it.in[0]);
     switch (it.op) {
     case B_MINMAX: case B_HIST: case B_F2I_STATS: return in;
@@ -927,10 +965,11 @@ static uint64_t item_bytes(const BItem &it, const std::vector<StreamDesc> &S)
     case B_GFC_COMPRESS: return in + L(it.out[1]) + L(it.out[2]);
     case B_GFC_COMPACT: return 2 * L(it.out[2]);
     case B_NONE_COPY: return 2 * in;
-    case B_AFL_UNPACK: case B_DELTA_DEC: case B_SCALE_ADD: case B_F2I_DEC: return L(it.in[1]) + L(it.out[0]);
-    case B_MERGE: return in + L(it.in[1]) + L(it.in[2]) + L(it.out[0]);
-    case B_RLE_SCAN: return L(it.in[1]);
-    case B_RLE_EXPAND: return L(it.in[2]) + L(it.out[0]);
+    case B_AFL_UNPACK: return L(it.in[1]) + L(it.out[0]);
+    case B_DELTA_DEC: case B_SCALE_ADD: case B_F2I_DEC: return D(1) + L(it.out[0]);
+    case B_MERGE: return in + (it.mode == SPLIT_DICT ? L(it.in[1]) : D(1)) + D(2) + L(it.out[0]);
+    case B_RLE_SCAN: return D(1);
+    case B_RLE_EXPAND: return D(2) + L(it.out[0]);
     case B_GFC_SIZES: return L(it.in[1]);
     case B_GFC_DEC: return L(it.in[2]) + L(it.out[0]);
     default: return 0;

@@ -61,6 +61,17 @@ struct StreamDesc {
     uint64_t pad;
 };
 
+// How a decode pass reads one of its inputs.  data >= 0 and afl_meta < 0: the stream `data` (a
+// child's decoded stream, or a none leaf inside the blob).  afl_meta >= 0: the child is an AFL
+// node whose packed bits are `data` (its none leaf, in the blob) and whose metadata is afl_meta;
+// element i is unpacked on the fly.  add[k] >= 0: then add the value in that scale node's metadata
+// (a scale child, decoded on the fly).  data < 0: the input comes from in[] as before.
+struct DView {
+    int32_t data = -1;
+    int32_t afl_meta = -1;
+    int32_t add[2] = {-1, -1};
+};
+
 // One unit of batched work: a pass of one tree node of one column.
 struct BItem {
     uint64_t tile_base;          // first global tile of this item
@@ -75,6 +86,7 @@ struct BItem {
     int8_t vop[kMaxViewOps];     // the input view: ops applied to in[0] (compress passes)
     int8_t vflags;               // bit 0: AFL width from the view's last scale (no own min/max pass)
     uint8_t *vscr[kMaxViewOps];  // V_SCALE: that scale node's scratch (its MinMaxAcc)
+    DView dv[2];                 // decode passes: how in[1] / in[2] are read (see DView)
 };
 
 // A tree node as the framing / parse kernels see it.
@@ -146,7 +158,7 @@ void pipeline_destroy(Pipeline *p);
 int pipeline_groups(const Pipeline *p);
 const std::vector<int> &pipeline_group_columns(const Pipeline *p, int g);  // ascending column indices
 void pipeline_compress_host(Pipeline *p, const void *const *host_cols, uint8_t *host_framed, uint64_t cap,
-                            uint64_t *sizes);
+                            uint64_t *sizes, bool decode);
 gtsc_status pipeline_decompress(Pipeline *p);
 const void *pipeline_column_input(Pipeline *p, int c);
 const void *pipeline_column_output(Pipeline *p, int c);

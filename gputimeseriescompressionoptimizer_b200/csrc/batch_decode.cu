@@ -114,11 +114,13 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
 {
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
-    const StreamDesc meta = S[it.in[0]], d = S[it.in[1]];
+    const StreamDesc meta = S[it.in[0]];
+    bool ok;
+    const DViewCtx dv = dview_ctx<ES>(it, S, 1, ok);
     StreamDesc &out = S[it.out[0]];
-    const uint64_t n = meta.len ? d.len / ES + 1 : 0;
-    if (n * ES > out.cap) {  // item-uniform: no tile of this item enters the look-back
-        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+    const uint64_t n = meta.len ? dv.n + 1 : 0;
+    if (!ok || n * ES > out.cap) {  // item-uniform: no tile of this item enters the look-back
+        if (tile == 0 && threadIdx.x == 0) set_status(status, ok ? GTSC_ERR_CAPACITY : GTSC_ERR_FORMAT);
         return;
     }
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
@@ -126,7 +128,10 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     const uint64_t m = n ? n - 1 : 0;
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     uint64_t v[kBVPT];
-    load_run<ES, kBVPT>(d.ptr, base, m, v);
+    load_dview<ES, kBVPT>(dv, base, v);
+#pragma unroll
+    for (int j = 0; j < (int)kBVPT; j++)
+        if (base + j >= m) v[j] = 0;
     unsigned long long local = 0;
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) local += v[j];
@@ -152,10 +157,12 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
 template <int ES>
 __device__ void p_scale_add(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
 {
-    const StreamDesc meta = S[it.in[0]], d = S[it.in[1]];
+    const StreamDesc meta = S[it.in[0]];
+    bool ok;
+    const DViewCtx dv = dview_ctx<ES>(it, S, 1, ok);
     StreamDesc &out = S[it.out[0]];
-    const uint64_t n = d.len / ES;
-    if (n * ES > out.cap || (n && meta.len < (uint64_t)ES)) {
+    const uint64_t n = dv.n;
+    if (!ok || n * ES > out.cap || (n && meta.len < (uint64_t)ES)) {
         if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
         return;
     }
@@ -164,7 +171,7 @@ __device__ void p_scale_add(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     if (base >= n) return;
     const uint64_t mn = ld_unaligned<ES>(meta.ptr);
     uint64_t v[kBVPT];
-    load_run<ES, kBVPT>(d.ptr, base, n, v);
+    load_dview<ES, kBVPT>(dv, base, v);
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) v[j] = wrap_es(v[j] + mn, ES);
     store_run<ES, kBVPT>(out.ptr, base, n, v);
@@ -177,11 +184,21 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
     const int mode = it.mode;
-    const StreamDesc meta = S[it.in[0]], in1 = S[it.in[1]];
-    const StreamDesc in2 = mode == SPLIT_NOT_CONST ? StreamDesc{nullptr, 0, 0, 0} : S[it.in[2]];
+    const StreamDesc meta = S[it.in[0]];
+    // dictionary: in1 is the packed code stream (read plainly); otherwise both inputs may be views
+    const StreamDesc in1 = mode == SPLIT_DICT ? S[it.in[1]] : StreamDesc{nullptr, 0, 0, 0};
+    bool ok1 = true, ok2 = true;
+    DViewCtx v1{}, v2{};
+    if (mode != SPLIT_DICT) v1 = dview_ctx<ES>(it, S, 1, ok1);
+    if (mode != SPLIT_NOT_CONST) v2 = dview_ctx<ES>(it, S, 2, ok2);
     StreamDesc &out = S[it.out[0]];
+    if (!ok1 || !ok2) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+        return;
+    }
+    const uint64_t len1 = mode == SPLIT_DICT ? in1.len : v1.n * ES, len2 = v2.n * ES;
     // empty-input rules of the three Decode()s
-    const bool empty = mode == SPLIT_NOT_CONST ? meta.len == 0 : (in1.len == 0 && in2.len == 0);
+    const bool empty = mode == SPLIT_NOT_CONST ? meta.len == 0 : (len1 == 0 && len2 == 0);
     const uint8_t *stencil = mode == SPLIT_NOT_CONST ? meta.ptr + ES : meta.ptr;
     const uint64_t sbytes = mode == SPLIT_NOT_CONST ? (meta.len > (uint64_t)ES ? meta.len - ES : 0) : meta.len;
     uint64_t n = 0;
@@ -205,7 +222,7 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     }
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
     // dictionary stream: 16-byte header, 4 values, codes
-    uint64_t top[4] = {0, 0, 0, 0}, yes_cap = 0, no_cap = in2.len / ES;
+    uint64_t top[4] = {0, 0, 0, 0}, yes_cap = 0, no_cap = v2.n;
     const uint8_t *codes = nullptr;
     if (mode == SPLIT_DICT) {
         if (in1.len >= 16 + 4ull * ES) {
@@ -217,9 +234,9 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
         }
     } else if (mode == SPLIT_NOT_CONST) {
         if (meta.len >= (uint64_t)ES) top[0] = ld_unaligned<ES>(meta.ptr);
-        yes_cap = in1.len / ES;
+        yes_cap = v1.n;
     } else {
-        yes_cap = in1.len / ES;
+        yes_cap = v1.n;
     }
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
@@ -244,16 +261,14 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     const uint64_t yes0 = s_prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
     bool bad = false;
     if (mode != SPLIT_DICT) {
-        const bool al = ((uintptr_t)in1.ptr & (ES - 1)) == 0;
         for (uint64_t i = threadIdx.x; i < ny; i += kBThreads) {
-            if (yes0 + i < yes_cap) st_elem<ES>(sm, i, ld_elem_any<ES>(in1.ptr, yes0 + i, al));
+            if (yes0 + i < yes_cap) st_elem<ES>(sm, i, dview_elem<ES>(v1, yes0 + i));
             else bad = true;
         }
     }
     if (mode != SPLIT_NOT_CONST) {
-        const bool al = ((uintptr_t)in2.ptr & (ES - 1)) == 0;
         for (uint64_t i = threadIdx.x; i < nn; i += kBThreads) {
-            if (no0 + i < no_cap) st_elem<ES>(sm, ny + i, ld_elem_any<ES>(in2.ptr, no0 + i, al));
+            if (no0 + i < no_cap) st_elem<ES>(sm, ny + i, dview_elem<ES>(v2, no0 + i));
             else bad = true;
         }
     }
@@ -272,7 +287,8 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
                         bad = true;
                     } else {
                         const uint32_t w = (uint32_t)ld_unaligned<4>(codes + 4 * (y >> 4));
-                        v[j] = top[(w >> (2 * (y & 15))) & 3u];
+                        const uint32_t c = (w >> (2 * (y & 15))) & 3u;  // select, not an indexed array
+                        v[j] = c == 0 ? top[0] : c == 1 ? top[1] : c == 2 ? top[2] : top[3];
                     }
                 } else if (ly < ny) {
                     v[j] = ld_elem_sm<ES>(sm, ly);
@@ -295,11 +311,22 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
 {
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
-    const StreamDesc meta = S[it.in[0]], lengths = S[it.in[1]], values = S[it.in[2]];
+    const StreamDesc meta = S[it.in[0]];
+    bool ok1, ok2;
+    const DViewCtx lengths = dview_ctx<4>(it, S, 1, ok1);  // int32 run lengths
+    uint64_t n_values = 0;
+    switch (it.es) {  // the values' count (their element size is the node's)
+    case 1: n_values = dview_ctx<1>(it, S, 2, ok2).n; break;
+    case 2: n_values = dview_ctx<2>(it, S, 2, ok2).n; break;
+    case 4: n_values = dview_ctx<4>(it, S, 2, ok2).n; break;
+    default: n_values = dview_ctx<8>(it, S, 2, ok2).n; break;
+    }
     int64_t runs = 0;
-    if (lengths.len) {
+    if (!ok1 || !ok2) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+    } else if (lengths.n) {
         runs = meta.len >= 4 ? (int32_t)ld_unaligned<4>(meta.ptr) : -1;
-        if (runs < 0 || (uint64_t)runs * 4 > lengths.len || (uint64_t)runs * it.es > values.len) {
+        if (runs < 0 || (uint64_t)runs > lengths.n || (uint64_t)runs > n_values) {
             if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
             runs = 0;
         }
@@ -312,7 +339,7 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
     bool neg = false;
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) {
-        v[j] = base + j < (uint64_t)runs ? (long long)(int32_t)ld_unaligned<4>(lengths.ptr + 4 * (base + j)) : 0;
+        v[j] = base + j < (uint64_t)runs ? (long long)(int32_t)dview_elem<4>(lengths, base + j) : 0;
         neg |= v[j] < 0;
         local += (unsigned long long)v[j];
     }
@@ -338,7 +365,8 @@ template <int ES>
 __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
 {
     __shared__ uint64_t s_lo, s_hi;
-    const StreamDesc values = S[it.in[2]];
+    bool ok;
+    const DViewCtx values = dview_ctx<ES>(it, S, 2, ok);
     StreamDesc &out = S[it.out[0]];
     const uint64_t runs = *(const unsigned long long *)(it.scratch + it.p[2]);
     const unsigned long long *ends = (const unsigned long long *)(it.scratch + it.p[1]);
@@ -367,14 +395,13 @@ __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint
     __syncthreads();
     const uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT;
     if (base >= n) return;
-    const bool val_al = ((uintptr_t)values.ptr & (ES - 1)) == 0;
     uint64_t r = ub(s_lo, s_hi, base);
     uint64_t v[kBVPT];
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) {
         const uint64_t i = base + j;
         while (r < runs && ends[r] <= i) ++r;
-        v[j] = (i < n && r < runs) ? ld_elem_any<ES>(values.ptr, r, val_al) : 0;
+        v[j] = (i < n && r < runs && r < values.n) ? dview_elem<ES>(values, r) : 0;
     }
     store_run<ES, kBVPT>(out.ptr, base, n, v);
     (void)status;
@@ -391,9 +418,15 @@ __device__ void p_f2i_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
         p10[threadIdx.x] = v;
     }
     __syncthreads();
-    const StreamDesc meta = S[it.in[0]], d = S[it.in[1]];
+    const StreamDesc meta = S[it.in[0]];
+    bool ok;
+    const DViewCtx d = dview_ctx<4>(it, S, 1, ok);  // the child's int32 stream
     StreamDesc &out = S[it.out[0]];
-    if (d.len == 0) {
+    if (!ok) {
+        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+        return;
+    }
+    if (d.n == 0) {
         if (tile == 0 && threadIdx.x == 0) out.len = 0;
         return;
     }
@@ -402,7 +435,7 @@ __device__ void p_f2i_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
         if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
         return;
     }
-    const uint64_t n = p < 10 ? d.len / 4 : d.len / ES;
+    const uint64_t n = p < 10 ? d.n : d.n * 4 / ES;
     if (n * ES > out.cap) {
         if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
         return;
@@ -410,17 +443,22 @@ __device__ void p_f2i_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     const Order o = (Order)it.order;
-    const bool d_al = ((uintptr_t)d.ptr & 3) == 0;
     for (int j = 0; j < (int)kBVPT && base + j < n; j++) {
         uint64_t v;
         if (p < 10) {
-            const int k = (int32_t)ld_elem_any<4>(d.ptr, base + j, d_al);
+            const int k = (int32_t)dview_elem<4>(d, base + j);
             if (o == ORD_F32) v = __float_as_uint(__double2float_rn(__ddiv_rn((double)__int2float_rn(k), p10[p])));
             else if (o == ORD_F64) v = (uint64_t)__double_as_longlong(__ddiv_rn((double)k, p10[p]));
             else if (ES == 8) v = (uint64_t)__double2ll_rz(__ddiv_rn((double)k, p10[p]));
             else v = (uint64_t)(long long)__double2int_rz(__ddiv_rn((double)sext((uint64_t)(long long)k, ES), p10[p]));
-        } else {
-            v = ld_elem_any<ES>(d.ptr, base + j, ((uintptr_t)d.ptr & (ES - 1)) == 0);
+        } else if (ES == 8) {  // raw bytes: two int32 per element
+            v = dview_elem<4>(d, 2 * (base + j)) | (dview_elem<4>(d, 2 * (base + j) + 1) << 32);
+        } else if (ES == 4) {
+            v = dview_elem<4>(d, base + j);
+        } else {  // 1- and 2-byte elements inside the int32 words
+            constexpr uint64_t emask = ES >= 8 ? ~0ull : ((1ull << (8 * (ES % 8))) - 1);
+            const uint64_t byte = (base + j) * ES;
+            v = (dview_elem<4>(d, byte / 4) >> (8 * (byte % 4))) & emask;
         }
         st_elem<ES>(out.ptr, base + j, v);
     }

@@ -298,6 +298,107 @@ __device__ __forceinline__ uint64_t view_elem(const BItem &it, const ViewCtx &vc
     return x[0];
 }
 
+// ------------------------------------------------------------------------------- decode views
+// A decode input read through its DView (or plainly through in[slot]).
+struct DViewCtx {
+    const uint8_t *p;      // plain: the stream; AFL: the packed words (rounded down to 4 bytes)
+    uint64_t n;            // elements
+    uint64_t bytes;        // AFL: readable bytes from p
+    uint64_t off_bits;     // AFL: bit offset of value 0 from p
+    uint64_t mask;
+    uint64_t c0, c1;       // constants added (0 when absent: addition of 0 is the identity)
+    int b;                 // AFL bit width; 0 = plain
+    bool aligned;          // plain: element aligned
+};
+
+// ok = false when AFL metadata is malformed (the view is then empty)
+template <int ES>
+__device__ __forceinline__ DViewCtx dview_ctx(const BItem &it, const StreamDesc *S, int slot, bool &ok)
+{
+    DViewCtx v{};
+    ok = true;
+    const DView &d = it.dv[slot - 1];
+    if (d.data < 0) {  // no view: the input stream itself
+        const StreamDesc in = S[it.in[slot]];
+        v.p = in.ptr;
+        v.n = in.len / ES;
+        v.aligned = ((uintptr_t)in.ptr & (ES - 1)) == 0;
+        return v;
+    }
+    const StreamDesc data = S[d.data];
+    if (d.afl_meta < 0) {
+        v.p = data.ptr;
+        v.n = data.len / ES;
+        v.aligned = ((uintptr_t)data.ptr & (ES - 1)) == 0;
+    } else {
+        const StreamDesc meta = S[d.afl_meta];
+        if (data.len) {
+            const int b = meta.len >= 2 ? (int8_t)meta.ptr[0] : 0, rest = meta.len >= 2 ? (int8_t)meta.ptr[1] : 0;
+            const int64_t bits = (int64_t)data.len * 8 - rest;
+            if (b < 1 || b > 8 * ES || bits < 0) {
+                ok = false;
+            } else {
+                const uintptr_t mis = (uintptr_t)data.ptr & 3;
+                v.p = data.ptr - mis;
+                v.bytes = data.len + mis;
+                v.off_bits = 8 * mis;
+                v.b = b;
+                v.mask = b >= 64 ? ~0ull : ((1ull << b) - 1);
+                v.n = (uint64_t)bits / b;
+            }
+        }
+    }
+    if (d.add[0] >= 0) {
+        const StreamDesc m = S[d.add[0]];
+        v.c0 = m.len >= (uint64_t)ES ? ld_unaligned<ES>(m.ptr) : 0;
+    }
+    if (d.add[1] >= 0) {
+        const StreamDesc m = S[d.add[1]];
+        v.c1 = m.len >= (uint64_t)ES ? ld_unaligned<ES>(m.ptr) : 0;
+    }
+    return v;
+}
+
+template <int ES>
+__device__ __forceinline__ uint64_t dview_elem(const DViewCtx &v, uint64_t i)
+{
+    uint64_t x;
+    if (v.b == 0) {
+        x = v.aligned ? ld_elem<ES>(v.p, i) : ld_unaligned<ES>(v.p + i * ES);
+    } else {
+        const StreamReader rd{(const uint32_t *)v.p, v.bytes};
+        const uint64_t pos = v.off_bits + i * (uint64_t)v.b;
+        const uint64_t w = pos >> 5;
+        const uint32_t s = (uint32_t)(pos & 31);
+        if (v.b <= 32) {
+            const uint32_t lo = rd.word(w);
+            const uint32_t hi = (s + v.b > 32) ? rd.word(w + 1) : 0u;
+            x = __funnelshift_r(lo, hi, s) & v.mask;
+        } else {
+            const uint64_t q0 = (uint64_t)rd.word(w) | ((uint64_t)rd.word(w + 1) << 32);
+            uint64_t y = q0 >> s;
+            if (s + v.b > 64) y |= (uint64_t)rd.word(w + 2) << (64 - s);
+            x = y & v.mask;
+        }
+    }
+    return wrap_es(x + v.c0 + v.c1, ES);
+}
+
+// elements [base, base + VPT) of the view (0 past its end)
+template <int ES, int VPT>
+__device__ __forceinline__ void load_dview(const DViewCtx &v, uint64_t base, uint64_t (&out)[VPT])
+{
+    if (v.b == 0 && v.aligned) {
+        load_run<ES, VPT>(v.p, base, v.n, out);
+        const uint64_t c = v.c0 + v.c1;
+#pragma unroll
+        for (int j = 0; j < VPT; j++) out[j] = wrap_es(out[j] + c, ES);
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < VPT; j++) out[j] = base + j < v.n ? dview_elem<ES>(v, base + j) : 0;
+}
+
 // the stage kernel skeleton: finds this block's (item, tile).  DYN passes take tiles in claim
 // order from a counter (look-back needs every predecessor claimed first), the others use the
 // block index; item_of[t] is the item of global tile t (one table per launch), and for DYN launches

@@ -372,7 +372,16 @@ gtsc_status gtsc_pipeline_compress_host(gtsc_pipeline *p, const void *const *hos
 {
     return guard([&] {
         if (!p || !host_cols || !host_framed || !group_bytes) fail(GTSC_ERR_ARG, "null argument");
-        pipeline_compress_host(p->p, host_cols, (uint8_t *)host_framed, cap, group_bytes);
+        pipeline_compress_host(p->p, host_cols, (uint8_t *)host_framed, cap, group_bytes, false);
+    });
+}
+
+gtsc_status gtsc_pipeline_roundtrip_host(gtsc_pipeline *p, const void *const *host_cols, void *host_framed,
+                                         uint64_t cap, uint64_t *group_bytes)
+{
+    return guard([&] {
+        if (!p || !host_cols || !host_framed || !group_bytes) fail(GTSC_ERR_ARG, "null argument");
+        pipeline_compress_host(p->p, host_cols, (uint8_t *)host_framed, cap, group_bytes, true);
     });
 }
 

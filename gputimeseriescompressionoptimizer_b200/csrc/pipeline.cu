@@ -93,7 +93,7 @@ const std::vector<int> &pipeline_group_columns(const Pipeline *p, int g) { retur
 // in order, that group's framed output (column count, blob sizes, blobs), back to back; *sizes
 // (groups entries) their bytes.  Host memory should be pinned for the copies to overlap.
 void pipeline_compress_host(Pipeline *p, const void *const *host_cols, uint8_t *host_framed, uint64_t cap,
-                            uint64_t *sizes)
+                            uint64_t *sizes, bool decode)
 {
     const int G = p->groups;
     for (int g = 0; g < G; g++) {
@@ -112,6 +112,11 @@ void pipeline_compress_host(Pipeline *p, const void *const *host_cols, uint8_t *
         p->framed[g] = batch_output(p->eng[g]);
         p->framed_bytes[g] = nb;
         GTSC_CUDA(cudaMemcpyAsync(host_framed + off, p->framed[g], nb, cudaMemcpyDeviceToHost, p->st[g]));
+        if (decode) {  // the round trip: this group's device decode runs while later groups copy
+            std::vector<void *> outs;
+            for (int c : p->members[g]) outs.push_back(p->d_out[c].get());
+            batch_decompress(p->eng[g], p->framed[g], nb, outs, p->st[g]);
+        }
         sizes[g] = nb;
         off += nb;
     }
@@ -119,7 +124,8 @@ void pipeline_compress_host(Pipeline *p, const void *const *host_cols, uint8_t *
     for (int g = 0; g < G; g++) {
         if (!p->eng[g]) continue;
         const gtsc_status st = batch_status(p->eng[g], p->st[g]);
-        if (st != GTSC_OK) fail(st, "pipeline: a compress step reported an error");
+        if (st != GTSC_OK) fail(st, decode ? "pipeline: a compress or decode step reported an error"
+                                           : "pipeline: a compress step reported an error");
     }
 }
 

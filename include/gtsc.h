@@ -217,6 +217,10 @@ gtsc_status gtsc_pipeline_group_columns(gtsc_pipeline *p, int32_t g, int32_t *co
  * (column count, blob sizes, blobs) back to back, group_bytes[g] their sizes.  Synchronises. */
 gtsc_status gtsc_pipeline_compress_host(gtsc_pipeline *p, const void *const *host_cols, void *host_framed,
                                         uint64_t cap, uint64_t *group_bytes);
+/* The same chunk plus, per group right after its framed output is read back, the device decode
+ * of that output into the per-column output buffers (a verified round trip of the chunk). */
+gtsc_status gtsc_pipeline_roundtrip_host(gtsc_pipeline *p, const void *const *host_cols, void *host_framed,
+                                         uint64_t cap, uint64_t *group_bytes);
 /* Decodes the last compressed chunk on the device (every group's step in flight together) into
  * the pipeline's per-column output buffers; the first failing status is returned. */
 gtsc_status gtsc_pipeline_decompress(gtsc_pipeline *p);
