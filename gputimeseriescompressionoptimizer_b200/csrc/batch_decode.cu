@@ -124,6 +124,8 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
         return;
     }
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
+    // a tile past the output has no successor waiting on its look-back descriptor
+    if (tile > 0 && (uint64_t)tile * kBTile >= n) return;
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     const uint64_t m = n ? n - 1 : 0;
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
@@ -238,6 +240,7 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     } else {
         yes_cap = v1.n;
     }
+    if (tile > 0 && (uint64_t)tile * kBTile >= n) return;  // past the output: no successor waits on it
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     const uint32_t valid_mask = base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
@@ -332,6 +335,7 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
         }
     }
     unsigned long long *ends = (unsigned long long *)(it.scratch + it.p[1]);
+    if (tile > 0 && (uint64_t)tile * kBTile >= (uint64_t)runs) return;  // past the runs
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     long long v[kBVPT];

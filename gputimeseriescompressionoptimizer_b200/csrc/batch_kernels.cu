@@ -479,6 +479,9 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
             if (mode != SPLIT_NOT_CONST) S[it.out[2]].len = 0;
         }
     }
+    // a tile past the input has no successor waiting on its look-back descriptor (every later
+    // tile is past the input too), so it leaves at once; grids are sized for the worst case
+    if (tile > 0 && (uint64_t)tile * kBTile >= n) return;
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     uint64_t v[kBVPT];
     load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
@@ -607,6 +610,7 @@ __device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
         }
         return;
     }
+    if ((uint64_t)tile * kBTile >= n) return;  // past the input: no successor needs this tile
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     uint64_t v[kBVPT];
     load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
@@ -920,6 +924,7 @@ __device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool d
     const DGfc g = d_gfc_geom(dbl, n, blocks, wpb);
     // decode: p[3] = the chunks the scratch holds (a larger count is reported by the sizes pass)
     if (decode && (uint64_t)g.warps > it.p[3]) return;
+    if (tile > 0 && (uint64_t)tile * kBTile >= (uint64_t)g.warps) return;  // past the chunks
     const int32_t *sizes = (const int32_t *)(it.scratch + it.p[1]);
     unsigned long long *incl = (unsigned long long *)(it.scratch + it.p[2]);
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
