@@ -580,17 +580,98 @@ __device__ __forceinline__ void parse_fail(uint32_t *status)
     atomicExch(status + 1, 1u);
 }
 
+// elements a decode input holds (a DView or in[slot]); 0 when its AFL metadata is malformed
+__device__ __forceinline__ uint64_t dview_len(const BItem &it, const StreamDesc *S, int slot, int es)
+{
+    const DView &d = it.dv[slot - 1];
+    if (d.data < 0) return S[it.in[slot]].len / es;
+    const StreamDesc data = S[d.data];
+    if (d.afl_meta < 0) return data.len / es;
+    const StreamDesc meta = S[d.afl_meta];
+    if (!data.len || meta.len < 2) return 0;
+    const int b = (int8_t)meta.ptr[0], rest = (int8_t)meta.ptr[1];
+    const int64_t bits = (int64_t)data.len * 8 - rest;
+    return (b < 1 || b > 8 * es || bits < 0) ? 0 : (uint64_t)bits / b;
+}
+
+// Tiles of an item that do work in a decode pass (tile 0 always runs: it sets the output length).
+template <int OP>
+__device__ __forceinline__ uint32_t dec_extent(const BItem &it, const StreamDesc *S)
+{
+    auto cdiv = [](uint64_t a, uint64_t b) { return (a + b - 1) / b; };
+    uint64_t e = it.tiles;
+    if constexpr (OP == B_SCALE_ADD) {
+        e = cdiv(dview_len(it, S, 1, it.es), kBTile);
+    } else if constexpr (OP == B_AFL_UNPACK) {
+        const StreamDesc data = S[it.in[1]], meta = S[it.in[0]];
+        uint64_t n = 0;
+        if (data.len && meta.len >= 2) {
+            const int b = (int8_t)meta.ptr[0], rest = (int8_t)meta.ptr[1];
+            const int64_t bits = (int64_t)data.len * 8 - rest;
+            if (b >= 1 && b <= 8 * it.es && bits >= 0) n = (uint64_t)bits / b;
+        }
+        e = cdiv(n, kBTile);
+    } else if constexpr (OP == B_RLE_EXPAND) {
+        const uint64_t runs = *(const unsigned long long *)(it.scratch + it.p[2]);
+        const uint64_t n = runs ? ((const unsigned long long *)(it.scratch + it.p[1]))[runs - 1] : 0;
+        e = cdiv(n, kBTile);
+    } else if constexpr (OP == B_F2I_DEC) {
+        const StreamDesc meta = S[it.in[0]];
+        const int p = meta.len >= 4 ? (int32_t)ld_unaligned<4>(meta.ptr) : 0;
+        const uint64_t k = dview_len(it, S, 1, 4);
+        e = cdiv(p < 10 ? k : k * 4 / it.es, kBTile);
+    }
+    if (e == 0) e = 1;
+    return (uint32_t)(e < it.tiles ? e : it.tiles);
+}
+
+template <int OP>
+__device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status,
+                                        unsigned char *smem);
+
+constexpr bool dec_persistent(int op)
+{
+    return op == B_AFL_UNPACK || op == B_SCALE_ADD || op == B_F2I_DEC || op == B_RLE_EXPAND;
+}
+
+// One launch of a decode pass over every item: look-back passes one tile per block in claim order,
+// the others persistent over the tiles (see k_bstage).
 template <int OP>
 __global__ void __launch_bounds__(kBThreads, 3)
-k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status)
+k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status,
+       uint32_t total_tiles)
 {
     constexpr bool DYN = OP == B_DELTA_DEC || OP == B_MERGE || OP == B_RLE_SCAN;
     __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : 16];
     if (*(volatile uint32_t *)(status + 1)) return;
-    BItem it;
-    uint32_t tile;
-    locate<DYN>(items, item_of, counter, it, tile);
-    if (tile >= it.tiles) return;
+    if constexpr (!dec_persistent(OP)) {
+        BItem it;
+        uint32_t tile;
+        locate<DYN>(items, item_of, counter, it, tile);
+        if (tile >= it.tiles) return;
+        run_dec<OP>(it, tile, S, status, smem);
+    } else {
+        uint32_t t = blockIdx.x;
+        while (t < total_tiles) {
+            const BItem it = items[item_of[t]];
+            const uint32_t tile = t - (uint32_t)it.tile_base;
+            if (tile >= dec_extent<OP>(it, S)) {
+                const uint64_t next = it.tile_base + it.tiles;
+                if (next >= total_tiles) break;
+                t = (uint32_t)(next + (blockIdx.x + gridDim.x - next % gridDim.x) % gridDim.x);
+                continue;
+            }
+            run_dec<OP>(it, tile, S, status, smem);
+            __syncthreads();
+            t += gridDim.x;
+        }
+    }
+}
+
+template <int OP>
+__device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status,
+                                        unsigned char *smem)
+{
 #define GTSC_ES_SWITCH(CALL)                       \
     switch (it.es) {                               \
     case 1: { constexpr int E = 1; CALL; } break;  \
@@ -781,16 +862,30 @@ __global__ void k_zero_ranges(const unsigned long long *ranges, int n)
 
 }  // namespace
 
+// as many blocks as fit at once for the streaming decode passes, else one block per tile
+template <class K>
+unsigned stage_grid_dec(K kernel, int op, uint64_t total_tiles)
+{
+    if (!dec_persistent(op)) return (unsigned)total_tiles;
+    int per_sm = 0;
+    GTSC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBThreads, 0));
+    const uint64_t resident = (uint64_t)(per_sm > 1 ? per_sm : 1) * (uint64_t)sm_count();
+    return (unsigned)(total_tiles < resident ? total_tiles : resident);
+}
+
 void launch_batch_decode_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items,
                                uint64_t total_tiles, StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status,
                                cudaStream_t s)
 {
     if (n_items == 0 || total_tiles == 0) return;
     if (total_tiles > 0x7fffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles in one stage");
-    const unsigned g = (unsigned)total_tiles;
     switch (op) {
-#define GTSC_STAGE(OPC) \
-    case OPC: k_bdec<OPC><<<g, kBThreads, 0, s>>>(d_items, d_item_of, d_streams, d_counter, d_status); break;
+#define GTSC_STAGE(OPC)                                                                                            \
+    case OPC: {                                                                                                    \
+        const unsigned g = stage_grid_dec(k_bdec<OPC>, OPC, total_tiles);                                          \
+        k_bdec<OPC><<<g, kBThreads, 0, s>>>(d_items, d_item_of, d_streams, d_counter, d_status, (uint32_t)total_tiles); \
+        break;                                                                                                     \
+    }
         GTSC_STAGE(B_NONE_COPY)
         GTSC_STAGE(B_AFL_UNPACK)
         GTSC_STAGE(B_DELTA_DEC)

@@ -8,6 +8,7 @@
 // Byte layouts are the per-encoding ones of encodings.cu (and of the reference).
 #include "batch_dev.cuh"
 
+#include <algorithm>
 #include <type_traits>
 
 namespace gtsc {
@@ -119,11 +120,16 @@ __device__ void p_afl_pack(const BItem &it, uint32_t tile, StreamDesc *S, unsign
         // [min, max]; c = min maps onto [0, max - min], unless max - min passes the type's largest
         // value (scale_min keeps c = min for the most negative min): then values wrap negative
         // and the width is the full word, as BITLEN gives for any negative minimum
-        int last = 0;
+        // the last scale of the view (static indices: no local-memory copy of the context)
+        uint64_t c = 0;
+        const uint8_t *scr = nullptr;
+#pragma unroll
         for (int k = 0; k < kMaxViewOps; k++)
-            if (it.vop[k] == V_SCALE) last = k;
-        acc_minmax((const MinMaxAcc *)it.vscr[last], ES, ORD_INT, mnb, mxb);
-        const uint64_t c = vc.c[last];
+            if (it.vop[k] == V_SCALE) {
+                c = vc.c[k];
+                scr = it.vscr[k];
+            }
+        acc_minmax((const MinMaxAcc *)scr, ES, ORD_INT, mnb, mxb);
         if (c == 0) {
             b = bitlen_signed(sext(mnb, ES), sext(mxb, ES), ES);
         } else {
@@ -542,17 +548,19 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
         // thread's range is stored, a shared one is merged with atomicOr (the words start zeroed)
         uint32_t *words = (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES);
         const uint64_t y0 = yes0 + excl, y1 = y0 + __popc(yes_bits);
-        uint32_t acc[2] = {0u, 0u};
+        uint32_t acc0 = 0u, acc1 = 0u;  // the first and the second code word of the range
         uint64_t y = y0;
 #pragma unroll
         for (int j = 0; j < (int)kBVPT; j++)
             if ((yes_bits >> j) & 1u) {
-                acc[(y >> 4) - (y0 >> 4)] |= ((codes >> (2 * j)) & 3u) << (2 * (y & 15));
+                const uint32_t bits2 = ((codes >> (2 * j)) & 3u) << (2 * (y & 15));
+                if ((y >> 4) == (y0 >> 4)) acc0 |= bits2;
+                else acc1 |= bits2;
                 ++y;
             }
         if (y1 > y0) {
             for (uint64_t w = y0 >> 4; w <= (y1 - 1) >> 4; w++) {
-                const uint32_t a = acc[w - (y0 >> 4)];
+                const uint32_t a = w == (y0 >> 4) ? acc0 : acc1;
                 if (16 * w >= y0 && 16 * w + 16 <= y1) words[w] = a;
                 else if (a) atomicOr(words + w, a);
             }
@@ -1008,16 +1016,87 @@ constexpr size_t stage_smem(int op)
                             : 16;
 }
 
+// Tiles of an item that do work in a pass (the grid is sized for worst-case capacities; the real
+// stream lengths are only known on the device).  Tile 0 of a pass that writes metadata always
+// runs.  Passes not listed run every reserved tile.
+template <int OP>
+__device__ __forceinline__ uint32_t stage_extent(const BItem &it, const StreamDesc *S)
+{
+    auto cdiv = [](uint64_t a, uint64_t b) { return (a + b - 1) / b; };
+    auto view_n = [&]() {
+        int nd = 0;
+        for (int k = 0; k < kMaxViewOps; k++) nd += it.vop[k] == V_DELTA;
+        const uint64_t n_src = S[it.in[0]].len / it.es;
+        return n_src > (uint64_t)nd ? n_src - nd : 0;
+    };
+    uint64_t e = it.tiles;
+    if constexpr (OP == B_MINMAX) e = cdiv(view_n(), kBMinMaxTile);
+    else if constexpr (OP == B_DELTA_ENC) {
+        const uint64_t n = view_n();
+        e = cdiv(n ? n - 1 : 0, kBTile);
+        if (e == 0) e = 1;
+    } else if constexpr (OP == B_SCALE_SUB || OP == B_AFL_PACK || OP == B_F2I_ENC || OP == B_F2I_RAW) {
+        e = cdiv(view_n(), kBTile);
+        if (e == 0) e = 1;
+    } else if constexpr (OP == B_F2I_STATS) e = cdiv(view_n(), kBTile);
+    else if constexpr (OP == B_RLE_LENGTHS) e = cdiv(S[it.out[1]].len / 4, kBTile);
+    else if constexpr (OP == B_GFC_COMPRESS || OP == B_GFC_COMPACT) {
+        const DGfc g = d_gfc_geom(it.es == 8, view_n(), 0, 0);
+        e = cdiv((uint64_t)g.warps, kBGfcChunks);
+        if (OP == B_GFC_COMPRESS && e == 0) e = 1;
+    }
+    return (uint32_t)(e < it.tiles ? e : it.tiles);
+}
+
+template <int OP>
+__device__ __forceinline__ void run_stage(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status,
+                                          unsigned char *smem);
+
+// passes whose tiles all do the same streaming work run persistent grids (see stage_grid)
+constexpr bool stage_persistent(int op)
+{
+    return op == B_MINMAX || op == B_DELTA_ENC || op == B_SCALE_SUB || op == B_AFL_PACK || op == B_F2I_STATS ||
+           op == B_F2I_ENC || op == B_F2I_RAW || op == B_RLE_LENGTHS;
+}
+
+// One launch of a pass over every item.  Look-back passes take one tile per block in claim order;
+// the others are persistent: an occupancy-sized grid strides over the tiles, skipping from a tile
+// past its item's real extent straight to its first tile of the next item.
 template <int OP>
 __global__ void __launch_bounds__(kBThreads, 3)
-k_bstage(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status)
+k_bstage(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status,
+         uint32_t total_tiles)
 {
     constexpr bool DYN = OP == B_SPLIT || OP == B_RLE_HEADS || OP == B_GFC_SCAN;
     __shared__ __align__(16) unsigned char smem[stage_smem(OP)];
-    BItem it;
-    uint32_t tile;
-    locate<DYN>(items, item_of, counter, it, tile);
-    if (tile >= it.tiles) return;
+    if constexpr (!stage_persistent(OP)) {
+        BItem it;
+        uint32_t tile;
+        locate<DYN>(items, item_of, counter, it, tile);
+        if (tile >= it.tiles) return;
+        run_stage<OP>(it, tile, S, status, smem);
+    } else {
+        uint32_t t = blockIdx.x;
+        while (t < total_tiles) {
+            const BItem it = items[item_of[t]];
+            const uint32_t tile = t - (uint32_t)it.tile_base;
+            if (tile >= stage_extent<OP>(it, S)) {
+                const uint64_t next = it.tile_base + it.tiles;  // the next item's first tile
+                if (next >= total_tiles) break;
+                t = (uint32_t)(next + (blockIdx.x + gridDim.x - next % gridDim.x) % gridDim.x);
+                continue;
+            }
+            run_stage<OP>(it, tile, S, status, smem);
+            __syncthreads();  // the next tile reuses the shared memory
+            t += gridDim.x;
+        }
+    }
+}
+
+template <int OP>
+__device__ __forceinline__ void run_stage(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status,
+                                          unsigned char *smem)
+{
 #define GTSC_ES_SWITCH(CALL)                       \
     switch (it.es) {                               \
     case 1: { constexpr int E = 1; CALL; } break;  \
@@ -1056,15 +1135,32 @@ void launch_batch_decode_stage(int op, const BItem *d_items, const uint32_t *d_i
                                uint64_t total_tiles, StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status,
                                cudaStream_t s);
 
+// Grid of a stage launch: as many blocks as can be resident at once for the streaming passes (the
+// kernel strides over the tiles), else one block per tile (look-back passes claim each tile once).
+template <class K>
+unsigned stage_grid(K kernel, int op, uint64_t total_tiles)
+{
+    // persistent where every tile does the same streaming work; one block per tile where tiles differ
+    // a lot (GFC chunks, histograms, top-k) and independent blocks balance better
+    if (!stage_persistent(op)) return (unsigned)total_tiles;
+    int per_sm = 0;
+    GTSC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBThreads, 0));
+    const uint64_t resident = (uint64_t)std::max(per_sm, 1) * (uint64_t)sm_count();
+    return (unsigned)std::min<uint64_t>(total_tiles, resident);
+}
+
 void launch_batch_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items, uint64_t total_tiles,
                         StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status, cudaStream_t s)
 {
     if (n_items == 0 || total_tiles == 0) return;
     if (total_tiles > 0x7fffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles in one stage");
-    const unsigned g = (unsigned)total_tiles;
     switch (op) {
-#define GTSC_STAGE(OPC) \
-    case OPC: k_bstage<OPC><<<g, kBThreads, 0, s>>>(d_items, d_item_of, d_streams, d_counter, d_status); break;
+#define GTSC_STAGE(OPC)                                                                                              \
+    case OPC: {                                                                                                      \
+        const unsigned g = stage_grid(k_bstage<OPC>, OPC, total_tiles);                                              \
+        k_bstage<OPC><<<g, kBThreads, 0, s>>>(d_items, d_item_of, d_streams, d_counter, d_status, (uint32_t)total_tiles); \
+        break;                                                                                                       \
+    }
         GTSC_STAGE(B_MINMAX)
         GTSC_STAGE(B_DELTA_ENC)
         GTSC_STAGE(B_SCALE_SUB)
