@@ -96,6 +96,11 @@ def lib():
         L.gtsc_sample_bytes.argtypes = [i32, u64]
         L.gtsc_sample_bytes.restype = u64
         L.gtsc_delta_decode_noalloc.argtypes = [i32, vp, vp, u64, vp, vp]
+        L.gtsc_afl32_bytes.argtypes = [i32, u32, u64]
+        L.gtsc_afl32_bytes.restype = u64
+        L.gtsc_afl32_compress_gpu.argtypes = [i32, u32, vp, u64, vp, u64, vp]
+        L.gtsc_afl32_decompress_gpu.argtypes = [i32, u32, vp, u64, vp, u64, vp]
+        L.gtsc_afl_values_gpu.argtypes = [i32, u32, i32, vp, u64, vp, u64, vp, vp]
         L.gtsc_stream_create.argtypes = [ctypes.POINTER(vp)]
         L.gtsc_stream_destroy.argtypes = [vp]
         L.gtsc_batch_create.argtypes = [ctypes.POINTER(Column), ctypes.c_uint32, i16p, i32p,
@@ -189,6 +194,50 @@ def to_host(buf, dtype=np.uint8, stream=None):
 
 def dtype_size(dtype):
     return lib().gtsc_dtype_size(dtype)
+
+
+def afl_pack(dtype, bit_length, data, n, omega=32, stream=None):
+    """Pack n integer elements into the FL (omega 1, run_afl_compress_gpu<T,1>) or aligned (omega 32,
+    run_afl_compress_gpu<T,32>) layout of compression/afl/afl_gpu.cu -> DeviceBuffer."""
+    L = lib()
+    es = dtype_size(dtype)
+    if omega == 32:
+        nb = L.gtsc_afl32_bytes(dtype, bit_length, n)
+        out = alloc(max(nb, es), stream)
+        check(L.gtsc_afl32_compress_gpu(dtype, bit_length, data.ptr, n, out.ptr, nb, stream), "afl32 compress")
+    else:
+        W = 8 * es
+        nb = (n * bit_length + W - 1) // W * es
+        out = alloc(max(nb, es), stream)
+        check(L.gtsc_afl_compress_gpu(dtype, bit_length, data.ptr, n, out.ptr, nb, stream), "afl compress")
+    out.nbytes = nb
+    return out
+
+
+def afl_unpack(dtype, bit_length, comp, n, omega=32, stream=None):
+    """All n elements of a packed stream (either layout) -> DeviceBuffer of n elements."""
+    L = lib()
+    out = alloc(max(n * dtype_size(dtype), 1), stream)
+    out.nbytes = n * dtype_size(dtype)
+    if omega == 32:
+        check(L.gtsc_afl32_decompress_gpu(dtype, bit_length, comp.ptr, comp.nbytes, out.ptr, n, stream),
+              "afl32 decompress")
+    else:
+        check(L.gtsc_afl_decompress_gpu(dtype, bit_length, comp.ptr, comp.nbytes, out.ptr, n, stream),
+              "afl decompress")
+    return out
+
+
+def afl_values(dtype, bit_length, comp, omega, index=None, n=None, stream=None):
+    """Random-access decode (run_afl_decompress_value_gpu): element index[t] (or t < n) of a packed
+    stream -> DeviceBuffer.  `index` is a device buffer of uint64 positions."""
+    m = index.nbytes // 8 if index is not None else int(n)
+    out = alloc(max(m * dtype_size(dtype), 1), stream)
+    out.nbytes = m * dtype_size(dtype)
+    check(lib().gtsc_afl_values_gpu(dtype, bit_length, omega, comp.ptr, comp.nbytes,
+                                    index.ptr if index is not None else None, m, out.ptr, stream),
+          "afl values")
+    return out
 
 
 def encode(encoding, dtype, data, stream=None):

@@ -207,6 +207,8 @@ void BatchEngine::build_node(const Tree &t, int &k, int col, int parent, int in_
         break;
     default: fail(GTSC_ERR_ARG, "batch: unsupported encoding in tree");
     }
+    if (me.enc == GTSC_AFL && is_fp(me.dt))
+        fail(GTSC_ERR_UNSUPPORTED, "batch: AFL of a floating-point node runs on the per-column path only");
     const int r = n_results(me.enc);
     if (me.virt) cap[1] = 0;  // read through the child's view, never written
     if (me.enc != GTSC_NONE)

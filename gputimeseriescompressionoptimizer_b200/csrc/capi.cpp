@@ -578,6 +578,60 @@ gtsc_status gtsc_plan_learned(gtsc_planner *p, const gtsc_column *cols, uint32_t
     });
 }
 
+static void afl_args(int32_t dtype, uint32_t b)
+{
+    const int es = dtype_size(dtype);
+    if (!es || is_fp(dtype)) fail(GTSC_ERR_TYPE, "afl kernels: integer data types only");
+    if (b < 1 || b > 8u * es) fail(GTSC_ERR_ARG, "afl kernels: bit length out of range");
+}
+
+uint64_t gtsc_afl32_bytes(int32_t dtype, uint32_t bit_length, uint64_t n)
+{
+    const int es = dtype_size(dtype);
+    return es ? afl32_words(n, (int)bit_length, es) * es : 0;
+}
+
+gtsc_status gtsc_afl32_compress_gpu(int32_t dtype, uint32_t bit_length, const void *d_data, uint64_t n, void *d_out,
+                                    uint64_t out_bytes, void *stream)
+{
+    return guard([&] {
+        afl_args(dtype, bit_length);
+        const int es = dtype_size(dtype);
+        if ((!d_data && n) || !d_out) fail(GTSC_ERR_ARG, "null argument");
+        if (((uintptr_t)d_data | (uintptr_t)d_out) % es) fail(GTSC_ERR_ARG, "afl32: pointers must be element aligned");
+        const uint64_t words = afl32_words(n, (int)bit_length, es);
+        if (out_bytes < words * es) fail(GTSC_ERR_CAPACITY, "afl32: output smaller than gtsc_afl32_bytes");
+        GTSC_CUDA(cudaMemsetAsync(d_out, 0, words * es, S(stream)));  // the layout has holes in a last block
+        launch_afl32_pack((const uint8_t *)d_data, n, es, (int)bit_length, (uint8_t *)d_out, words, S(stream));
+    });
+}
+
+gtsc_status gtsc_afl32_decompress_gpu(int32_t dtype, uint32_t bit_length, const void *d_comp, uint64_t comp_bytes,
+                                      void *d_out, uint64_t n, void *stream)
+{
+    return guard([&] {
+        afl_args(dtype, bit_length);
+        const int es = dtype_size(dtype);
+        if ((!d_comp || !d_out) && n) fail(GTSC_ERR_ARG, "null argument");
+        if (((uintptr_t)d_comp | (uintptr_t)d_out) % es) fail(GTSC_ERR_ARG, "afl32: pointers must be element aligned");
+        launch_afl32_unpack((const uint8_t *)d_comp, comp_bytes / es, n, es, (int)bit_length, (uint8_t *)d_out, S(stream));
+    });
+}
+
+gtsc_status gtsc_afl_values_gpu(int32_t dtype, uint32_t bit_length, int32_t omega, const void *d_comp,
+                                uint64_t comp_bytes, const uint64_t *d_index, uint64_t n, void *d_out, void *stream)
+{
+    return guard([&] {
+        afl_args(dtype, bit_length);
+        const int es = dtype_size(dtype);
+        if (omega != 1 && omega != 32) fail(GTSC_ERR_ARG, "afl values: omega is 1 or 32");
+        if ((!d_comp || !d_out) && n) fail(GTSC_ERR_ARG, "null argument");
+        if (((uintptr_t)d_comp | (uintptr_t)d_out) % es) fail(GTSC_ERR_ARG, "afl values: pointers must be element aligned");
+        launch_afl_values((const uint8_t *)d_comp, comp_bytes / es, es, (int)bit_length, omega, d_index, n,
+                          (uint8_t *)d_out, S(stream));
+    });
+}
+
 gtsc_status gtsc_afl_compress_gpu(int32_t dtype, uint32_t bit_length, const void *d_data, uint64_t n,
                                   void *d_out, uint64_t out_bytes, void *stream)
 {

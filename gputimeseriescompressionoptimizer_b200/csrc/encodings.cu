@@ -86,11 +86,15 @@ void column_minmax(View in, int es, Order o, uint64_t *mn, uint64_t *mx, cudaStr
 
 // ------------------------------------------------------------------------------------ AFL
 
+Parts afl_float_encode(View in, cudaStream_t s);
+DevBuf afl_float_decode(View meta, View data, cudaStream_t s);
+
 // AflEncoding::Encode<T> (compression/afl/afl_encoding.cu:15-56)
 Parts afl_encode(int dt, View in, cudaStream_t s)
 {
     const int es = dtype_size(dt);
-    if (is_fp(dt)) fail(GTSC_ERR_TYPE, "afl: floating-point columns are not supported");
+    if (dt == GTSC_FLOAT) return afl_float_encode(in, s);
+    if (is_fp(dt)) fail(GTSC_ERR_TYPE, "afl: double columns are not supported (EncodeDouble returns no buffers)");
     const uint64_t n = in.bytes / es;
     if (n == 0) return {empty_buf(), empty_buf()};
     DevBuf keep;
@@ -112,7 +116,8 @@ Parts afl_encode(int dt, View in, cudaStream_t s)
 DevBuf afl_decode(int dt, View meta, View data, cudaStream_t s)
 {
     const int es = dtype_size(dt);
-    if (is_fp(dt)) fail(GTSC_ERR_TYPE, "afl: floating-point columns are not supported");
+    if (dt == GTSC_FLOAT) return afl_float_decode(meta, data, s);
+    if (is_fp(dt)) fail(GTSC_ERR_TYPE, "afl: double columns are not supported (DecodeDouble returns no buffer)");
     if (data.bytes == 0) return empty_buf();
     if (meta.bytes < 2) fail(GTSC_ERR_FORMAT, "afl: metadata too short");
     int8_t m[2];
@@ -124,6 +129,74 @@ DevBuf afl_decode(int dt, View meta, View data, cudaStream_t s)
     const uint64_t n = (uint64_t)bits / b;
     DevBuf out = dev_alloc(n * es, s);
     launch_afl_unpack(data.ptr, data.bytes, n, es, b, out.get(), s);
+    return out;
+}
+
+// AflEncoding::Encode(SharedCudaPtr<float>) (afl_encoding.cu:116-170).  data = mantissa metadata
+// + mantissa words + exponent metadata + exponent words; metadata = size_t mantissa-word bytes, a
+// sign byte (1 all positive, 2 all negative, 0: the packed sign stencil follows).  The sign byte is
+// decided on the sign bits (the reference's min >= 0 / max < 0 would drop the sign of -0.0 and of
+// NaNs).
+Parts afl_float_encode(View in, cudaStream_t s)
+{
+    const uint64_t n = in.bytes / 4;
+    if (n == 0) return {empty_buf(), empty_buf()};
+    DevBuf mant = dev_alloc(4 * n, s), expo = dev_alloc(4 * n, s);
+    DevBuf st = dev_alloc(1 + (n + 7) / 8, s), flags = dev_alloc(4, s);
+    GTSC_CUDA(cudaMemsetAsync(flags.get(), 0, 4, s));
+    launch_float_split(in.ptr, n, (int32_t *)mant.get(), (int32_t *)expo.get(), st.get(), (uint32_t *)flags.get(), s);
+    uint32_t f = 0;
+    d2h(&f, flags.get(), 4, s);
+    const uint8_t sign = (f & 1) == 0 ? 1 : (f & 2) == 0 ? 2 : 0;
+    Parts pm = afl_encode(GTSC_INT, View(mant), s);
+    Parts pe = afl_encode(GTSC_INT, View(expo), s);
+    const uint64_t msize = pm[1].bytes, esize = pe[1].bytes;
+    DevBuf data = dev_alloc(8 + msize + esize, s);
+    uint8_t *d = data.get();
+    GTSC_CUDA(cudaMemcpyAsync(d, pm[0].get(), 4, cudaMemcpyDeviceToDevice, s));
+    if (msize) GTSC_CUDA(cudaMemcpyAsync(d + 4, pm[1].get(), msize, cudaMemcpyDeviceToDevice, s));
+    GTSC_CUDA(cudaMemcpyAsync(d + 4 + msize, pe[0].get(), 4, cudaMemcpyDeviceToDevice, s));
+    if (esize) GTSC_CUDA(cudaMemcpyAsync(d + 8 + msize, pe[1].get(), esize, cudaMemcpyDeviceToDevice, s));
+    const uint64_t sbytes = sign == 0 ? 1 + (n + 7) / 8 : 0;
+    DevBuf meta = dev_alloc(9 + sbytes, s);
+    uint8_t head[9];
+    std::memcpy(head, &msize, 8);
+    head[8] = sign;
+    GTSC_CUDA(cudaMemcpyAsync(meta.get(), head, 9, cudaMemcpyHostToDevice, s));
+    if (sbytes) GTSC_CUDA(cudaMemcpyAsync(meta.get() + 9, st.get(), sbytes, cudaMemcpyDeviceToDevice, s));
+    GTSC_CUDA(cudaStreamSynchronize(s));  // `head` is a host stack buffer
+    return {meta, data};
+}
+
+// AflEncoding::Decode<float> (afl_encoding.cu:189-254)
+DevBuf afl_float_decode(View meta, View data, cudaStream_t s)
+{
+    if (data.bytes == 0) return empty_buf();
+    if (meta.bytes < 9 || data.bytes < 8) fail(GTSC_ERR_FORMAT, "afl float: stream too short");
+    uint8_t head[9];
+    d2h(head, meta.ptr, 9, s);
+    uint64_t msize;
+    std::memcpy(&msize, head, 8);
+    const int sign = (int8_t)head[8];
+    if (msize > data.bytes - 8 || sign < 0 || sign > 2) fail(GTSC_ERR_FORMAT, "afl float: bad metadata");
+    const uint64_t esize = data.bytes - msize - 8;
+    DevBuf m = afl_decode(GTSC_INT, View(data.ptr, 4), View(data.ptr + 4, msize), s);
+    DevBuf e = afl_decode(GTSC_INT, View(data.ptr + 4 + msize, 4), View(data.ptr + 8 + msize, esize), s);
+    const uint64_t n = m.bytes / 4;
+    if (e.bytes / 4 < n) fail(GTSC_ERR_FORMAT, "afl float: fewer exponents than mantissas");
+    const uint8_t *stencil = nullptr;
+    if (sign == 0) {
+        // Stencil(metadata, sizeof(size_t) + 1): rest byte, then the sign bits
+        int8_t rest;
+        d2h(&rest, meta.ptr + 9, 1, s);
+        const int64_t bits = (int64_t)(meta.bytes - 10) * 8 - (rest ? 8 - rest : 0);
+        if (meta.bytes < 10 || rest < 0 || rest > 7 || bits < (int64_t)n)
+            fail(GTSC_ERR_FORMAT, "afl float: sign stencil too short");
+        stencil = meta.ptr + 10;
+    }
+    DevBuf out = dev_alloc(4 * n, s);
+    launch_float_compose((const int32_t *)m.get(), (const int32_t *)e.get(), stencil, sign == 0 ? 0 : sign - 1, n,
+                         (uint32_t *)out.get(), s);
     return out;
 }
 

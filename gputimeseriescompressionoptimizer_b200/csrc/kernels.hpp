@@ -121,4 +121,20 @@ void launch_split(int mode, const uint8_t *in, uint64_t n, int es, const SplitAr
 void launch_merge(int mode, const uint8_t *stencil, uint64_t n, int es, const MergeArgs &a, uint8_t *out,
                   uint8_t *scratch, cudaStream_t s);
 
+// AflEncoding's float path (afl_float.cu): split into mantissa / exponent int32 arrays and the sign
+// stencil (1 + ceil(n/8) bytes); flags |= 1 when a sign bit is set, |= 2 when one is clear
+void launch_float_split(const uint8_t *in, uint64_t n, int32_t *mant, int32_t *expo, uint8_t *stencil,
+                        uint32_t *flags, cudaStream_t s);
+// the inverse; stencil = the packed sign bits (without its rest byte), or null and `fill` for all
+void launch_float_compose(const int32_t *mant, const int32_t *expo, const uint8_t *stencil, int fill, uint64_t n,
+                          uint32_t *out, cudaStream_t s);
+
+// aligned AFL layout (afl32.cu): words of a stream of n elements at b bits (element units)
+uint64_t afl32_words(uint64_t n, int b, int es);
+void launch_afl32_pack(const uint8_t *in, uint64_t n, int es, int b, uint8_t *out, uint64_t words, cudaStream_t s);
+void launch_afl32_unpack(const uint8_t *comp, uint64_t words, uint64_t n, int es, int b, uint8_t *out, cudaStream_t s);
+// random access: out[t] = element (idx ? idx[t] : t) of an FL (omega 1) or aligned (omega 32) stream
+void launch_afl_values(const uint8_t *comp, uint64_t words, int es, int b, int omega, const uint64_t *idx,
+                       uint64_t n, uint8_t *out, cudaStream_t s);
+
 }  // namespace gtsc

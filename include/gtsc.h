@@ -291,6 +291,26 @@ gtsc_status gtsc_afl_decompress_gpu(int32_t dtype, uint32_t bit_length, const vo
                                     uint64_t comp_bytes, void *d_out, uint64_t n, void *stream);
 
 /*
+ * run_afl_compress_gpu<T,32> / run_afl_decompress_gpu<T,32> (compression/afl/afl_gpu.cu:67-81, the
+ * aligned layout instantiated at afl_gpu.cu:263-265): blocks of 32*W values (W = element bits),
+ * value j of lane l of a block at element 32j + l, lane l's packed words at 32k + l.  The packed
+ * stream takes gtsc_afl32_bytes(dtype, b, n) bytes (whole blocks; holes in the last one are 0).
+ * Integer types; element-aligned pointers.
+ */
+uint64_t gtsc_afl32_bytes(int32_t dtype, uint32_t bit_length, uint64_t n);
+gtsc_status gtsc_afl32_compress_gpu(int32_t dtype, uint32_t bit_length, const void *d_data, uint64_t n, void *d_out,
+                                    uint64_t out_bytes, void *stream);
+gtsc_status gtsc_afl32_decompress_gpu(int32_t dtype, uint32_t bit_length, const void *d_comp, uint64_t comp_bytes,
+                                      void *d_out, uint64_t n, void *stream);
+/*
+ * Random-access decode, run_afl_decompress_value_gpu<T,omega> (afl_gpu.cu:83-121, 197-222):
+ * out[t] = element (d_index ? d_index[t] : t) of an FL (omega 1, AflEncoding's layout) or aligned
+ * (omega 32) packed stream, for t < n; each element is decoded on its own.
+ */
+gtsc_status gtsc_afl_values_gpu(int32_t dtype, uint32_t bit_length, int32_t omega, const void *d_comp,
+                                uint64_t comp_bytes, const uint64_t *d_index, uint64_t n, void *d_out, void *stream);
+
+/*
  * Delta decode that allocates no device memory (no counterpart in the reference).  For callers that
  * cannot call cudaMalloc -- e.g. code whose device memory is all owned by a host framework's pool.
  * Decodes the delta stream (d_first = the metadata, the column's first value; d_deltas = n_deltas

@@ -226,6 +226,86 @@ def ref_afl_compress(dtype, data, bit_length):
     return out[:words].view(np.uint8).copy()
 
 
+def afl_layout_words(omega, dtype, b, n):
+    L = lib()
+    L.or_afl_words.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64]
+    L.or_afl_words.restype = ctypes.c_uint64
+    return L.or_afl_words(omega, dtype, b, n)
+
+
+def afl_layout_pack(omega, dtype, data, b):
+    """The packed stream of `data` in the FL (omega 1) or aligned (omega 32) layout, as bytes."""
+    L = lib()
+    x = np.ascontiguousarray(data)
+    words = afl_layout_words(omega, dtype, b, x.size)
+    out = np.zeros(max(words * x.itemsize, 1), np.uint8)
+    L.or_afl_pack.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                              ctypes.c_void_p, ctypes.c_uint64]
+    r = L.or_afl_pack(omega, dtype, b, _ptr(x), x.size, _ptr(out), words)
+    if r:
+        raise OracleError(r)
+    return out[:words * x.itemsize].copy()
+
+
+def afl_layout_values(omega, dtype, packed, b, n, idx=None):
+    """Elements idx (or 0..n-1) of a packed stream, in the dtype's integer type."""
+    L = lib()
+    npt = _REF_T[dtype][1]
+    es = np.dtype(npt).itemsize
+    comp = np.ascontiguousarray(packed, np.uint8)
+    ix = None if idx is None else np.ascontiguousarray(idx, np.uint64)
+    m = n if ix is None else ix.size
+    out = np.zeros(max(m, 1), npt)
+    L.or_afl_values.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    r = L.or_afl_values(omega, dtype, b, _ptr(comp), comp.size // es, None if ix is None else _ptr(ix), m,
+                        _ptr(out))
+    if r:
+        raise OracleError(r)
+    return out[:m].copy()
+
+
+def ref_afl32_compress(dtype, data, bit_length):
+    """run_afl_compress_cpu<T,32> of the reference (afl_gpu.cu:5-30) -> packed words as bytes."""
+    R = ref()
+    name, npt = _REF_T[dtype]
+    x = np.ascontiguousarray(data, npt)
+    words = afl_layout_words(32, dtype, bit_length, x.size)
+    out = np.zeros(max(words, 1) + 64, npt)
+    fn = getattr(R, f"ref_afl32_compress_{name}")
+    fn.argtypes = [ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulong, ctypes.c_ulong]
+    fn(bit_length, _ptr(x), _ptr(out), x.size, words)
+    assert not out[words:].any()
+    return out[:words].view(np.uint8).copy()
+
+
+def ref_afl32_decompress(dtype, packed, bit_length, n):
+    """run_afl_decompress_cpu<T,32> of the reference (afl_gpu.cu:43-65)."""
+    R = ref()
+    name, npt = _REF_T[dtype]
+    W = np.dtype(npt).itemsize
+    comp = np.zeros((packed.size + W - 1) // W + 64, npt)
+    comp.view(np.uint8)[:packed.size] = packed
+    out = np.zeros(max(n, 1), npt)
+    fn = getattr(R, f"ref_afl32_decompress_{name}")
+    fn.argtypes = [ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulong]
+    fn(bit_length, _ptr(comp), _ptr(out), n)
+    return out[:n].copy()
+
+
+def ref_afl_value(dtype, omega, packed, bit_length, i):
+    """afl_decompress_base_value_gpu<T,omega> of the reference (afl_gpu.cu:197-222), int or long."""
+    R = ref()
+    name, npt = _REF_T[dtype]
+    W = np.dtype(npt).itemsize
+    comp = np.zeros((packed.size + W - 1) // W + 64, npt)
+    comp.view(np.uint8)[:packed.size] = packed
+    fn = getattr(R, f"ref_afl_value_{name}")
+    fn.argtypes = [ctypes.c_uint, ctypes.c_int, ctypes.c_void_p, ctypes.c_ulong]
+    fn.restype = ctypes.c_long if name == "long" else ctypes.c_int
+    return fn(bit_length, omega, _ptr(comp), i)
+
+
 def ref_afl_decompress(dtype, packed, bit_length, n):
     R = ref()
     name, npt = _REF_T[dtype]

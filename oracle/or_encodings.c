@@ -239,6 +239,143 @@ static int afl_decode(int dt, const uint8_t *meta, uint64_t mb, const uint8_t *d
     return OR_OK;
 }
 
+/*
+ * Bit position of element i of a packed stream, omega = 1 (FL) or 32 (the aligned layout of
+ * run_afl_compress_cpu<T,32>, afl_gpu.cu:5-30 and 124-163, addressed as in
+ * afl_decompress_base_value_gpu, afl_gpu.cu:197-222): blocks of omega*W elements; element i is row
+ * r = (i % omega*W) / omega of lane l = i % omega, and lane l of block B holds its rows LSB first in
+ * the words B*omega*b + l + omega*k.  Returns the first bit (in word units: word, bit).
+ */
+static void afl_locate(int omega, int W, int b, uint64_t i, uint64_t *word, int *bit)
+{
+    uint64_t per = (uint64_t)omega * W, blk = i / per, in_blk = i % per;
+    uint64_t lane = in_blk % omega, row = in_blk / omega;
+    *word = blk * omega * (uint64_t)b + lane + (row * b / W) * omega;
+    *bit = (int)(row * b % W);
+}
+
+uint64_t or_afl_words(int omega, int dtype, int b, uint64_t n)
+{
+    uint64_t W = 8ull * es_of(dtype);
+    if (omega == 1) return (n * b + W - 1) / W;
+    return (n + 32 * W - 1) / (32 * W) * 32 * b;
+}
+
+/* packs n elements into `words` zeroed words; bits of a value that straddle a word continue at bit
+ * 0 of the lane's next word (word + omega) */
+int or_afl_pack(int omega, int dtype, int b, const uint8_t *in, uint64_t n, uint8_t *out, uint64_t words)
+{
+    int es = es_of(dtype), W = 8 * es;
+    if (!es || b < 1 || b > W || (omega != 1 && omega != 32)) return OR_ERR_ARG;
+    memset(out, 0, words * es);
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t w, v = ld_u(in, es, i);
+        int bit;
+        afl_locate(omega, W, b, i, &w, &bit);
+        for (int k = 0; k < b; k++, bit++) {
+            if (bit == W) { bit = 0; w += omega; }
+            if (w >= words) return OR_ERR_CAP;
+            if ((v >> k) & 1) out[w * es + bit / 8] |= (uint8_t)(1u << (bit % 8));
+        }
+    }
+    return OR_OK;
+}
+
+/* element idx[t] (or t when idx is NULL) of a packed stream, t < n; bits past `words` read 0 */
+int or_afl_values(int omega, int dtype, int b, const uint8_t *comp, uint64_t words, const uint64_t *idx,
+                  uint64_t n, uint8_t *out)
+{
+    int es = es_of(dtype), W = 8 * es;
+    if (!es || b < 1 || b > W || (omega != 1 && omega != 32)) return OR_ERR_ARG;
+    for (uint64_t t = 0; t < n; t++) {
+        uint64_t w, v = 0;
+        int bit;
+        afl_locate(omega, W, b, idx ? idx[t] : t, &w, &bit);
+        for (int k = 0; k < b; k++, bit++) {
+            if (bit == W) { bit = 0; w += omega; }
+            if (w < words && ((comp[w * es + bit / 8] >> (bit % 8)) & 1)) v |= 1ull << k;
+        }
+        st_u(out, es, t, v);
+    }
+    return OR_OK;
+}
+
+/* AflEncoding::Encode(SharedCudaPtr<float>) (afl_encoding.cu:116-170): every float is split into
+ * its 23-bit mantissa, 8-bit exponent and sign; the mantissa and exponent int32 arrays are AFL
+ * packed.  data = mantissa metadata (4) + mantissa words + exponent metadata (4) + exponent words;
+ * metadata = size_t mantissa-word bytes, one sign byte (1 all positive, 2 all negative, 0 = the
+ * packed stencil of the sign bits follows).  Deviation: "all positive / all negative" is decided
+ * on the sign bits; the reference's min >= 0 / max < 0 would drop the sign of -0.0 and of NaNs. */
+static int afl_float_encode(const uint8_t *in, uint64_t n, uint8_t *meta, uint8_t *out, uint64_t cap,
+                            uint64_t ob[3])
+{
+    if (n == 0) { ob[0] = ob[1] = 0; return OR_OK; }
+    int32_t *mant = (int32_t *)malloc(4 * n), *expo = (int32_t *)malloc(4 * n), *sg = (int32_t *)malloc(4 * n);
+    int any1 = 0, all1 = 1;
+    for (uint64_t i = 0; i < n; i++) {
+        uint32_t u = (uint32_t)ld_u(in, 4, i);
+        mant[i] = (int32_t)(u & 0x7fffffu);
+        expo[i] = (int32_t)((u >> 23) & 0xffu);
+        sg[i] = (int32_t)(u >> 31);
+        any1 |= sg[i];
+        all1 &= sg[i];
+    }
+    int sign = !any1 ? 1 : all1 ? 2 : 0;
+    uint64_t obm[3], obe[3];
+    int r = cap < 8 ? OR_ERR_CAP : afl_encode(OR_INT, (const uint8_t *)mant, n, out, out + 4, cap - 8, obm);
+    if (!r) r = afl_encode(OR_INT, (const uint8_t *)expo, n, out + 4 + obm[1], out + 8 + obm[1], cap - 8 - obm[1], obe);
+    if (!r) {
+        uint64_t msize = obm[1];
+        memcpy(meta, &msize, 8);
+        meta[8] = (uint8_t)sign;
+        ob[0] = 9 + (sign == 0 ? or_stencil_pack(sg, n, meta + 9) : 0);
+        ob[1] = 8 + obm[1] + obe[1];
+    }
+    free(mant);
+    free(expo);
+    free(sg);
+    return r;
+}
+
+/* AflEncoding::Decode<float> (afl_encoding.cu:189-254) */
+static int afl_float_decode(const uint8_t *meta, uint64_t mb, const uint8_t *data, uint64_t db, uint8_t *out,
+                            uint64_t cap, uint64_t *ob)
+{
+    if (db == 0) { *ob = 0; return OR_OK; }
+    if (mb < 9 || db < 8) return OR_ERR_FORMAT;
+    uint64_t msize;
+    memcpy(&msize, meta, 8);
+    int sign = (int8_t)meta[8];
+    if (msize > db - 8 || sign < 0 || sign > 2) return OR_ERR_FORMAT;
+    uint64_t esize = db - msize - 8;
+    uint64_t tcap = 4 * (8 * (msize > esize ? msize : esize) + 8);
+    uint8_t *m = (uint8_t *)malloc(tcap), *e = (uint8_t *)malloc(tcap);
+    uint64_t obm = 0, obe = 0;
+    int r = afl_decode(OR_INT, data, 4, data + 4, msize, m, tcap, &obm);
+    if (!r) r = afl_decode(OR_INT, data + 4 + msize, 4, data + 8 + msize, esize, e, tcap, &obe);
+    uint64_t n = obm / 4;
+    if (!r && obe / 4 < n) r = OR_ERR_FORMAT;
+    if (!r && 4 * n > cap) r = OR_ERR_CAP;
+    int32_t *sg = NULL;
+    if (!r && sign == 0) {
+        sg = (int32_t *)malloc(4 * (8 * mb + 8));
+        int64_t k = or_stencil_unpack(meta + 9, mb - 9, sg, 8 * mb + 8);
+        if (k < (int64_t)n) r = OR_ERR_FORMAT;
+    }
+    if (!r) {
+        for (uint64_t i = 0; i < n; i++) {
+            uint32_t s1 = sign == 0 ? (uint32_t)(sg[i] & 1) : (uint32_t)(sign - 1);
+            uint32_t u = (s1 << 31) | (((uint32_t)ld_u(e, 4, i) & 0xffu) << 23) | ((uint32_t)ld_u(m, 4, i) & 0x7fffffu);
+            st_u(out, 4, i, u);
+        }
+        *ob = 4 * n;
+    }
+    free(m);
+    free(e);
+    free(sg);
+    return r;
+}
+
 /* ---------------------------------------------------------------- delta / scale / none --- */
 
 /* DeltaEncoding::Encode/Decode (compression/delta/delta_encoding.cu:19-102); float/double go
@@ -792,8 +929,10 @@ int or_encode(int enc, int dt, const uint8_t *in, uint64_t in_bytes,
     ob[0] = ob[1] = ob[2] = 0;
     switch (enc) {
     case OR_AFL:
-        if (is_fp(dt)) return OR_ERR_UNSUPPORTED;
-        *n_out = 2; return afl_encode(dt, in, n, o0, o1, cap, ob);
+        *n_out = 2;
+        if (dt == OR_FLOAT) return afl_float_encode(in, n, o0, o1, cap, ob);
+        if (is_fp(dt)) return OR_ERR_UNSUPPORTED;  /* EncodeDouble returns no buffers at all */
+        return afl_encode(dt, in, n, o0, o1, cap, ob);
     case OR_DELTA: *n_out = 2; return delta_encode(dt, in, n, o0, o1, ob);
     case OR_SCALE: *n_out = 2; return scale_encode(dt, in, n, o0, o1, ob);
     case OR_NONE:
@@ -823,6 +962,7 @@ int or_decode(int enc, int dt, const uint8_t *i0, uint64_t b0, const uint8_t *i1
     *ob = 0;
     switch (enc) {
     case OR_AFL:
+        if (dt == OR_FLOAT) return afl_float_decode(i0, b0, i1, b1, out, cap, ob);
         if (is_fp(dt)) return OR_ERR_UNSUPPORTED;
         return afl_decode(dt, i0, b0, i1, b1, out, cap, ob);
     case OR_DELTA: return delta_decode(dt, i0, b0, i1, b1, out, cap, ob);

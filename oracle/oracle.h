@@ -55,6 +55,16 @@ int or_encode(int enc, int dtype, const uint8_t *in, uint64_t in_bytes,
               uint8_t *out0, uint8_t *out1, uint8_t *out2, uint64_t cap,
               uint64_t out_bytes[3], int *n_out);
 
+/*
+ * The packed AFL layouts by bit position (afl_gpu.cu:5-65, 197-222): omega 1 (FL) or 32
+ * (aligned).  or_afl_words = words of n elements at b bits; or_afl_pack writes them (zero
+ * filled); or_afl_values reads element idx[t] (t when idx is NULL) for t < n.
+ */
+uint64_t or_afl_words(int omega, int dtype, int b, uint64_t n);
+int or_afl_pack(int omega, int dtype, int b, const uint8_t *in, uint64_t n, uint8_t *out, uint64_t words);
+int or_afl_values(int omega, int dtype, int b, const uint8_t *comp, uint64_t words, const uint64_t *idx,
+                  uint64_t n, uint8_t *out);
+
 /* Encoding::Decode (compression/encoding.hpp:49-68). */
 int or_decode(int enc, int dtype,
               const uint8_t *in0, uint64_t b0, const uint8_t *in1, uint64_t b1,

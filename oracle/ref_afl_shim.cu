@@ -5,7 +5,9 @@
  * src/compression/afl/afl_gpu.cu from the reference tree (the include path is given by
  * oracle/Makefile) and wraps the explicitly instantiated host entry points
  * run_afl_compress_cpu<T,1> / run_afl_decompress_cpu<T,1> (afl_gpu.cu:6-65, 253-269) in
- * extern "C" functions.  The output goes to oracle/_ref/, which is never committed.
+ * extern "C" functions, as well as the aligned layout run_afl_compress_cpu<T,32> /
+ * run_afl_decompress_cpu<T,32> and the random-access afl_decompress_base_value_gpu<T,W> (host
+ * callable).  The output goes to oracle/_ref/, which is never committed.
  *
  * The reference host path masks with NBITSTOMASK(n) = (1<<n)-1 (core/cuda_macros.cuh:6), which is
  * undefined for n equal to the word width, so callers only use bit widths below the word width.
@@ -31,5 +33,25 @@ void ref_afl_decompress_int(unsigned b, int *comp, int *out, unsigned long n)
 { run_afl_decompress_cpu<int, 1>(b, comp, out, n); }
 void ref_afl_decompress_long(unsigned b, long *comp, long *out, unsigned long n)
 { run_afl_decompress_cpu<long, 1>(b, comp, out, n); }
+
+
+void ref_afl32_compress_int(unsigned b, int *data, int *out, unsigned long n, unsigned long words)
+{ run_afl_compress_cpu<int, 32>(b, data, out, n, words); }
+void ref_afl32_compress_long(unsigned b, long *data, long *out, unsigned long n, unsigned long words)
+{ run_afl_compress_cpu<long, 32>(b, data, out, n, words); }
+void ref_afl32_compress_short(unsigned b, short *data, short *out, unsigned long n, unsigned long words)
+{ run_afl_compress_cpu<short, 32>(b, data, out, n, words); }
+void ref_afl32_decompress_int(unsigned b, int *comp, int *out, unsigned long n)
+{ run_afl_decompress_cpu<int, 32>(b, comp, out, n); }
+void ref_afl32_decompress_long(unsigned b, long *comp, long *out, unsigned long n)
+{ run_afl_decompress_cpu<long, 32>(b, comp, out, n); }
+void ref_afl32_decompress_short(unsigned b, short *comp, short *out, unsigned long n)
+{ run_afl_decompress_cpu<short, 32>(b, comp, out, n); }
+
+// element i of a packed int stream, FL (omega 1) or aligned (omega 32)
+int ref_afl_value_int(unsigned b, int omega, int *comp, unsigned long i)
+{ return omega == 32 ? afl_decompress_base_value_gpu<int, 32>(b, comp, i) : afl_decompress_base_value_gpu<int, 1>(b, comp, i); }
+long ref_afl_value_long(unsigned b, int omega, long *comp, unsigned long i)
+{ return omega == 32 ? afl_decompress_base_value_gpu<long, 32>(b, comp, i) : afl_decompress_base_value_gpu<long, 1>(b, comp, i); }
 
 }

@@ -175,3 +175,54 @@ def test_device_nan_to_int_conversion(G, O, dt, npt, bits, expected):
     x = np.array([0, expected, expected], npt)
     x.view(np.uint64 if npt == np.float64 else np.uint32)[0] = bits
     assert G.stats(dt, G.to_device(x)).rl_metric == 2.0 == O.stats(dt, x).rl_metric
+
+
+def float_cases(rng):
+    for n in [0, 1, 7, 8, 9, 1000, 100001]:
+        x = np.round(rng.normal(0, 100, n), 2).astype(np.float32)
+        yield "mixed", x
+        yield "positive", np.abs(x)
+        yield "negative", -np.abs(x) - np.float32(1)
+        if n >= 16:
+            y = x.copy()
+            y[3] = np.float32(-0.0)
+            y[5] = np.float32(np.inf)
+            y[6] = -np.float32(np.inf)
+            bits = y.view(np.uint32)
+            bits[7] = np.uint32(0xffc00123)  # a negative NaN with a payload
+            yield "specials", y
+            z = np.abs(x)
+            z[2] = np.float32(-0.0)  # all positive but one -0.0: the sign must survive
+            yield "minus_zero", z
+
+
+def test_afl_float_split(G, O, rng):
+    """AflEncoding's float path (afl_encoding.cu:116-254): mantissa / exponent AFL streams and the
+    sign byte or stencil, byte-identical to the oracle, bit-exact round trip"""
+    for name, x in float_cases(rng):
+        ref = O.encode(OR.AFL, OR.FLOAT, x)
+        parts = G.encode(G.AFL, G.FLOAT, G.to_device(x))
+        assert len(parts) == len(ref) == 2
+        for a, b in zip(parts, ref):
+            assert np.array_equal(G.to_host(a), b), (name, x.size)
+        out = G.decode(G.AFL, G.FLOAT, parts)
+        assert G.to_host(out).tobytes() == x.tobytes(), (name, x.size)
+        if x.size:  # sign byte: 1 all sign bits clear, 2 all set, 0 a stencil follows
+            neg = int(np.signbit(x).sum())
+            expect = 1 if neg == 0 else 2 if neg == x.size else 0
+            assert int(G.to_host(parts[0])[8]) == expect, name
+            if name == "minus_zero":
+                assert expect == 0
+
+
+def test_afl_float_in_trees(G, O, rng):
+    x = np.round(rng.normal(0, 10, 20000), 1).astype(np.float32)
+    for path in ([OR.AFL, OR.NONE], [OR.DELTA, OR.AFL, OR.NONE], [OR.PATCH, OR.AFL, OR.NONE, OR.AFL, OR.NONE]):
+        nodes = G.tree_from_path(path, OR.FLOAT)
+        blob = G.tree_compress(nodes, G.to_device(x))
+        assert np.array_equal(G.to_host(blob), O.tree_compress(nodes, x))
+        out, _ = G.tree_decompress(blob)
+        assert G.to_host(out).tobytes() == x.tobytes()
+        assert G.tree_predict_size(nodes, G.to_device(x)) == O.tree_predict_size(nodes, x)
+    with pytest.raises(G.GtscError):  # double: EncodeDouble returns no buffers in the reference
+        G.encode(G.AFL, G.DOUBLE, G.to_device(x.astype(np.float64)))

@@ -105,6 +105,32 @@ def test_afl_oracle_matches_reference(O, rng, dt, npt):
             assert np.array_equal(O.ref_afl_decompress(dt, data, b, n), x)
 
 
+@pytest.mark.parametrize("dt,npt", [(OR.SHORT, np.int16), (OR.INT, np.int32), (OR.TIME, np.int64)])
+def test_afl_layouts_match_reference(O, rng, dt, npt):
+    """The oracle's bit-position restatement of both packed layouts against the reference's own
+    run_afl_compress_cpu / run_afl_decompress_cpu <T,1|32> and afl_decompress_base_value_gpu
+    (afl_gpu.cu:5-65, 197-222).  The reference's host bit extraction is defined for b < W only."""
+    if not OR.build_ref():
+        pytest.skip("reference AFL sources not available")
+    W = 8 * np.dtype(npt).itemsize
+    for n in [1, 31, 32, 33, 32 * W - 1, 32 * W, 32 * W + 1, 3 * 32 * W + 77, 20000]:
+        for b in sorted({1, 3, 7, W // 2 + 1, W - 1}):
+            x = rng.integers(0, 2 ** b, n).astype(npt)
+            x[-1] = 2 ** b - 1
+            p1 = OR.afl_layout_pack(1, dt, x, b)
+            p32 = OR.afl_layout_pack(32, dt, x, b)
+            assert p32.size == OR.afl_layout_words(32, dt, b, n) * x.itemsize
+            assert np.array_equal(O.ref_afl_compress(dt, x, b), p1)
+            assert np.array_equal(O.ref_afl32_compress(dt, x, b), p32)
+            assert np.array_equal(O.ref_afl32_decompress(dt, p32, b, n), x)
+            assert np.array_equal(OR.afl_layout_values(1, dt, p1, b, n), x)
+            assert np.array_equal(OR.afl_layout_values(32, dt, p32, b, n), x)
+            if dt != OR.SHORT:
+                for i in sorted({0, n // 3, n - 1}):
+                    assert O.ref_afl_value(dt, 1, p1, b, i) == x[i]
+                    assert O.ref_afl_value(dt, 32, p32, b, i) == x[i]
+
+
 def test_afl_config1_sizes(O, rng):
     """2^20 int32 uniform in [0, 2^11): b = 11, 1 441 792 data bytes + 4 metadata bytes."""
     x = rng.integers(0, 2 ** 11, 1 << 20).astype(np.int32)
