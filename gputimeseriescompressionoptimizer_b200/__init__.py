@@ -96,6 +96,7 @@ def lib():
         L.gtsc_sample_bytes.argtypes = [i32, u64]
         L.gtsc_sample_bytes.restype = u64
         L.gtsc_delta_decode_noalloc.argtypes = [i32, vp, vp, u64, vp, vp]
+        L.gtsc_predict_sizes.argtypes = [i32, i32, vp, u64, ctypes.POINTER(u64), ctypes.POINTER(u64), vp]
         L.gtsc_afl32_bytes.argtypes = [i32, u32, u64]
         L.gtsc_afl32_bytes.restype = u64
         L.gtsc_afl32_compress_gpu.argtypes = [i32, u32, vp, u64, vp, u64, vp]
@@ -194,6 +195,14 @@ def to_host(buf, dtype=np.uint8, stream=None):
 
 def dtype_size(dtype):
     return lib().gtsc_dtype_size(dtype)
+
+
+def predict_sizes(encoding, dtype, data, stream=None):
+    """GetMetadataSize / GetCompressedSize of one encoding for a device column -> (meta, data) bytes."""
+    m, d = ctypes.c_uint64(), ctypes.c_uint64()
+    check(lib().gtsc_predict_sizes(encoding, dtype, data.ptr, data.nbytes, ctypes.byref(m), ctypes.byref(d), stream),
+          "predict_sizes")
+    return m.value, d.value
 
 
 def afl_pack(dtype, bit_length, data, n, omega=32, stream=None):

@@ -4,6 +4,7 @@
 #include "encodings.hpp"
 #include "kernels.hpp"
 #include "batch.hpp"
+#include "predict.hpp"
 #include "learned.hpp"
 #include "planner.hpp"
 #include "tree.hpp"
@@ -575,6 +576,17 @@ gtsc_status gtsc_plan_learned(gtsc_planner *p, const gtsc_column *cols, uint32_t
             node_counts[c] = t.size();
             used += t.size();
         }
+    });
+}
+
+gtsc_status gtsc_predict_sizes(int32_t encoding, int32_t dtype, const void *d_in, uint64_t in_bytes,
+                               uint64_t *metadata_bytes, uint64_t *compressed_bytes, void *stream)
+{
+    return guard([&] {
+        if ((!d_in && in_bytes) || !metadata_bytes || !compressed_bytes) fail(GTSC_ERR_ARG, "null argument");
+        const SizePrediction p = predict_sizes(encoding, dtype, View(d_in, in_bytes), S(stream));
+        *metadata_bytes = p.meta;
+        *compressed_bytes = p.data;
     });
 }
 

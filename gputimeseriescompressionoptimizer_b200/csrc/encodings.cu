@@ -884,6 +884,7 @@ Parts encode(int enc, int dt, View in, cudaStream_t s)
     case GTSC_PATCH: return patch_encode(dt, in, s);
     case GTSC_FLOAT_TO_INT: return f2i_encode(dt, in, s);
     case GTSC_GFC: return gfc_encode(dt, in, s);
+    case GTSC_UNIQUE: return unique_encode(dt, in, s);
     default: fail(GTSC_ERR_UNSUPPORTED, "encoding not available");
     }
 }
@@ -904,6 +905,7 @@ DevBuf decode(int enc, int dt, const std::vector<View> &in, cudaStream_t s)
     case GTSC_PATCH: return patch_decode(dt, v[0], v[1], v[2], s);
     case GTSC_FLOAT_TO_INT: return f2i_decode(dt, v[0], v[1], s);
     case GTSC_GFC: return gfc_decode(dt, v[0], v[1], v[2], s);
+    case GTSC_UNIQUE: return unique_decode(dt, v[0], v[1], s);
     default: fail(GTSC_ERR_UNSUPPORTED, "encoding not available");
     }
 }

@@ -10,6 +10,12 @@ namespace gtsc {
 Parts encode(int enc, int dt, View in, cudaStream_t s);
 DevBuf decode(int enc, int dt, const std::vector<View> &in, cudaStream_t s);
 
+// the standalone UniqueEncoding (unique.cu)
+Parts unique_encode(int dt, View in, cudaStream_t s);
+DevBuf unique_decode(int dt, View meta, View data, cudaStream_t s);
+// number of distinct values (bit patterns) of a column
+uint64_t unique_count(int dt, View in, cudaStream_t s);
+
 // number of child streams (GetNumberOfResults) and their data types (GetReturnTypes)
 int n_results(int enc);
 int return_type(int enc, int dt, int j);

@@ -291,6 +291,18 @@ gtsc_status gtsc_afl_decompress_gpu(int32_t dtype, uint32_t bit_length, const vo
                                     uint64_t comp_bytes, void *d_out, uint64_t n, void *stream);
 
 /*
+ * Encoding::GetMetadataSize / GetCompressedSize (compression/encoding.hpp:74-76; the per-encoding
+ * predictors, e.g. rle_encode.cu:64-97, dict_encoding.cu:132-161, afl_encoding.cu:281-343,
+ * unique_encoding.cu:306-326): *metadata_bytes = the size of out[0], *compressed_bytes = the sizes
+ * of the data outputs together, computed by counting passes without encoding.  Exact for none,
+ * delta, scale, rle, dict, const, integer afl and unique; patch and floatToInt predict the input
+ * size, gfc 0 data bytes and float afl 9 metadata bytes, as the reference's predictors do.
+ * Synchronises the stream.
+ */
+gtsc_status gtsc_predict_sizes(int32_t encoding, int32_t dtype, const void *d_in, uint64_t in_bytes,
+                               uint64_t *metadata_bytes, uint64_t *compressed_bytes, void *stream);
+
+/*
  * run_afl_compress_gpu<T,32> / run_afl_decompress_gpu<T,32> (compression/afl/afl_gpu.cu:67-81, the
  * aligned layout instantiated at afl_gpu.cu:263-265): blocks of 32*W values (W = element bits),
  * value j of lane l of a block at element 32j + l, lane l's packed words at 32k + l.  The packed

@@ -226,3 +226,88 @@ def test_afl_float_in_trees(G, O, rng):
         assert G.tree_predict_size(nodes, G.to_device(x)) == O.tree_predict_size(nodes, x)
     with pytest.raises(G.GtscError):  # double: EncodeDouble returns no buffers in the reference
         G.encode(G.AFL, G.DOUBLE, G.to_device(x.astype(np.float64)))
+
+
+@pytest.mark.parametrize("dt,npt", ALL_TYPES)
+@pytest.mark.parametrize("n", SIZES + [4095, 4096, 4097, 300001])
+def test_unique(G, O, rng, dt, npt, n):
+    """The standalone UniqueEncoding (unique_encoding.cu:133-181, 261-304): sorted table of the
+    distinct bit patterns and packed codes, byte-identical to the oracle."""
+    for kind in KINDS:
+        check_encoding(G, O, OR.UNIQUE, dt, gen(kind, npt, n, rng))
+
+
+@pytest.mark.parametrize("dt,npt", ALL_TYPES)
+def test_unique_table_sizes(G, O, rng, dt, npt):
+    """1 distinct value (1-bit codes), 2^k and 2^k + 1 distinct values around the code widths, and
+    every value distinct (a table too large for shared memory, one code per word)."""
+    info = np.iinfo(npt) if not np.issubdtype(npt, np.floating) else None
+    for m in [1, 2, 3, 4, 5, 16, 17, 255, 256, 257, 40000]:
+        if info is not None and m > info.max - info.min + 1:
+            continue
+        vals = rng.permutation(np.arange(m)) - m // 2
+        vals = vals.astype(npt) if info is None else np.clip(vals, info.min, info.max).astype(npt)
+        x = vals[rng.integers(0, m, 50000)]
+        x[:m] = vals
+        check_encoding(G, O, OR.UNIQUE, dt, x)
+        meta = G.to_host(G.encode(OR.UNIQUE, dt, G.to_device(x))[0])
+        assert int(meta[:8].view(np.uint64)[0]) == np.unique(x.view(f"u{x.itemsize}")).size
+
+
+def test_unique_large(G, rng):
+    """2^24 int32 with ~10^6 distinct values: round trip and table size (size-independent checks)."""
+    n = 1 << 24
+    x = rng.integers(-(1 << 30), 1 << 30, 1 << 20).astype(np.int32)[rng.integers(0, 1 << 20, n)]
+    parts = G.encode(OR.UNIQUE, OR.INT, G.to_device(x))
+    meta = G.to_host(parts[0])
+    table = meta[16:].view(np.int32)
+    assert np.array_equal(table, np.unique(x))
+    assert G.to_host(G.decode(OR.UNIQUE, OR.INT, parts), np.int32).tobytes() == x.tobytes()
+
+
+def test_unique_in_trees_and_corrupt_codes(G, O, rng):
+    x = rng.integers(0, 50, 20000).astype(np.int32)
+    for path in ([OR.UNIQUE, OR.NONE], [OR.UNIQUE, OR.AFL, OR.NONE], [OR.DELTA, OR.UNIQUE, OR.AFL, OR.NONE]):
+        nodes = G.tree_from_path(path, OR.INT)
+        blob = G.tree_compress(nodes, G.to_device(x))
+        assert np.array_equal(G.to_host(blob), O.tree_compress(nodes, x))
+        out, _ = G.tree_decompress(blob)
+        assert G.to_host(out).tobytes() == x.tobytes()
+    # 3 distinct values -> 2-bit codes; code 3 points past the table
+    y = np.array([5, 6, 7, 5], np.int32)
+    meta, data = O.encode(OR.UNIQUE, OR.INT, y)
+    bad = data.copy()
+    bad[0] |= 0b11
+    with pytest.raises(G.GtscError) as e:
+        G.decode(OR.UNIQUE, OR.INT, [G.to_device(meta), G.to_device(bad)])
+    assert e.value.status == -4
+
+
+EXACT_PREDICTORS = [OR.NONE, OR.DELTA, OR.SCALE, OR.RLE, OR.DICT, OR.CONST, OR.UNIQUE]
+
+
+@pytest.mark.parametrize("dt,npt", ALL_TYPES)
+@pytest.mark.parametrize("n", [0, 1, 33, 4097, 65537])
+def test_size_predictors(G, O, rng, dt, npt, n):
+    """GetMetadataSize / GetCompressedSize == the emitted sizes (the reference's TestGetMetadataSize /
+    TestGetCompressedSize, test/compression_unittest_base.hpp:32-54) for the exact predictors; the
+    reference's fixed formulas for the others."""
+    es = np.dtype(npt).itemsize
+    for kind in KINDS:
+        x = gen(kind, npt, n, rng)
+        dev = G.to_device(x)
+        for enc in EXACT_PREDICTORS + ([OR.AFL] if dt != OR.DOUBLE else []):
+            parts = O.encode(enc, dt, x)
+            meta, data = G.predict_sizes(enc, dt, dev)
+            if n == 0:  # the reference's formulas: only none and dict have no empty guard
+                assert (meta, data) == ({OR.NONE: 8, OR.DICT: 1}.get(enc, 0), 0)
+                continue
+            if enc == OR.AFL and dt == OR.FLOAT:
+                assert meta == (9 if n else 0)
+            else:
+                assert meta == parts[0].size, (OR.ENC_NAMES[enc], kind)
+            assert data == sum(p.size for p in parts[1:]), (OR.ENC_NAMES[enc], kind)
+        stencil = (n + 7) // 8 + 1 if n else 0
+        assert G.predict_sizes(OR.PATCH, dt, dev) == (stencil, n * es)
+        assert G.predict_sizes(OR.FLOAT2INT, dt, dev) == ((4 if n else 0), n * es)
+        assert G.predict_sizes(OR.GFC, dt, dev) == (12, 0)
