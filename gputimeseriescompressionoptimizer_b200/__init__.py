@@ -96,6 +96,26 @@ def lib():
         L.gtsc_sample_bytes.argtypes = [i32, u64]
         L.gtsc_sample_bytes.restype = u64
         L.gtsc_delta_decode_noalloc.argtypes = [i32, vp, vp, u64, vp, vp]
+        i16, f64 = ctypes.c_int16, ctypes.c_double
+        L.gtsc_optimizer_create.argtypes = [i32, ctypes.POINTER(vp)]
+        L.gtsc_optimizer_compress.argtypes = [vp, vp, u64, vp, vp, vp, vp]
+        L.gtsc_optimizer_tree.argtypes = [vp, vp, vp, i32, vp]
+        L.gtsc_optimizer_statistics.argtypes = [vp, ctypes.POINTER(vp)]
+        L.gtsc_optimizer_destroy.argtypes = [vp]
+        L.gtsc_edge_stats_create.argtypes = [i32, ctypes.POINTER(vp)]
+        L.gtsc_edge_stats_destroy.argtypes = [vp]
+        L.gtsc_edge_stats_set.argtypes = [vp, i32, i16, i16, f64]
+        L.gtsc_edge_stats_update.argtypes = [vp, i32, i16, i16, f64]
+        L.gtsc_edge_stats_get.argtypes = [vp, i32, i16, i16, vp]
+        L.gtsc_edge_stats_best.argtypes = [vp, i32, i16, i16, i32, vp, vp, vp]
+        L.gtsc_edge_stats_entries.argtypes = [vp, i32, vp, vp, i32, vp]
+        L.gtsc_tree_edges.argtypes = [vp, i32, vp, vp, vp, i32, vp]
+        L.gtsc_tree_update_statistics.argtypes = [vp, vp, i32, vp]
+        L.gtsc_optimal_tree_create.argtypes = [vp, vp, i32, vp, ctypes.POINTER(vp)]
+        L.gtsc_optimal_tree_set_ratio.argtypes = [vp, i32, f64]
+        L.gtsc_optimal_tree_try_correct.argtypes = [vp, vp]
+        L.gtsc_optimal_tree_get.argtypes = [vp, vp, vp, i32, vp]
+        L.gtsc_optimal_tree_destroy.argtypes = [vp]
         L.gtsc_predict_sizes.argtypes = [i32, i32, vp, u64, ctypes.POINTER(u64), ctypes.POINTER(u64), vp]
         L.gtsc_afl32_bytes.argtypes = [i32, u32, u64]
         L.gtsc_afl32_bytes.restype = u64
@@ -533,6 +553,141 @@ def planner_features(cols, dtypes, stream=None):
     out = alloc(4 * N_FEATURES * max(len(cols), 1), stream)
     check(lib().gtsc_planner_features(_columns(cols, dtypes), len(cols), out.ptr, stream), "planner_features")
     return out
+
+
+# --------------------------------------------------------------------- online tree maintenance
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class EdgeStats:
+    """CompressionStatistics (tree/compression_statistics.cpp): edge scores of compression trees.
+    Host-only; no GPU needed."""
+
+    def __init__(self, tree_height=5, _handle=None, _owner=None):
+        self._owner = _owner
+        if _handle is not None:
+            self.h = _handle
+            self._owned = False
+        else:
+            h = ctypes.c_void_p()
+            check(lib().gtsc_edge_stats_create(tree_height, ctypes.byref(h)), "edge_stats_create")
+            self.h, self._owned = h.value, True
+
+    def __del__(self):
+        if getattr(self, "_owned", False) and _lib is not None:
+            _lib.gtsc_edge_stats_destroy(self.h)
+            self._owned = False
+
+    def set(self, edge, frm, to, value):
+        check(lib().gtsc_edge_stats_set(self.h, edge, frm, to, value), "edge_stats_set")
+
+    def update(self, edge, frm, to, ratio):
+        check(lib().gtsc_edge_stats_update(self.h, edge, frm, to, ratio), "edge_stats_update")
+
+    def get(self, edge, frm, to):
+        v = ctypes.c_double()
+        check(lib().gtsc_edge_stats_get(self.h, edge, frm, to, ctypes.byref(v)), "edge_stats_get")
+        return v.value
+
+    def best(self, edge, frm, to, same_beginning=False):
+        """GetBest -> ((parent, child), score)"""
+        a, b, v = ctypes.c_int16(), ctypes.c_int16(), ctypes.c_double()
+        check(lib().gtsc_edge_stats_best(self.h, edge, frm, to, int(same_beginning), ctypes.byref(a),
+                                         ctypes.byref(b), ctypes.byref(v)), "edge_stats_best")
+        return (a.value, b.value), v.value
+
+    def entries(self, edge):
+        """{(parent, child): score} of one edge"""
+        n = ctypes.c_int32()
+        pairs = np.zeros(2 * 256, np.int16)
+        vals = np.zeros(256, np.float64)
+        check(lib().gtsc_edge_stats_entries(self.h, edge, _ptr(pairs), _ptr(vals), 256, ctypes.byref(n)),
+              "edge_stats_entries")
+        return {(int(pairs[2 * k]), int(pairs[2 * k + 1])): float(vals[k]) for k in range(n.value)}
+
+
+def tree_edges(nodes):
+    """CompressionTree::GetEdges -> [(edge number, parent node index, child node index)] (pre-order
+    node indices)."""
+    nd, _ = _i16(nodes)
+    no, fr, to = (np.zeros(128, np.int32) for _ in range(3))
+    n = ctypes.c_int32()
+    check(lib().gtsc_tree_edges(_ptr(nd), nd.size // 2, _ptr(no), _ptr(fr), _ptr(to), 128, ctypes.byref(n)),
+          "tree_edges")
+    return [(int(no[k]), int(fr[k]), int(to[k])) for k in range(n.value)]
+
+
+def tree_update_statistics(nodes, ratios, stats):
+    nd, _ = _i16(nodes)
+    r = np.ascontiguousarray(ratios, np.float64)
+    check(lib().gtsc_tree_update_statistics(_ptr(nd), _ptr(r), nd.size // 2, stats.h), "tree_update_statistics")
+
+
+def _read_tree(fn, h, what):
+    nodes = np.zeros(2 * 1024, np.int16)
+    ratios = np.zeros(1024, np.float64)
+    n = ctypes.c_int32()
+    check(fn(h, _ptr(nodes), _ptr(ratios), 1024, ctypes.byref(n)), what)
+    return nodes[:2 * n.value].copy(), ratios[:n.value].copy()
+
+
+class OptimalTree:
+    """OptimalTree (optimizer/optimal_tree.cpp) over live statistics; host-only."""
+
+    def __init__(self, nodes, ratios, stats):
+        nd, _ = _i16(nodes)
+        r = np.ascontiguousarray(ratios, np.float64)
+        h = ctypes.c_void_p()
+        check(lib().gtsc_optimal_tree_create(_ptr(nd), _ptr(r), nd.size // 2, stats.h, ctypes.byref(h)),
+              "optimal_tree_create")
+        self.h, self.stats = h.value, stats
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.gtsc_optimal_tree_destroy(self.h)
+            self.h = None
+
+    def set_ratio(self, node, ratio):
+        check(lib().gtsc_optimal_tree_set_ratio(self.h, node, ratio), "optimal_tree_set_ratio")
+
+    def try_correct(self):
+        c = ctypes.c_int32()
+        check(lib().gtsc_optimal_tree_try_correct(self.h, ctypes.byref(c)), "optimal_tree_try_correct")
+        return bool(c.value)
+
+    def tree(self):
+        return _read_tree(lib().gtsc_optimal_tree_get, self.h, "optimal_tree_get")
+
+
+class Optimizer:
+    """CompressionOptimizer::CompressData for one column: compress() takes one part (a device
+    buffer) and returns (blob DeviceBuffer, full_update, corrected)."""
+
+    def __init__(self, dtype):
+        h = ctypes.c_void_p()
+        check(lib().gtsc_optimizer_create(dtype, ctypes.byref(h)), "optimizer_create")
+        self.h, self.dtype = h.value, dtype
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.gtsc_optimizer_destroy(self.h)
+            self.h = None
+
+    def compress(self, data, stream=None):
+        out = Buffer()
+        full, corr = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().gtsc_optimizer_compress(self.h, data.ptr, data.nbytes, ctypes.byref(out), ctypes.byref(full),
+                                            ctypes.byref(corr), stream), "optimizer_compress")
+        return DeviceBuffer(out.ptr, out.bytes), bool(full.value), bool(corr.value)
+
+    def tree(self):
+        return _read_tree(lib().gtsc_optimizer_tree, self.h, "optimizer_tree")
+
+    def statistics(self):
+        h = ctypes.c_void_p()
+        check(lib().gtsc_optimizer_statistics(self.h, ctypes.byref(h)), "optimizer_statistics")
+        return EdgeStats(_handle=h.value, _owner=self)
 
 
 class Planner:

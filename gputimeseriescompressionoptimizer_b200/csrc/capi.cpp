@@ -6,6 +6,7 @@
 #include "batch.hpp"
 #include "predict.hpp"
 #include "learned.hpp"
+#include "optimizer.hpp"
 #include "planner.hpp"
 #include "tree.hpp"
 
@@ -665,6 +666,235 @@ gtsc_status gtsc_afl_decompress_gpu(int32_t dtype, uint32_t bit_length, const vo
         if (comp_bytes * 8 < n * (uint64_t)bit_length) fail(GTSC_ERR_FORMAT, "afl: stream too short");
         launch_afl_unpack((const uint8_t *)d_comp, comp_bytes, n, es, (int)bit_length, (uint8_t *)d_out, S(stream));
     });
+}
+
+
+struct gtsc_edge_stats {
+    std::shared_ptr<EdgeStats> p;
+};
+struct gtsc_optimal_tree {
+    std::unique_ptr<OptimalTree> t;
+};
+struct gtsc_optimizer {
+    Optimizer o;
+    gtsc_edge_stats view;
+    explicit gtsc_optimizer(int dt) : o(dt) { view.p = o.stats; }
+};
+
+static void write_flat(const FlatTree &f, int16_t *nodes_out, double *ratios_out, int32_t cap, int32_t *n_nodes)
+{
+    if (!n_nodes) fail(GTSC_ERR_ARG, "null output");
+    std::vector<double> r;
+    const Tree t = f.preorder(&r);
+    *n_nodes = t.size();
+    if (t.size() > cap) fail(GTSC_ERR_CAPACITY, "node list longer than cap");
+    if (nodes_out) tree_to_nodes(t, nodes_out);
+    if (ratios_out) std::memcpy(ratios_out, r.data(), sizeof(double) * r.size());
+}
+
+static FlatTree flat_of(const int16_t *nodes, const double *ratios, int32_t n_nodes)
+{
+    const Tree t = tree_from_nodes(nodes, n_nodes);
+    std::vector<double> r;
+    if (ratios) r.assign(ratios, ratios + n_nodes);
+    return FlatTree::from(t, r);
+}
+
+gtsc_status gtsc_optimizer_create(int32_t dtype, gtsc_optimizer **out)
+{
+    return guard([&] {
+        if (!out) fail(GTSC_ERR_ARG, "null output");
+        if (!dtype_size(dtype)) fail(GTSC_ERR_ARG, "unknown data type");
+        *out = new gtsc_optimizer(dtype);
+    });
+}
+
+gtsc_status gtsc_optimizer_compress(gtsc_optimizer *o, const void *d_in, uint64_t in_bytes, gtsc_buffer *blob,
+                                    int32_t *full_update, int32_t *corrected, void *stream)
+{
+    return guard([&] {
+        if (!o || !blob || (!d_in && in_bytes)) fail(GTSC_ERR_ARG, "null argument");
+        bool full = false, corr = false;
+        DevBuf b = o->o.compress_data(View(d_in, in_bytes), &full, &corr, S(stream));
+        if (full_update) *full_update = full;
+        if (corrected) *corrected = corr;
+        *blob = release(b);
+    });
+}
+
+gtsc_status gtsc_optimizer_tree(const gtsc_optimizer *o, int16_t *nodes_out, double *ratios_out, int32_t cap,
+                                int32_t *n_nodes)
+{
+    return guard([&] {
+        if (!o) fail(GTSC_ERR_ARG, "null optimizer");
+        if (!o->o.opt) fail(GTSC_ERR_ARG, "optimizer: no part compressed yet");
+        write_flat(o->o.opt->tree, nodes_out, ratios_out, cap, n_nodes);
+    });
+}
+
+gtsc_status gtsc_optimizer_statistics(gtsc_optimizer *o, gtsc_edge_stats **stats)
+{
+    return guard([&] {
+        if (!o || !stats) fail(GTSC_ERR_ARG, "null argument");
+        *stats = &o->view;
+    });
+}
+
+gtsc_status gtsc_optimizer_destroy(gtsc_optimizer *o)
+{
+    return guard([&] { delete o; });
+}
+
+gtsc_status gtsc_edge_stats_create(int32_t tree_height, gtsc_edge_stats **out)
+{
+    return guard([&] {
+        if (!out) fail(GTSC_ERR_ARG, "null output");
+        auto *s = new gtsc_edge_stats();
+        try {
+            s->p = std::make_shared<EdgeStats>(tree_height);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+gtsc_status gtsc_edge_stats_destroy(gtsc_edge_stats *s)
+{
+    return guard([&] { delete s; });
+}
+
+gtsc_status gtsc_edge_stats_set(gtsc_edge_stats *s, int32_t edge, int16_t from, int16_t to, double value)
+{
+    return guard([&] {
+        if (!s) fail(GTSC_ERR_ARG, "null statistics");
+        s->p->set(edge, EdgeType{from, to}, value);
+    });
+}
+
+gtsc_status gtsc_edge_stats_update(gtsc_edge_stats *s, int32_t edge, int16_t from, int16_t to, double ratio)
+{
+    return guard([&] {
+        if (!s) fail(GTSC_ERR_ARG, "null statistics");
+        if (edge < 0 || edge >= s->p->edges()) fail(GTSC_ERR_ARG, "edge number out of range");
+        s->p->update(edge, EdgeType{from, to}, ratio);
+    });
+}
+
+gtsc_status gtsc_edge_stats_get(const gtsc_edge_stats *s, int32_t edge, int16_t from, int16_t to, double *value)
+{
+    return guard([&] {
+        if (!s || !value) fail(GTSC_ERR_ARG, "null argument");
+        *value = s->p->get(edge, EdgeType{from, to});
+    });
+}
+
+gtsc_status gtsc_edge_stats_best(const gtsc_edge_stats *s, int32_t edge, int16_t from, int16_t to,
+                                 int32_t same_beginning, int16_t *best_from, int16_t *best_to, double *value)
+{
+    return guard([&] {
+        if (!s || !best_from || !best_to || !value) fail(GTSC_ERR_ARG, "null argument");
+        const EdgeStats::Best b = s->p->best(edge, EdgeType{from, to}, same_beginning != 0);
+        *best_from = (int16_t)b.type.first;
+        *best_to = (int16_t)b.type.second;
+        *value = b.value;
+    });
+}
+
+gtsc_status gtsc_edge_stats_entries(const gtsc_edge_stats *s, int32_t edge, int16_t *pairs_out, double *values_out,
+                                    int32_t cap, int32_t *n)
+{
+    return guard([&] {
+        if (!s || !n) fail(GTSC_ERR_ARG, "null argument");
+        if (edge < 0 || edge >= s->p->edges()) fail(GTSC_ERR_ARG, "edge number out of range");
+        const auto &m = s->p->e[edge];
+        *n = (int32_t)m.size();
+        if ((int32_t)m.size() > cap) fail(GTSC_ERR_CAPACITY, "more entries than cap");
+        int k = 0;
+        for (auto &kv : m) {
+            if (pairs_out) {
+                pairs_out[2 * k] = (int16_t)kv.first.first;
+                pairs_out[2 * k + 1] = (int16_t)kv.first.second;
+            }
+            if (values_out) values_out[k] = kv.second;
+            k++;
+        }
+    });
+}
+
+gtsc_status gtsc_tree_edges(const int16_t *nodes, int32_t n_nodes, int32_t *edge_no, int32_t *from_node,
+                            int32_t *to_node, int32_t cap, int32_t *n_edges)
+{
+    return guard([&] {
+        if (!n_edges) fail(GTSC_ERR_ARG, "null output");
+        const FlatTree f = flat_of(nodes, nullptr, n_nodes);  // node k of f = pre-order node k
+        const std::vector<TreeEdge> ed = tree_edges(f);
+        *n_edges = (int32_t)ed.size();
+        if ((int32_t)ed.size() > cap) fail(GTSC_ERR_CAPACITY, "more edges than cap");
+        for (size_t k = 0; k < ed.size(); k++) {
+            if (edge_no) edge_no[k] = ed[k].no;
+            if (from_node) from_node[k] = ed[k].from;
+            if (to_node) to_node[k] = ed[k].to;
+        }
+    });
+}
+
+gtsc_status gtsc_tree_update_statistics(const int16_t *nodes, const double *ratios, int32_t n_nodes,
+                                        gtsc_edge_stats *s)
+{
+    return guard([&] {
+        if (!s || !ratios) fail(GTSC_ERR_ARG, "null argument");
+        update_statistics(flat_of(nodes, ratios, n_nodes), *s->p);
+    });
+}
+
+gtsc_status gtsc_optimal_tree_create(const int16_t *nodes, const double *ratios, int32_t n_nodes,
+                                     gtsc_edge_stats *stats, gtsc_optimal_tree **out)
+{
+    return guard([&] {
+        if (!stats || !out || !ratios) fail(GTSC_ERR_ARG, "null argument");
+        auto *t = new gtsc_optimal_tree();
+        try {
+            t->t.reset(new OptimalTree(flat_of(nodes, ratios, n_nodes), stats->p));
+        } catch (...) {
+            delete t;
+            throw;
+        }
+        *out = t;
+    });
+}
+
+gtsc_status gtsc_optimal_tree_set_ratio(gtsc_optimal_tree *t, int32_t node, double ratio)
+{
+    return guard([&] {
+        if (!t) fail(GTSC_ERR_ARG, "null tree");
+        if (node < 0 || node >= (int32_t)t->t->tree.ratio.size()) fail(GTSC_ERR_ARG, "node out of range");
+        t->t->tree.ratio[node] = ratio;  // the tree is kept in pre-order
+    });
+}
+
+gtsc_status gtsc_optimal_tree_try_correct(gtsc_optimal_tree *t, int32_t *corrected)
+{
+    return guard([&] {
+        if (!t) fail(GTSC_ERR_ARG, "null tree");
+        const bool c = t->t->try_correct();
+        if (corrected) *corrected = c;
+    });
+}
+
+gtsc_status gtsc_optimal_tree_get(const gtsc_optimal_tree *t, int16_t *nodes_out, double *ratios_out, int32_t cap,
+                                  int32_t *n_nodes)
+{
+    return guard([&] {
+        if (!t) fail(GTSC_ERR_ARG, "null tree");
+        write_flat(t->t->tree, nodes_out, ratios_out, cap, n_nodes);
+    });
+}
+
+gtsc_status gtsc_optimal_tree_destroy(gtsc_optimal_tree *t)
+{
+    return guard([&] { delete t; });
 }
 
 }  // extern "C"

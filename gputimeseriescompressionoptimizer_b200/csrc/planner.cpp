@@ -44,6 +44,7 @@ struct Cand {
     Tree tree;
 };
 
+
 void append(Tree &dst, const Tree &src)
 {
     dst.enc.insert(dst.enc.end(), src.enc.begin(), src.enc.end());
@@ -84,6 +85,51 @@ bool fsu(View data, int et, int dt, int level, Cand &best, PlanCounters &ctr, cu
         if (cand.size < best.size) best = cand;
     }
     return true;
+}
+
+// FullStatisticsUpdate with every candidate kept (compression_optimizer.cpp:88-140, CrossTrees
+// :38-78): per continuation, the crossed children candidates (left-major), or the bare node
+void fsu_all(View data, int et, int dt, int level, std::vector<Candidate> &out, cudaStream_t s)
+{
+    const Stats st = column_stats(dt, data, s);
+    for (int c : continuations(et, dt, st, level)) {
+        Parts p = encode(c, dt, data, s);
+        uint64_t psize = 8;
+        for (auto &b : p) psize += b.bytes;
+        const int r = n_results(c);
+        std::vector<Candidate> kid[2];
+        bool crossed = r > 0;
+        for (int j = 0; j < r; j++) {
+            fsu_all(View(p[j + 1]), c, return_type(c, dt, j), level + 1, kid[j], s);
+            crossed = crossed && !kid[j].empty();
+        }
+        auto make = [&](uint64_t size, const Candidate *a, const Candidate *b) {
+            Candidate x;
+            x.size = size;
+            x.tree.enc.push_back((int16_t)c);
+            x.tree.dt.push_back((int16_t)dt);
+            x.ratio.push_back(compression_ratio(data.bytes, size));
+            for (const Candidate *k : {a, b}) {
+                if (!k) continue;
+                append(x.tree, k->tree);
+                x.ratio.insert(x.ratio.end(), k->ratio.begin(), k->ratio.end());
+            }
+            out.push_back(std::move(x));
+        };
+        if (!crossed) {  // CompressNode::Fix gives the bare node `none` children of its own type
+            Candidate x;
+            x.size = psize;
+            x.tree = leaf_tree(c, dt);
+            x.ratio.assign(x.tree.size(), 1.0);
+            x.ratio[0] = compression_ratio(data.bytes, psize);
+            out.push_back(std::move(x));
+        } else if (r == 1) {
+            for (auto &a : kid[0]) make(a.size + p[0].bytes + 8, &a, nullptr);
+        } else {
+            for (auto &a : kid[0])
+                for (auto &b : kid[1]) make(a.size + b.size + p[0].bytes + 8, &a, &b);
+        }
+    }
 }
 
 // PathGenerator::GeneratePaths (optimizer/path_generator.cpp:20-68): 6 x 5 paths
@@ -133,6 +179,14 @@ Tree plan_exhaustive(int dt, View sample, uint64_t *best_size, PlanCounters *cou
     if (best_size) *best_size = best.size;
     if (counters) *counters = ctr;
     return best.tree;
+}
+
+std::vector<Candidate> plan_candidates(int dt, View sample, cudaStream_t s)
+{
+    if (!dtype_size(dt)) fail(GTSC_ERR_ARG, "unknown data type");
+    std::vector<Candidate> out;
+    fsu_all(sample, GTSC_NONE, dt, 0, out, s);
+    return out;
 }
 
 Tree optimize_tree(int dt, View data, uint64_t *best_size, cudaStream_t s)

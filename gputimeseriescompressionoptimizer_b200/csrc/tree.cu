@@ -16,6 +16,9 @@
 
 namespace gtsc {
 
+// Encoding::GetCompressionRatio (compression/encoding.hpp:78-84)
+double compression_ratio(uint64_t in, uint64_t out) { return (out == 0 || out > in) ? 1.0 : (double)in / (double)out; }
+
 namespace {
 
 constexpr int kMaxNodes = 1024;
@@ -96,11 +99,20 @@ struct Seg {
     uint64_t bytes;
 };
 
+uint64_t seg_bytes(const std::vector<Seg> &segs, size_t from)
+{
+    uint64_t b = 0;
+    for (size_t k = from; k < segs.size(); k++) b += segs[k].bytes;
+    return b;
+}
+
 void compress_rec(const Tree &t, int &i, View in, std::vector<Seg> &segs, std::vector<uint8_t> &hdrs,
-                  std::vector<DevBuf> &keep, cudaStream_t s)
+                  std::vector<DevBuf> &keep, cudaStream_t s, std::vector<double> *ratios)
 {
     if (i >= t.size()) fail(GTSC_ERR_ARG, "tree: incomplete node list");
     const int enc = t.enc[i], dt = t.dt[i];
+    const int me = i;
+    const size_t seg0 = segs.size();
     ++i;
     auto push_hdr = [&](int32_t meta_len) {
         int16_t h[2] = {(int16_t)enc, (int16_t)dt};
@@ -118,6 +130,7 @@ void compress_rec(const Tree &t, int &i, View in, std::vector<Seg> &segs, std::v
         memcpy(hdrs.data() + off, &b, 8);
         segs.push_back(Seg{nullptr, off, 8});
         if (in.bytes) segs.push_back(Seg{in.ptr, 0, in.bytes});
+        if (ratios) (*ratios)[me] = compression_ratio(in.bytes, seg_bytes(segs, seg0));
         return;
     }
     Parts p = encode(enc, dt, in, s);
@@ -125,7 +138,10 @@ void compress_rec(const Tree &t, int &i, View in, std::vector<Seg> &segs, std::v
     const int r = n_results(enc);
     push_hdr((int32_t)p[0].bytes);
     if (p[0].bytes) segs.push_back(Seg{p[0].get(), 0, p[0].bytes});
-    for (int j = 0; j < r; j++) compress_rec(t, i, View(p[j + 1]), segs, hdrs, keep, s);
+    for (int j = 0; j < r; j++) compress_rec(t, i, View(p[j + 1]), segs, hdrs, keep, s, ratios);
+    // CompressionNode::Compress (tree/compression_node.cpp:103-135): input over everything the
+    // subtree wrote, headers included
+    if (ratios) (*ratios)[me] = compression_ratio(in.bytes, seg_bytes(segs, seg0));
 }
 
 // ----------------------------------------------------------------------- decompress
@@ -221,13 +237,14 @@ Tree leaf_tree(int enc, int dtype)
     return t;
 }
 
-DevBuf tree_compress(const Tree &t, View in, cudaStream_t s)
+DevBuf tree_compress(const Tree &t, View in, cudaStream_t s, std::vector<double> *ratios)
 {
     std::vector<Seg> segs;
     std::vector<uint8_t> hdrs;
     std::vector<DevBuf> keep;
     int i = 0;
-    compress_rec(t, i, in, segs, hdrs, keep, s);
+    if (ratios) ratios->assign(t.size(), 1.0);
+    compress_rec(t, i, in, segs, hdrs, keep, s, ratios);
     if (i != t.size()) fail(GTSC_ERR_ARG, "tree: extra nodes");
     uint64_t total = 0;
     for (auto &g : segs) total += g.bytes;

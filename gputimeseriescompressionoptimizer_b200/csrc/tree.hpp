@@ -21,8 +21,11 @@ Tree tree_from_path(const int16_t *encs, int n, int dtype);
 // CompressionNode::Fix (tree/compression_node.cpp:209-223) of a single-node tree
 Tree leaf_tree(int enc, int dtype);
 
-// CompressionTree::Compress (tree/compression_tree.cpp:98-103): the serialized blob
-DevBuf tree_compress(const Tree &t, View in, cudaStream_t s);
+// CompressionTree::Compress (tree/compression_tree.cpp:98-103): the serialized blob; `ratios`, when
+// given, receives each node's compression ratio in pre-order (CompressionNode::Compress)
+DevBuf tree_compress(const Tree &t, View in, cudaStream_t s, std::vector<double> *ratios = nullptr);
+// Encoding::GetCompressionRatio (compression/encoding.hpp:78-84)
+double compression_ratio(uint64_t in, uint64_t out);
 // CompressionTree::Decompress (tree/compression_tree.cpp:105-155); *dtype = root data type
 DevBuf tree_decompress(View blob, int *dtype, cudaStream_t s);
 // CompressionNode::PredictCompressionSize (tree/compression_node.cpp:163-177)

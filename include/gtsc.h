@@ -323,6 +323,66 @@ gtsc_status gtsc_afl_values_gpu(int32_t dtype, uint32_t bit_length, int32_t omeg
                                 uint64_t comp_bytes, const uint64_t *d_index, uint64_t n, void *d_out, void *stream);
 
 /*
+ * Online tree maintenance: CompressionOptimizer::CompressData (optimizer/compression_optimizer.cpp
+ * 142-193) for one column.  Each call compresses one part (a chunk of the column) and returns its
+ * serialized tree blob.  The first part and every 10th after run a full statistics update:
+ * every FullStatisticsUpdate candidate on the part's first 10 000 elements is folded into the edge
+ * statistics (CompressionTree::UpdateStatistics, tree/compression_tree.cpp:232-240) and the best
+ * becomes the optimal tree.  Every part is compressed with the optimal tree, its node ratios folded
+ * in, and the tree corrected (OptimalTree::TryCorrectTree, optimizer/optimal_tree.cpp:38-93).
+ * *full_update / *corrected (optional) report what this call did.  The blob decodes with
+ * gtsc_tree_decompress.
+ */
+typedef struct gtsc_optimizer gtsc_optimizer;
+gtsc_status gtsc_optimizer_create(int32_t dtype, gtsc_optimizer **out);
+gtsc_status gtsc_optimizer_compress(gtsc_optimizer *o, const void *d_in, uint64_t in_bytes, gtsc_buffer *blob,
+                                    int32_t *full_update, int32_t *corrected, void *stream);
+/* GetOptimalTree()->GetTree(): pre-order (encoding, data type) pairs and each node's last ratio */
+gtsc_status gtsc_optimizer_tree(const gtsc_optimizer *o, int16_t *nodes_out, double *ratios_out, int32_t cap,
+                                int32_t *n_nodes);
+/* GetStatistics(): the statistics object the optimizer updates (owned by it; valid until destroy) */
+typedef struct gtsc_edge_stats gtsc_edge_stats;
+gtsc_status gtsc_optimizer_statistics(gtsc_optimizer *o, gtsc_edge_stats **stats);
+gtsc_status gtsc_optimizer_destroy(gtsc_optimizer *o);
+
+/*
+ * CompressionStatistics (tree/compression_statistics.cpp): per edge number (breadth-first over a
+ * full binary tree of height h: 2^(h+1) - 2 edges) a score per (parent encoding, child encoding).
+ * update: score = (max(score, 1) + max(ratio, 1)) / 2.  best: GetBest -- the highest score above 1
+ * whose child differs from `to` (and whose parent is `from` when same_beginning); ties go to the
+ * smallest (parent, child).  Host-only: these calls do no device work.
+ */
+gtsc_status gtsc_edge_stats_create(int32_t tree_height, gtsc_edge_stats **out);
+gtsc_status gtsc_edge_stats_destroy(gtsc_edge_stats *s);
+gtsc_status gtsc_edge_stats_set(gtsc_edge_stats *s, int32_t edge, int16_t from, int16_t to, double value);
+gtsc_status gtsc_edge_stats_update(gtsc_edge_stats *s, int32_t edge, int16_t from, int16_t to, double ratio);
+gtsc_status gtsc_edge_stats_get(const gtsc_edge_stats *s, int32_t edge, int16_t from, int16_t to, double *value);
+gtsc_status gtsc_edge_stats_best(const gtsc_edge_stats *s, int32_t edge, int16_t from, int16_t to,
+                                 int32_t same_beginning, int16_t *best_from, int16_t *best_to, double *value);
+/* every (parent, child) entry of one edge in (parent, child) order: pairs_out 2 per entry */
+gtsc_status gtsc_edge_stats_entries(const gtsc_edge_stats *s, int32_t edge, int16_t *pairs_out, double *values_out,
+                                    int32_t cap, int32_t *n);
+/* CompressionTree::GetEdges (:199-230): edge numbers and pre-order node indices of each edge */
+gtsc_status gtsc_tree_edges(const int16_t *nodes, int32_t n_nodes, int32_t *edge_no, int32_t *from_node,
+                            int32_t *to_node, int32_t cap, int32_t *n_edges);
+/* CompressionTree::UpdateStatistics (:232-240) for a tree with the given node ratios (pre-order) */
+gtsc_status gtsc_tree_update_statistics(const int16_t *nodes, const double *ratios, int32_t n_nodes,
+                                        gtsc_edge_stats *s);
+/*
+ * OptimalTree (optimizer/optimal_tree.hpp:24-63): a tree (pre-order nodes + ratios; ratio of the
+ * root = the tree's ratio) bound to live statistics `stats`, of which it keeps a snapshot.
+ * set_ratio changes one node's ratio (as a compression would); try_correct is TryCorrectTree.
+ */
+typedef struct gtsc_optimal_tree gtsc_optimal_tree;
+gtsc_status gtsc_optimal_tree_create(const int16_t *nodes, const double *ratios, int32_t n_nodes,
+                                     gtsc_edge_stats *stats, gtsc_optimal_tree **out);
+gtsc_status gtsc_optimal_tree_set_ratio(gtsc_optimal_tree *t, int32_t node, double ratio);
+gtsc_status gtsc_optimal_tree_try_correct(gtsc_optimal_tree *t, int32_t *corrected);
+gtsc_status gtsc_optimal_tree_get(const gtsc_optimal_tree *t, int16_t *nodes_out, double *ratios_out, int32_t cap,
+                                  int32_t *n_nodes);
+gtsc_status gtsc_optimal_tree_destroy(gtsc_optimal_tree *t);
+
+/*
  * Delta decode that allocates no device memory (no counterpart in the reference).  For callers that
  * cannot call cudaMalloc -- e.g. code whose device memory is all owned by a host framework's pool.
  * Decodes the delta stream (d_first = the metadata, the column's first value; d_deltas = n_deltas
