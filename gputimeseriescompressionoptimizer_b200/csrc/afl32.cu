@@ -17,75 +17,96 @@ namespace gtsc {
 
 namespace {
 
-template <int ES>
-__device__ __forceinline__ uint64_t afl_mask(int bits)
+// the packed word type of an element width: 32-bit arithmetic for elements of up to 4 bytes
+template <int ES> struct WordOf { using T = uint32_t; };
+template <> struct WordOf<8> { using T = unsigned long long; };
+
+template <typename T>
+__device__ __forceinline__ T low_mask(int bits)
 {
-    return bits >= 64 ? ~0ull : ((1ull << bits) - 1);
+    return bits >= (int)(8 * sizeof(T)) ? ~T(0) : ((T(1) << bits) - 1);
 }
 
+// one thread = one lane of one block of 32*W elements
 template <int ES>
-__device__ __forceinline__ void st_word(uint8_t *p, uint64_t i, uint64_t v)
+__global__ void __launch_bounds__(256) k_afl32_pack(const uint8_t *__restrict__ in, uint64_t n, int b,
+                                                    uint8_t *__restrict__ out, uint64_t words)
 {
-    st_elem<ES>(p, i, v);
-}
-
-// one thread = one lane of one block
-template <int ES>
-__global__ void k_afl32_pack(const uint8_t *__restrict__ in, uint64_t n, int b, uint8_t *__restrict__ out,
-                             uint64_t words)
-{
+    using T = typename WordOf<ES>::T;
     constexpr int W = 8 * ES;
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t blk = t / 32, lane = t % 32;
+    const uint64_t blk = t >> 5, lane = t & 31;
     const uint64_t first = blk * 32ull * W + lane;
     if (blk * 32ull * W >= n) return;
-    const uint64_t vmask = afl_mask<ES>(b), wmask = afl_mask<ES>(W);
-    uint64_t acc = 0, idx = first, wpos = blk * 32ull * b + lane;
+    const T vmask = low_mask<T>(b), wmask = low_mask<T>(W);
+    T acc = 0;
+    uint64_t wpos = blk * 32ull * b + lane;
     int fill = 0;
+    if ((blk + 1) * 32ull * W <= n) {  // a whole block: every load first, then the packing
+        T v[W];
+#pragma unroll
+        for (int j = 0; j < W; j++) v[j] = (T)ld_elem<ES>(in, first + 32ull * j) & vmask;
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            acc |= (v[j] << fill) & wmask;
+            if (fill >= W - b) {  // the word is full
+                st_elem<ES>(out, wpos, acc);
+                wpos += 32;
+                const int used = W - fill;
+                fill = b - used;
+                acc = used >= W ? T(0) : (v[j] >> used) & low_mask<T>(fill);
+            } else {
+                fill += b;
+            }
+        }
+        return;  // the last word of a whole block ends exactly at bit W*b
+    }
+    uint64_t idx = first;
     for (int j = 0; j < W && idx < n; j++, idx += 32) {
-        const uint64_t x = ld_elem<ES>(in, idx) & vmask;
+        const T x = (T)ld_elem<ES>(in, idx) & vmask;
         acc |= (x << fill) & wmask;
-        if (fill >= W - b) {  // the word is full
-            if (wpos < words) st_word<ES>(out, wpos, acc);
+        if (fill >= W - b) {
+            if (wpos < words) st_elem<ES>(out, wpos, acc);
             wpos += 32;
-            const int used = W - fill;  // bits of x in the word just written
+            const int used = W - fill;
             fill = b - used;
-            acc = used >= 64 ? 0 : (x >> used) & afl_mask<ES>(fill);
+            acc = used >= W ? T(0) : (x >> used) & low_mask<T>(fill);
         } else {
             fill += b;
         }
     }
-    if (idx >= n && idx < n + 32 && wpos < words) st_word<ES>(out, wpos, acc);
+    if (idx >= n && idx < n + 32 && wpos < words) st_elem<ES>(out, wpos, acc);
 }
 
 template <int ES>
-__global__ void k_afl32_unpack(const uint8_t *__restrict__ comp, uint64_t words, int b, uint64_t n,
-                               uint8_t *__restrict__ out)
+__global__ void __launch_bounds__(256) k_afl32_unpack(const uint8_t *__restrict__ comp, uint64_t words, int b,
+                                                      uint64_t n, uint8_t *__restrict__ out)
 {
+    using T = typename WordOf<ES>::T;
     constexpr int W = 8 * ES;
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t blk = t / 32, lane = t % 32;
+    const uint64_t blk = t >> 5, lane = t & 31;
     uint64_t idx = blk * 32ull * W + lane;
     if (blk * 32ull * W >= n) return;
-    const uint64_t vmask = afl_mask<ES>(b);
+    const T vmask = low_mask<T>(b);
     uint64_t wpos = blk * 32ull * b + lane;
-    uint64_t cur = wpos < words ? ld_elem<ES>(comp, wpos) : 0;
+    T cur = wpos < words ? (T)ld_elem<ES>(comp, wpos) : T(0);
     int pos = 0;
     for (int j = 0; j < W && idx < n; j++, idx += 32) {
-        uint64_t v;
+        T v;
         if (pos > W - b) {  // the value continues in the lane's next word
             const int have = W - pos;
-            v = (cur >> pos) & afl_mask<ES>(have);
+            v = (cur >> pos) & low_mask<T>(have);
             wpos += 32;
-            cur = wpos < words ? ld_elem<ES>(comp, wpos) : 0;
+            cur = wpos < words ? (T)ld_elem<ES>(comp, wpos) : T(0);
             pos = b - have;
-            v |= (cur & afl_mask<ES>(pos)) << have;
+            v |= (cur & low_mask<T>(pos)) << have;
         } else {
             v = (cur >> pos) & vmask;
             pos += b;
             if (pos == W && j + 1 < W) {  // the next value starts a new word
                 wpos += 32;
-                cur = wpos < words ? ld_elem<ES>(comp, wpos) : 0;
+                cur = wpos < words ? (T)ld_elem<ES>(comp, wpos) : T(0);
                 pos = 0;
             }
         }
@@ -93,34 +114,50 @@ __global__ void k_afl32_unpack(const uint8_t *__restrict__ comp, uint64_t words,
     }
 }
 
-// element i of a packed stream; omega = 1 (FL) or 32 (aligned)
-template <int ES>
-__device__ __forceinline__ uint64_t afl_value(const uint8_t *comp, uint64_t words, int b, int omega, uint64_t i)
+// element i of a packed stream, OMEGA = 1 (FL) or 32 (aligned); words past the stream read 0
+template <int ES, int OMEGA, typename I>
+__device__ __forceinline__ uint64_t afl_value(const uint8_t *comp, I words, int b, I i)
 {
+    using T = typename WordOf<ES>::T;
     constexpr int W = 8 * ES;
-    const uint64_t per = (uint64_t)omega * W;
-    const uint64_t blk = i / per, in_blk = i % per;
-    const uint64_t lane = in_blk % omega, row = in_blk / omega;
-    const uint64_t word = blk * (uint64_t)omega * b + lane + (row * b / W) * omega;
-    const int bit = (int)(row * b % W);
+    constexpr I per = (I)OMEGA * W;
+    const I blk = i / per, in_blk = i % per;
+    const uint32_t lane = (uint32_t)(in_blk % OMEGA), row = (uint32_t)(in_blk / OMEGA);
+    const uint32_t rb = row * (uint32_t)b;
+    const I word = blk * (I)(OMEGA * b) + lane + (I)(rb / W) * OMEGA;
+    const int bit = (int)(rb % W);
     const int first = bit <= W - b ? b : W - bit;
-    uint64_t v = word < words ? (ld_elem<ES>(comp, word) >> bit) & afl_mask<ES>(first) : 0;
+    T v = word < words ? ((T)ld_elem<ES>(comp, word) >> bit) & low_mask<T>(first) : T(0);
     if (first < b) {
-        const uint64_t w2 = word + omega;
-        const uint64_t hi = w2 < words ? ld_elem<ES>(comp, w2) & afl_mask<ES>(b - first) : 0;
+        const I w2 = word + OMEGA;
+        const T hi = w2 < words ? (T)ld_elem<ES>(comp, w2) & low_mask<T>(b - first) : T(0);
         v |= hi << first;
     }
     return v;
 }
 
-template <int ES>
-__global__ void k_afl_values(const uint8_t *__restrict__ comp, uint64_t words, int b, int omega,
-                             const uint64_t *__restrict__ idx, uint64_t n, uint8_t *__restrict__ out)
+template <int ES, int OMEGA>
+__global__ void __launch_bounds__(256) k_afl_values(const uint8_t *__restrict__ comp, uint64_t words, int b,
+                                                    const uint64_t *__restrict__ idx, uint64_t n,
+                                                    uint8_t *__restrict__ out)
 {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const uint64_t i = idx ? idx[t] : t;
-    st_elem<ES>(out, t, afl_value<ES>(comp, words, b, omega, i));
+    const uint64_t i = idx ? __ldg(idx + t) : t;
+    // 32-bit index arithmetic while it cannot wrap (the words read lie below i + 2 * OMEGA)
+    const uint64_t v = i < 0xffffff00ull && words < 0xffffff00ull
+                           ? afl_value<ES, OMEGA, uint32_t>(comp, (uint32_t)words, b, (uint32_t)i)
+                           : afl_value<ES, OMEGA, uint64_t>(comp, words, b, i);
+    st_elem<ES>(out, t, v);
+}
+
+template <int ES>
+void values_es(const uint8_t *comp, uint64_t words, int b, int omega, const uint64_t *idx, uint64_t n, uint8_t *out,
+               cudaStream_t s)
+{
+    const unsigned g = (unsigned)((n + 255) / 256);
+    if (omega == 32) k_afl_values<ES, 32><<<g, 256, 0, s>>>(comp, words, b, idx, n, out);
+    else k_afl_values<ES, 1><<<g, 256, 0, s>>>(comp, words, b, idx, n, out);
 }
 
 }  // namespace
@@ -163,12 +200,11 @@ void launch_afl_values(const uint8_t *comp, uint64_t words, int es, int b, int o
                        uint64_t n, uint8_t *out, cudaStream_t s)
 {
     if (!n) return;
-    const unsigned g = (unsigned)((n + 255) / 256);
     switch (es) {
-    case 1: k_afl_values<1><<<g, 256, 0, s>>>(comp, words, b, omega, idx, n, out); break;
-    case 2: k_afl_values<2><<<g, 256, 0, s>>>(comp, words, b, omega, idx, n, out); break;
-    case 4: k_afl_values<4><<<g, 256, 0, s>>>(comp, words, b, omega, idx, n, out); break;
-    default: k_afl_values<8><<<g, 256, 0, s>>>(comp, words, b, omega, idx, n, out); break;
+    case 1: values_es<1>(comp, words, b, omega, idx, n, out, s); break;
+    case 2: values_es<2>(comp, words, b, omega, idx, n, out, s); break;
+    case 4: values_es<4>(comp, words, b, omega, idx, n, out, s); break;
+    default: values_es<8>(comp, words, b, omega, idx, n, out, s); break;
     }
     GTSC_CUDA(cudaGetLastError());
 }
