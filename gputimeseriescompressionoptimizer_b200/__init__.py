@@ -388,7 +388,8 @@ class Stream:
 PASS_NAMES = dict(enumerate(
     ["minmax", "delta_enc", "scale_sub", "afl_pack", "hist", "topk", "split", "rle_heads", "rle_lengths",
      "f2i_stats", "f2i_enc", "f2i_raw", "gfc_compress", "gfc_scan", "gfc_compact", "none_copy", "afl_unpack",
-     "delta_dec", "scale_add", "merge", "rle_scan", "rle_expand", "f2i_dec", "gfc_sizes", "gfc_dec", "vmeta"]))
+     "delta_dec", "scale_add", "merge", "rle_scan", "rle_expand", "f2i_dec", "gfc_sizes", "gfc_dec", "vmeta",
+     "merge_count"]))
 PASS_NAMES.update({-1: "set_streams", -2: "zero", -3: "frame_sizes", -4: "frame_layout", -5: "frame_copy",
                    -6: "parse_frames"})
 

@@ -95,8 +95,7 @@ struct Launch {
 // passes whose tiles chain through a decoupled look-back (claimed in order from a counter)
 bool dyn_pass(int op)
 {
-    return op == B_SPLIT || op == B_RLE_HEADS || op == B_GFC_SCAN || op == B_DELTA_DEC || op == B_MERGE ||
-           op == B_RLE_SCAN;
+    return op == B_SPLIT || op == B_RLE_HEADS || op == B_GFC_SCAN || op == B_DELTA_DEC || op == B_RLE_SCAN;
 }
 
 uint64_t gfc_warps_for(bool dbl, uint64_t n)
@@ -516,6 +515,11 @@ void BatchEngine::plan_passes()
             BItem it = ditem(B_MERGE, t2k);
             it.mode = (int16_t)(nd.enc == GTSC_PATCH ? SPLIT_LOWER : nd.enc == GTSC_DICT ? SPLIT_DICT : SPLIT_NOT_CONST);
             it.p[0] = nd.dlb_off;
+            // the stencil counts need only the node's metadata, parsed before the first level: one
+            // launch ahead of every level (a merge may itself run at level 0)
+            BItem cnt = it;
+            cnt.op = B_MERGE_COUNT;
+            pass_d.push_back(Pass{-1, B_MERGE_COUNT, id, cnt});
             ps.push_back(it);
             break;
         }
@@ -694,7 +698,8 @@ void BatchEngine::layout(cudaStream_t s)
         for (int which = 0; which < 2; which++) {
             const int sid = which ? nd.data : nd.meta;
             if (sid < 0) continue;
-            const uint64_t cap = streams[sid].cap;
+            // a lone none root copies the caller's column: an external stream with no arena capacity
+            const uint64_t cap = std::max(streams[sid].cap, streams[sid].len);
             BItem it{};
             it.tiles = (uint32_t)std::max<uint64_t>(1, cdiv(cap, batch_copy_piece()));
             it.tile_base = copy_tiles;
@@ -971,6 +976,7 @@ static uint64_t item_bytes(const BItem &it, const std::vector<StreamDesc> &S)
     case B_DELTA_DEC: case B_SCALE_ADD: case B_F2I_DEC: return D(1) + L(it.out[0]);
     case B_MERGE: return in + (it.mode == SPLIT_DICT ? L(it.in[1]) : D(1)) + D(2) + L(it.out[0]);
     case B_RLE_SCAN: return D(1);
+    case B_MERGE_COUNT: return L(it.in[0]);
     case B_RLE_EXPAND: return D(2) + L(it.out[0]);
     case B_GFC_SIZES: return L(it.in[1]);
     case B_GFC_DEC: return L(it.in[2]) + L(it.out[0]);

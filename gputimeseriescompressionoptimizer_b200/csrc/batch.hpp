@@ -42,6 +42,7 @@ enum BOp : int {
     B_GFC_SIZES,
     B_GFC_DEC,
     B_VMETA,           // compress: metadata of a node whose output is read through a view
+    B_MERGE_COUNT,     // decode: stencil matches per merge tile and per group of 64 tiles
     B_NUM_OPS
 };
 

@@ -27,15 +27,17 @@ __device__ void block_copy(uint8_t *dst, const uint8_t *src, uint64_t n)
     const uint32_t *sw = (const uint32_t *)((uintptr_t)sp & ~(uintptr_t)3);
     uint32_t *dw = (uint32_t *)d;
     if (sh == 0) {
-        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = sw[k];
+#pragma unroll 4
+        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = __ldg(sw + k);
     } else {
-        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = __funnelshift_r(sw[k], sw[k + 1], sh);
+#pragma unroll 4
+        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = __funnelshift_r(__ldg(sw + k), __ldg(sw + k + 1), sh);
     }
     const uint64_t tail = (n - h) - 4 * words;
     if (threadIdx.x < tail) d[4 * words + threadIdx.x] = sp[4 * words + threadIdx.x];
 }
 
-constexpr uint64_t kCopyPiece = 1ull << 22;  // bytes of one copy tile
+constexpr uint64_t kCopyPiece = 1ull << 16;  // bytes of one copy tile (one block each)
 
 // ------------------------------------------------------------------------------- none / copy
 // in[0] = source stream, out[0] = destination stream; p[0] = destination byte offset inside it
@@ -180,11 +182,76 @@ __device__ void p_scale_add(const BItem &it, uint32_t tile, StreamDesc *S, uint3
 }
 
 // ------------------------------------------------------------------------------- merge
+// Merge tiles find their offsets in the match / non-match streams without a look-back chain: a
+// counting pass (B_MERGE_COUNT, any order) stores each tile's number of stencil matches and adds it
+// to its group of kMergeGroup tiles; a merge tile's exclusive prefix is then the sum of the groups
+// before its own plus the tiles before it inside its group.  Scratch at it.p[0]: 16 bytes, the
+// group sums (u64), then the tile counts (u32) -- within the look-back area's 16 + 16 * tiles.
+constexpr uint32_t kMergeGroup = 64;
+
+__device__ __forceinline__ unsigned long long *merge_groups(const BItem &it)
+{
+    return (unsigned long long *)(it.scratch + it.p[0] + 16);
+}
+__device__ __forceinline__ uint32_t *merge_counts(const BItem &it)
+{
+    return (uint32_t *)(it.scratch + it.p[0] + 16 + 8ull * ((it.tiles + kMergeGroup - 1) / kMergeGroup));
+}
+
+// the stencil of a merge node and the element count its rest byte gives (0 when malformed)
+template <int ES>
+__device__ __forceinline__ const uint8_t *merge_stencil(const BItem &it, const StreamDesc &meta, uint64_t &n)
+{
+    const uint8_t *stencil = it.mode == SPLIT_NOT_CONST ? meta.ptr + ES : meta.ptr;
+    const uint64_t sbytes = it.mode == SPLIT_NOT_CONST ? (meta.len > (uint64_t)ES ? meta.len - ES : 0) : meta.len;
+    n = 0;
+    if (sbytes >= 1) {
+        const int rest = (int8_t)stencil[0];
+        int64_t nn = (int64_t)(sbytes - 1) * 8;
+        if (rest) nn -= 8 - rest;
+        if (nn >= 0 && rest >= 0 && rest <= 7) n = (uint64_t)nn;
+    }
+    return stencil;
+}
+
+template <int ES>
+__device__ void p_merge_count(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    __shared__ unsigned long long ws[32];
+    uint64_t n;
+    const uint8_t *stencil = merge_stencil<ES>(it, S[it.in[0]], n);
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    uint32_t bits = 0;
+#pragma unroll
+    for (int q = 0; q < (int)kBVPT / 8; q++)
+        if (base + 8 * q < n) bits |= (uint32_t)stencil[1 + base / 8 + q] << (8 * q);
+    const uint32_t valid_mask = base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
+    unsigned long long total;
+    block_exclusive_scan<kBThreads>((unsigned long long)__popc(bits & valid_mask), ws, total);
+    if (threadIdx.x == 0) {
+        merge_counts(it)[tile] = (uint32_t)total;
+        if (total) atomicAdd(merge_groups(it) + tile / kMergeGroup, total);
+    }
+}
+
+// matches before `tile` (its exclusive prefix) from the counting pass; the same in every thread
+__device__ __forceinline__ unsigned long long merge_prefix(const BItem &it, uint32_t tile, unsigned long long *ws)
+{
+    const uint32_t g = tile / kMergeGroup;
+    const unsigned long long *groups = merge_groups(it);
+    const uint32_t *counts = merge_counts(it);
+    unsigned long long part = 0;
+    for (uint32_t k = threadIdx.x; k < g; k += kBThreads) part += groups[k];
+    for (uint32_t k = g * kMergeGroup + threadIdx.x; k < tile; k += kBThreads) part += counts[k];
+    unsigned long long total;
+    block_exclusive_scan<kBThreads>(part, ws, total);
+    return total;
+}
+
 template <int ES>
 __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, uint8_t *sm)
 {
     __shared__ unsigned long long ws[32];
-    __shared__ unsigned long long s_prefix;
     const int mode = it.mode;
     const StreamDesc meta = S[it.in[0]];
     // dictionary: in1 is the packed code stream (read plainly); otherwise both inputs may be views
@@ -240,8 +307,7 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     } else {
         yes_cap = v1.n;
     }
-    if (tile > 0 && (uint64_t)tile * kBTile >= n) return;  // past the output: no successor waits on it
-    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
+    if ((uint64_t)tile * kBTile >= n) return;  // past the output
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     const uint32_t valid_mask = base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
     uint32_t bits = 0;
@@ -251,18 +317,26 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     bits &= valid_mask;
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(bits), ws, total);
-    if (threadIdx.x < 32) {
-        const unsigned long long e = lookback_exclusive(lb, tile, total);
-        if (threadIdx.x == 0) s_prefix = e;
-    }
-    __syncthreads();
+    const unsigned long long prefix = merge_prefix(it, tile, ws);
     // the tile's runs of both streams are staged in shared memory with coalesced loads (matches
     // first, then the rest), then every thread assembles its values from there
     const uint64_t tile_base = (uint64_t)tile * kBTile;
     const uint64_t tile_n = tile_base < n ? (n - tile_base < kBTile ? n - tile_base : kBTile) : 0;
     const uint64_t ny = total, nn = tile_n - ny;
-    const uint64_t yes0 = s_prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
+    const uint64_t yes0 = prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
     bool bad = false;
+    // dictionary: the code words of the tile's matches, staged once (coalesced, whole words)
+    __shared__ uint32_t s_codes[kBTile / 16 + 2];
+    const uint64_t w0 = yes0 >> 4;
+    if (mode == SPLIT_DICT && ny) {
+        const uint64_t nw = ((yes0 + ny + 15) >> 4) - w0;
+        const uint64_t avail = in1.len >= 16 + 4ull * ES ? (in1.len - 16 - 4ull * ES) / 4 : 0;
+        const bool al = ((uintptr_t)codes & 3) == 0;
+        for (uint64_t k = threadIdx.x; k < nw; k += kBThreads) {
+            const uint64_t w = w0 + k;
+            s_codes[k] = w >= avail ? 0u : al ? __ldg((const uint32_t *)codes + w) : (uint32_t)ld_unaligned<4>(codes + 4 * w);
+        }
+    }
     if (mode != SPLIT_DICT) {
         for (uint64_t i = threadIdx.x; i < ny; i += kBThreads) {
             if (yes0 + i < yes_cap) st_elem<ES>(sm, i, dview_elem<ES>(v1, yes0 + i));
@@ -289,7 +363,7 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
                     if (y >= yes_cap) {
                         bad = true;
                     } else {
-                        const uint32_t w = (uint32_t)ld_unaligned<4>(codes + 4 * (y >> 4));
+                        const uint32_t w = s_codes[(y >> 4) - w0];
                         const uint32_t c = (w >> (2 * (y & 15))) & 3u;  // select, not an indexed array
                         v[j] = c == 0 ? top[0] : c == 1 ? top[1] : c == 2 ? top[2] : top[3];
                     }
@@ -615,6 +689,15 @@ __device__ __forceinline__ uint32_t dec_extent(const BItem &it, const StreamDesc
         const uint64_t runs = *(const unsigned long long *)(it.scratch + it.p[2]);
         const uint64_t n = runs ? ((const unsigned long long *)(it.scratch + it.p[1]))[runs - 1] : 0;
         e = cdiv(n, kBTile);
+    } else if constexpr (OP == B_MERGE_COUNT) {
+        uint64_t n;
+        switch (it.es) {
+        case 1: merge_stencil<1>(it, S[it.in[0]], n); break;
+        case 2: merge_stencil<2>(it, S[it.in[0]], n); break;
+        case 4: merge_stencil<4>(it, S[it.in[0]], n); break;
+        default: merge_stencil<8>(it, S[it.in[0]], n); break;
+        }
+        e = cdiv(n, kBTile);
     } else if constexpr (OP == B_F2I_DEC) {
         const StreamDesc meta = S[it.in[0]];
         const int p = meta.len >= 4 ? (int32_t)ld_unaligned<4>(meta.ptr) : 0;
@@ -631,7 +714,7 @@ __device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDe
 
 constexpr bool dec_persistent(int op)
 {
-    return op == B_AFL_UNPACK || op == B_SCALE_ADD || op == B_F2I_DEC || op == B_RLE_EXPAND;
+    return op == B_AFL_UNPACK || op == B_SCALE_ADD || op == B_F2I_DEC || op == B_RLE_EXPAND || op == B_MERGE_COUNT;
 }
 
 // One launch of a decode pass over every item: look-back passes one tile per block in claim order,
@@ -641,7 +724,7 @@ __global__ void __launch_bounds__(kBThreads, 3)
 k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status,
        uint32_t total_tiles)
 {
-    constexpr bool DYN = OP == B_DELTA_DEC || OP == B_MERGE || OP == B_RLE_SCAN;
+    constexpr bool DYN = OP == B_DELTA_DEC || OP == B_RLE_SCAN;
     __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : 16];
     if (*(volatile uint32_t *)(status + 1)) return;
     if constexpr (!dec_persistent(OP)) {
@@ -684,6 +767,7 @@ __device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDe
     else if constexpr (OP == B_DELTA_DEC) { GTSC_ES_SWITCH(p_delta_dec<E>(it, tile, S, status)) }
     else if constexpr (OP == B_SCALE_ADD) { GTSC_ES_SWITCH(p_scale_add<E>(it, tile, S, status)) }
     else if constexpr (OP == B_MERGE) { GTSC_ES_SWITCH(p_merge<E>(it, tile, S, status, smem)) }
+    else if constexpr (OP == B_MERGE_COUNT) { GTSC_ES_SWITCH(p_merge_count<E>(it, tile, S)) }
     else if constexpr (OP == B_RLE_SCAN) p_rle_scan(it, tile, S, status);
     else if constexpr (OP == B_RLE_EXPAND) { GTSC_ES_SWITCH(p_rle_expand<E>(it, tile, S, status)) }
     else if constexpr (OP == B_F2I_DEC) { GTSC_ES_SWITCH(p_f2i_dec<E>(it, tile, S, status)) }
@@ -891,6 +975,7 @@ void launch_batch_decode_stage(int op, const BItem *d_items, const uint32_t *d_i
         GTSC_STAGE(B_DELTA_DEC)
         GTSC_STAGE(B_SCALE_ADD)
         GTSC_STAGE(B_MERGE)
+        GTSC_STAGE(B_MERGE_COUNT)
         GTSC_STAGE(B_RLE_SCAN)
         GTSC_STAGE(B_RLE_EXPAND)
         GTSC_STAGE(B_F2I_DEC)

@@ -311,6 +311,25 @@ struct DViewCtx {
     bool aligned;          // plain: element aligned
 };
 
+// a plain stream that is not element aligned (a none leaf inside a blob) is read like a packed
+// stream of full-width values: whole 4-byte words and funnel shifts instead of ES byte loads
+template <int ES>
+__device__ __forceinline__ void dview_plain(DViewCtx &v, const uint8_t *ptr, uint64_t len)
+{
+    v.n = len / ES;
+    v.aligned = ((uintptr_t)ptr & (ES - 1)) == 0;
+    if (v.aligned) {
+        v.p = ptr;
+        return;
+    }
+    const uintptr_t mis = (uintptr_t)ptr & 3;
+    v.p = ptr - mis;
+    v.bytes = len + mis;
+    v.off_bits = 8 * mis;
+    v.b = 8 * ES;
+    v.mask = ES == 8 ? ~0ull : ((1ull << (8 * ES)) - 1);
+}
+
 // ok = false when AFL metadata is malformed (the view is then empty)
 template <int ES>
 __device__ __forceinline__ DViewCtx dview_ctx(const BItem &it, const StreamDesc *S, int slot, bool &ok)
@@ -320,16 +339,12 @@ __device__ __forceinline__ DViewCtx dview_ctx(const BItem &it, const StreamDesc 
     const DView &d = it.dv[slot - 1];
     if (d.data < 0) {  // no view: the input stream itself
         const StreamDesc in = S[it.in[slot]];
-        v.p = in.ptr;
-        v.n = in.len / ES;
-        v.aligned = ((uintptr_t)in.ptr & (ES - 1)) == 0;
+        dview_plain<ES>(v, in.ptr, in.len);
         return v;
     }
     const StreamDesc data = S[d.data];
     if (d.afl_meta < 0) {
-        v.p = data.ptr;
-        v.n = data.len / ES;
-        v.aligned = ((uintptr_t)data.ptr & (ES - 1)) == 0;
+        dview_plain<ES>(v, data.ptr, data.len);
     } else {
         const StreamDesc meta = S[d.afl_meta];
         if (data.len) {
