@@ -175,7 +175,8 @@ constexpr uint32_t kBTile = 256 * kBVPT; // elements per tile of those passes (2
 constexpr uint32_t kBMinMaxTile = 8192;
 constexpr uint32_t kBHistTile = 16384;
 constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
-constexpr uint32_t kBHistSmem = 2048;
+constexpr uint32_t kBHistSmem = 2048;    // shared hash slots of a histogram block (8-byte values)
+constexpr uint32_t kBHistPacked = 4096;  // the same for values of up to 4 bytes (packed slots)
 
 // scratch layout of a histogram item
 struct BHistHdr {

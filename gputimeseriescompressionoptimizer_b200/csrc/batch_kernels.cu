@@ -277,7 +277,7 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
     constexpr unsigned long long EMPTY = ~0ull;
     unsigned long long *skeys = (unsigned long long *)smem;
     unsigned int *scounts = (unsigned int *)(smem + 8 * kBHistSmem);
-    unsigned long long(*snan)[4] = (unsigned long long(*)[4])(smem + 12 * kBHistSmem);
+    unsigned long long(*snan)[4] = (unsigned long long(*)[4])(smem + 8 * kBHistPacked);
     const StreamDesc in = S[it.in[0]];
     const ViewCtx vc = view_ctx<ES>(it, in);
     const uint64_t n = vc.n;
@@ -291,7 +291,53 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         for (uint64_t w = t0 / 16 + threadIdx.x; w < (e_end + 15) / 16; w += kBThreads) words[w] = 0u;
     }
     unsigned long long nan_min[4] = {EMPTY, EMPTY, EMPTY, EMPTY};
-    if (t0 < n) {
+    if (ES <= 4 && t0 < n) {
+        // values of up to 4 bytes: 32-bit keys and counts (twice the slots of the layout below); a
+        // value already in the table costs a plain key read and one 32-bit atomicAdd.  0xffffffff
+        // marks an empty slot, so that value itself is counted apart.
+        uint32_t *k32 = (uint32_t *)smem;
+        uint32_t *c32 = k32 + kBHistPacked;
+        __shared__ uint32_t s_ones;
+        for (int i = threadIdx.x; i < (int)kBHistPacked; i += kBThreads) {
+            k32[i] = 0xffffffffu;
+            c32[i] = 0u;
+        }
+        if (threadIdx.x == 0) s_ones = 0;
+        __syncthreads();
+        const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
+        for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
+            const unsigned long long key = view_elem<ES>(it, vc, in.ptr, i);
+            if (is_nan_bits(key, o)) {
+                unsigned long long k = order_key(key, ES, o);
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
+                continue;
+            }
+            const uint32_t kk = (uint32_t)key;
+            if (kk == 0xffffffffu) {
+                atomicAdd(&s_ones, 1u);
+                continue;
+            }
+            uint32_t h = (uint32_t)bhash(key) & (kBHistPacked - 1);
+            bool done = false;
+            for (int p = 0; p < 8; p++) {
+                uint32_t cur = ((volatile uint32_t *)k32)[h];
+                if (cur == 0xffffffffu) cur = atomicCAS(&k32[h], 0xffffffffu, kk);
+                if (cur == 0xffffffffu || cur == kk) {
+                    atomicAdd(&c32[h], 1u);
+                    done = true;
+                    break;
+                }
+                h = (h + 1) & (kBHistPacked - 1);
+            }
+            if (!done) g_insert(t, key, 1u, status);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < (int)kBHistPacked; i += kBThreads)
+            if (k32[i] != 0xffffffffu) g_insert(t, (unsigned long long)k32[i], c32[i], status);
+        if (threadIdx.x == 0 && s_ones) g_insert(t, 0xffffffffull, s_ones, status);
+    } else if (t0 < n) {
         for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads) {
             skeys[i] = EMPTY;
             scounts[i] = 0;
@@ -1010,7 +1056,7 @@ __device__ void p_vmeta(const BItem &it, StreamDesc *S)
 constexpr size_t stage_smem(int op)
 {
     return op == B_AFL_PACK ? 8 * (kBTile + kBTile / 16 + 8)
-         : op == B_HIST     ? 12 * kBHistSmem + 8 * 4 * (kBThreads / 32)
+         : op == B_HIST     ? 8 * kBHistPacked + 8 * 4 * (kBThreads / 32)
          : op == B_TOPK     ? sizeof(Cand) * kBThreads * 4
          : op == B_SPLIT    ? 8 * kBTile
                             : 16;
