@@ -49,7 +49,7 @@ struct HNode {
     uint64_t lb_off = 64, tab_off = 0, starts_off = 0, g_sizes = 0, g_incl = 0, g_layout = 0, tab_cap = 0;
     uint64_t hist_tiles = 0, split_tiles = 0, gfc_warps = 0;
     // decode scratch layout (relative to scratch)
-    uint64_t dlb_off = 0, dends_off = 0, druns_off = 0, dsizes_off = 0, dincl_off = 0;
+    uint64_t dlb_off = 0, dends_off = 0, druns_off = 0, dtiles_off = 0, dsizes_off = 0, dincl_off = 0;
     int last_c_level = 0, last_d_level = 0;
     // compress input view: the node reads stream in_sid through vop[] (V_SCALE ops take their
     // constant from scale node vnode[k]); a virtual node's own output is never written, its child
@@ -286,7 +286,8 @@ void BatchEngine::plan_passes()
             nd.dlb_off = nd.c_bytes;
             nd.dends_off = nd.dlb_off + align_up(lookback_bytes(tiles), 256);
             nd.druns_off = nd.dends_off + align_up(8 * n + 16, 256);
-            d = nd.druns_off + 256 - nd.c_bytes;
+            nd.dtiles_off = nd.druns_off + 256;  // run holding each expand tile's first element
+            d = nd.dtiles_off + align_up(8 * tiles + 16, 256) - nd.c_bytes;
             break;
         case GTSC_GFC:
             if (is_fp(nd.dt)) {
@@ -528,6 +529,7 @@ void BatchEngine::plan_passes()
             it.p[0] = nd.dlb_off;
             it.p[1] = nd.dends_off;
             it.p[2] = nd.druns_off;
+            it.p[3] = nd.dtiles_off;
             ps.push_back(it);
             BItem ex = it;
             ex.op = B_RLE_EXPAND;

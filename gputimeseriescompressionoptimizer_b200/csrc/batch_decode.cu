@@ -430,10 +430,17 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
     }
     __syncthreads();
     unsigned long long acc = s_prefix + excl;
+    unsigned long long *first_run = (unsigned long long *)(it.scratch + it.p[3]);
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) {
         acc += (unsigned long long)v[j];
-        if (base + j < (uint64_t)runs) ends[base + j] = acc;
+        if (base + j < (uint64_t)runs) {
+            ends[base + j] = acc;
+            // the expand tiles whose first element lies in this run start from it
+            if (v[j] > 0)
+                for (uint64_t t = (acc - (unsigned long long)v[j] + kBTile - 1) / kBTile; t <= (acc - 1) / kBTile && t < it.tiles; t++)
+                    first_run[t] = base + j;
+        }
     }
     // p[2] holds the run count for the expand pass
     if (tile == 0 && threadIdx.x == 0) *(unsigned long long *)(it.scratch + it.p[2]) = (unsigned long long)runs;
@@ -442,7 +449,8 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
 template <int ES>
 __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
 {
-    __shared__ uint64_t s_lo, s_hi;
+    // the tile's run ends relative to its first element, clamped to kBTile (at most kBTile + 1 runs)
+    __shared__ uint16_t s_end[kBTile + 2];
     bool ok;
     const DViewCtx values = dview_ctx<ES>(it, S, 2, ok);
     StreamDesc &out = S[it.out[0]];
@@ -456,30 +464,34 @@ __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
     const uint64_t t0 = (uint64_t)tile * kBTile;
     if (t0 >= n) return;
-    auto ub = [&](uint64_t lo, uint64_t hi, uint64_t pos) {
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (ends[mid] > pos) hi = mid;
-            else lo = mid + 1;
-        }
-        return lo;
-    };
-    if (threadIdx.x == 0) {
-        s_lo = ub(0, runs, t0);
-        const uint64_t last = t0 + kBTile - 1 < n ? t0 + kBTile - 1 : n - 1;
-        const uint64_t hi = ub(s_lo, runs, last);
-        s_hi = hi < runs ? hi + 1 : runs;
+    // the scan pass recorded the run holding each tile's first element
+    const unsigned long long *first_run = (const unsigned long long *)(it.scratch + it.p[3]);
+    uint64_t r_lo = first_run[tile];
+    uint64_t r_hi = t0 + kBTile < n && tile + 1 < it.tiles ? first_run[tile + 1] + 1 : runs;
+    if (r_hi > runs) r_hi = runs;
+    if (r_lo > r_hi) r_lo = r_hi;  // only on corrupt lengths (reported by the scan pass)
+    // <= kBTile + 1 when ends rise by at least 1 per run; corrupt zero-length runs are cut off
+    const uint32_t m = (uint32_t)(r_hi - r_lo < kBTile + 2 ? r_hi - r_lo : kBTile + 2);
+    for (uint32_t k = threadIdx.x; k < m; k += kBThreads) {
+        const uint64_t e = ends[r_lo + k] - t0;
+        s_end[k] = (uint16_t)(e < kBTile ? e : kBTile);
     }
     __syncthreads();
-    const uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT;
+    const uint32_t b = threadIdx.x * kBVPT;  // relative to t0
+    const uint64_t base = t0 + b;
     if (base >= n) return;
-    uint64_t r = ub(s_lo, s_hi, base);
+    uint32_t lo = 0, hi = m;  // first staged run ending after b
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_end[mid] > b) hi = mid;
+        else lo = mid + 1;
+    }
     uint64_t v[kBVPT];
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) {
-        const uint64_t i = base + j;
-        while (r < runs && ends[r] <= i) ++r;
-        v[j] = (i < n && r < runs && r < values.n) ? dview_elem<ES>(values, r) : 0;
+        while (lo < m && s_end[lo] <= b + j) ++lo;
+        const uint64_t r = r_lo + lo;
+        v[j] = (base + j < n && lo < m && r < values.n) ? dview_elem<ES>(values, r) : 0;
     }
     store_run<ES, kBVPT>(out.ptr, base, n, v);
     (void)status;
