@@ -513,13 +513,15 @@ void BatchEngine::plan_passes()
         case GTSC_DELTA: { BItem it = ditem(B_DELTA_DEC, t2k); it.p[0] = nd.dlb_off; ps.push_back(it); break; }
         case GTSC_SCALE: ps.push_back(ditem(B_SCALE_ADD, t2k)); break;
         case GTSC_PATCH: case GTSC_DICT: case GTSC_CONST: {
-            BItem it = ditem(B_MERGE, t2k);
+            BItem it = ditem(B_MERGE, cdiv(t2k, kBMergeSub));
             it.mode = (int16_t)(nd.enc == GTSC_PATCH ? SPLIT_LOWER : nd.enc == GTSC_DICT ? SPLIT_DICT : SPLIT_NOT_CONST);
             it.p[0] = nd.dlb_off;
+            it.p[1] = t2k;
             // the stencil counts need only the node's metadata, parsed before the first level: one
             // launch ahead of every level (a merge may itself run at level 0)
             BItem cnt = it;
             cnt.op = B_MERGE_COUNT;
+            cnt.tiles = (uint32_t)t2k;
             pass_d.push_back(Pass{-1, B_MERGE_COUNT, id, cnt});
             ps.push_back(it);
             break;

@@ -174,6 +174,7 @@ constexpr uint32_t kBVPT = 16;         // values per thread of the element-wise 
 constexpr uint32_t kBTile = 256 * kBVPT; // elements per tile of those passes (256 threads per block)
 constexpr uint32_t kBMinMaxTile = 8192;
 constexpr uint32_t kBHistTile = 16384;
+constexpr uint32_t kBMergeSub = 4;      // kBTile tiles per block of the merge pass
 constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
 constexpr uint32_t kBHistSmem = 2048;    // shared hash slots of a histogram block (8-byte values)
 constexpr uint32_t kBHistPacked = 4096;  // the same for values of up to 4 bytes (packed slots)

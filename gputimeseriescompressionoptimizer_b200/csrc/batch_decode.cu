@@ -182,6 +182,20 @@ __device__ void p_scale_add(const BItem &it, uint32_t tile, StreamDesc *S, uint3
 }
 
 // ------------------------------------------------------------------------------- merge
+// elements [p0, p0 + cnt) of a decode view into shared memory at element slot `at`; unpacked views
+// take plain loads, packed ones the view's bit extraction
+template <int ES>
+__device__ __forceinline__ void stage_view(const DViewCtx &v, uint64_t p0, uint32_t cnt, uint8_t *sm, uint32_t at)
+{
+    if (v.b == 0) {
+        const uint64_t c = v.c0 + v.c1;
+        for (uint32_t i = threadIdx.x; i < cnt; i += kBThreads)
+            st_elem<ES>(sm, at + i, wrap_es(ld_elem<ES>(v.p, p0 + i) + c, ES));  // plain views are aligned
+    } else {
+        for (uint32_t i = threadIdx.x; i < cnt; i += kBThreads) st_elem<ES>(sm, at + i, dview_elem<ES>(v, p0 + i));
+    }
+}
+
 // Merge tiles find their offsets in the match / non-match streams without a look-back chain: a
 // counting pass (B_MERGE_COUNT, any order) stores each tile's number of stencil matches and adds it
 // to its group of kMergeGroup tiles; a merge tile's exclusive prefix is then the sum of the groups
@@ -191,11 +205,11 @@ constexpr uint32_t kMergeGroup = 64;
 
 __device__ __forceinline__ unsigned long long *merge_groups(const BItem &it)
 {
-    return (unsigned long long *)(it.scratch + it.p[0] + 16);
+    return (unsigned long long *)(it.scratch + it.p[0] + 16);  // p[1] = tiles of kBTile elements
 }
 __device__ __forceinline__ uint32_t *merge_counts(const BItem &it)
 {
-    return (uint32_t *)(it.scratch + it.p[0] + 16 + 8ull * ((it.tiles + kMergeGroup - 1) / kMergeGroup));
+    return (uint32_t *)(it.scratch + it.p[0] + 16 + 8ull * ((it.p[1] + kMergeGroup - 1) / kMergeGroup));
 }
 
 // the stencil of a merge node and the element count its rest byte gives (0 when malformed)
@@ -249,8 +263,9 @@ __device__ __forceinline__ unsigned long long merge_prefix(const BItem &it, uint
 }
 
 template <int ES>
-__device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, uint8_t *sm)
+__device__ void p_merge(const BItem &it, uint32_t stile, StreamDesc *S, uint32_t *status, uint8_t *sm)
 {
+    // a block merges kBMergeSub consecutive tiles of its item; the setup below is done once for them
     __shared__ unsigned long long ws[32];
     const int mode = it.mode;
     const StreamDesc meta = S[it.in[0]];
@@ -262,7 +277,7 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     if (mode != SPLIT_NOT_CONST) v2 = dview_ctx<ES>(it, S, 2, ok2);
     StreamDesc &out = S[it.out[0]];
     if (!ok1 || !ok2) {
-        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+        if (stile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
         return;
     }
     const uint64_t len1 = mode == SPLIT_DICT ? in1.len : v1.n * ES, len2 = v2.n * ES;
@@ -273,23 +288,23 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     uint64_t n = 0;
     if (!empty) {
         if (sbytes < 1) {
-            if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+            if (stile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
             return;
         }
         const int rest = (int8_t)stencil[0];
         int64_t nn = (int64_t)(sbytes - 1) * 8;
         if (rest) nn -= 8 - rest;
         if (nn < 0 || rest < 0 || rest > 7) {
-            if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
+            if (stile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_FORMAT);
             return;
         }
         n = (uint64_t)nn;
     }
     if (n * ES > out.cap) {
-        if (tile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
+        if (stile == 0 && threadIdx.x == 0) set_status(status, GTSC_ERR_CAPACITY);
         return;
     }
-    if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
+    if (stile == 0 && threadIdx.x == 0) out.len = n * ES;
     // dictionary stream: 16-byte header, 4 values, codes
     uint64_t top[4] = {0, 0, 0, 0}, yes_cap = 0, no_cap = v2.n;
     const uint8_t *codes = nullptr;
@@ -307,7 +322,10 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     } else {
         yes_cap = v1.n;
     }
-    if ((uint64_t)tile * kBTile >= n) return;  // past the output
+    bool bad = false;
+    for (uint32_t sub = 0; sub < kBMergeSub; sub++) {
+    const uint32_t tile = stile * kBMergeSub + sub;
+    if ((uint64_t)tile * kBTile >= n) break;  // past the output
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     const uint32_t valid_mask = base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
     uint32_t bits = 0;
@@ -324,7 +342,6 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     const uint64_t tile_n = tile_base < n ? (n - tile_base < kBTile ? n - tile_base : kBTile) : 0;
     const uint64_t ny = total, nn = tile_n - ny;
     const uint64_t yes0 = prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
-    bool bad = false;
     // dictionary: the code words of the tile's matches, staged once (coalesced, whole words)
     __shared__ uint32_t s_codes[kBTile / 16 + 2];
     const uint64_t w0 = yes0 >> 4;
@@ -337,47 +354,56 @@ __device__ void p_merge(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
             s_codes[k] = w >= avail ? 0u : al ? __ldg((const uint32_t *)codes + w) : (uint32_t)ld_unaligned<4>(codes + 4 * w);
         }
     }
+    // in-tile counts fit 32 bits; a stream position past the stream's end is corrupt input
+    const uint32_t ny32 = (uint32_t)ny, nn32 = (uint32_t)nn;
     if (mode != SPLIT_DICT) {
-        for (uint64_t i = threadIdx.x; i < ny; i += kBThreads) {
-            if (yes0 + i < yes_cap) st_elem<ES>(sm, i, dview_elem<ES>(v1, yes0 + i));
-            else bad = true;
-        }
+        const uint32_t ok = yes_cap > yes0 ? (uint32_t)(yes_cap - yes0 < ny ? yes_cap - yes0 : ny) : 0u;
+        bad |= ok < ny32;
+        stage_view<ES>(v1, yes0, ok, sm, 0);
     }
     if (mode != SPLIT_NOT_CONST) {
-        for (uint64_t i = threadIdx.x; i < nn; i += kBThreads) {
-            if (no0 + i < no_cap) st_elem<ES>(sm, ny + i, dview_elem<ES>(v2, no0 + i));
-            else bad = true;
-        }
+        const uint32_t ok = no_cap > no0 ? (uint32_t)(no_cap - no0 < nn ? no_cap - no0 : nn) : 0u;
+        bad |= ok < nn32;
+        stage_view<ES>(v2, no0, ok, sm, ny32);
     }
     __syncthreads();
     if (base < n) {
-        uint64_t ly = excl, ln = (uint64_t)threadIdx.x * kBVPT - excl;
+        uint32_t ly = (uint32_t)excl, ln = threadIdx.x * kBVPT - (uint32_t)excl;
         uint64_t v[kBVPT];
+        if (mode == SPLIT_DICT) {
+            // match k of the tile is code (yes0 + k) of the stream: word ((yes0 & 15) + k) / 16 of s_codes
+            const uint32_t y0 = (uint32_t)(yes0 & 15);
+            const uint32_t lim = yes_cap > yes0 ? (uint32_t)(yes_cap - yes0 < kBTile ? yes_cap - yes0 : kBTile) : 0u;
 #pragma unroll
-        for (int j = 0; j < (int)kBVPT; j++) {
-            v[j] = 0;
-            if (!((valid_mask >> j) & 1u)) continue;
-            if ((bits >> j) & 1u) {
-                if (mode == SPLIT_DICT) {
-                    const uint64_t y = yes0 + ly;
-                    if (y >= yes_cap) {
-                        bad = true;
-                    } else {
-                        const uint32_t w = s_codes[(y >> 4) - w0];
-                        const uint32_t c = (w >> (2 * (y & 15))) & 3u;  // select, not an indexed array
-                        v[j] = c == 0 ? top[0] : c == 1 ? top[1] : c == 2 ? top[2] : top[3];
-                    }
-                } else if (ly < ny) {
-                    v[j] = ld_elem_sm<ES>(sm, ly);
+            for (int j = 0; j < (int)kBVPT; j++) {
+                v[j] = 0;
+                if ((bits >> j) & 1u) {
+                    bad |= ly >= lim;
+                    const uint32_t y = y0 + ly;
+                    const uint32_t c = (s_codes[y >> 4] >> (2 * (y & 15))) & 3u;  // select, not an indexed array
+                    v[j] = c == 0 ? top[0] : c == 1 ? top[1] : c == 2 ? top[2] : top[3];
+                    ++ly;
+                } else if ((valid_mask >> j) & 1u) {
+                    v[j] = ld_elem_sm<ES>(sm, ny32 + ln);
+                    ++ln;
                 }
-                ++ly;
-            } else {
-                if (mode == SPLIT_NOT_CONST) v[j] = top[0];
-                else v[j] = ld_elem_sm<ES>(sm, ny + ln);
-                ++ln;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < (int)kBVPT; j++) {
+                v[j] = 0;
+                if ((bits >> j) & 1u) {
+                    v[j] = ld_elem_sm<ES>(sm, ly);
+                    ++ly;
+                } else if ((valid_mask >> j) & 1u) {
+                    v[j] = mode == SPLIT_NOT_CONST ? top[0] : ld_elem_sm<ES>(sm, ny32 + ln);
+                    ++ln;
+                }
             }
         }
         store_run<ES, kBVPT>(out.ptr, base, n, v);
+    }
+    __syncthreads();  // the next tile restages the shared buffers
     }
     if (bad) set_status(status, GTSC_ERR_FORMAT);
 }
