@@ -766,15 +766,21 @@ k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *cou
     __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : 16];
     if (*(volatile uint32_t *)(status + 1)) return;
     if constexpr (!dec_persistent(OP)) {
-        BItem it;
         uint32_t tile;
-        locate<DYN>(items, item_of, counter, it, tile);
+        const BItem &it = locate<DYN>(items, item_of, counter, tile);
         if (tile >= it.tiles) return;
         run_dec<OP>(it, tile, S, status, smem);
     } else {
         uint32_t t = blockIdx.x;
+        uint32_t cur = 0xffffffffu;  // the item in the shared descriptor
         while (t < total_tiles) {
-            const BItem it = items[item_of[t]];
+            const uint32_t k = item_of[t];
+            if (k != cur) {
+                __syncthreads();  // nobody reads the previous descriptor any more
+                shared_item(items, k);
+                cur = k;
+            }
+            const BItem &it = shared_item_ref();
             const uint32_t tile = t - (uint32_t)it.tile_base;
             if (tile >= dec_extent<OP>(it, S)) {
                 const uint64_t next = it.tile_base + it.tiles;
@@ -887,9 +893,8 @@ __global__ void k_frame_layout(const BColumnDev *cols, int ncols, BNodeDev *node
 __global__ void __launch_bounds__(kBThreads)
 k_frame_copy(const BItem *items, const uint32_t *item_of, const BNodeDev *nodes, const StreamDesc *S, uint8_t *framed)
 {
-    BItem it;
     uint32_t tile;
-    locate<false>(items, item_of, nullptr, it, tile);
+    const BItem &it = locate<false>(items, item_of, nullptr, tile);
     const BNodeDev &nd = nodes[it.p[0]];
     const StreamDesc src = S[it.p[1] ? nd.data : nd.meta];
     const uint64_t dst = it.p[1] ? nd.data_dst : nd.meta_dst;

@@ -418,9 +418,26 @@ __device__ __forceinline__ void load_dview(const DViewCtx &v, uint64_t base, uin
 // order from a counter (look-back needs every predecessor claimed first), the others use the
 // block index; item_of[t] is the item of global tile t (one table per launch), and for DYN launches
 // item_of[grid + c] is the tile taken by the c-th claim.
+// copies items[k] into the block's shared descriptor (every thread of the block calls it; the
+// caller makes sure no thread still reads the previous one); fields are then read from shared
+// memory instead of every thread loading the whole descriptor into registers
+static __shared__ __align__(16) unsigned long long s_item_words[sizeof(BItem) / 8];  // raw: BItem has initialisers
+
+__device__ __forceinline__ const BItem &shared_item_ref() { return *reinterpret_cast<const BItem *>(s_item_words); }
+
+__device__ __forceinline__ const BItem &shared_item(const BItem *items, uint32_t k)
+{
+    static_assert(sizeof(BItem) % 8 == 0, "BItem is copied in 8-byte words");
+    constexpr int W = (int)(sizeof(BItem) / 8);
+    if (threadIdx.x < W)
+        s_item_words[threadIdx.x] = __ldg((const unsigned long long *)(items + k) + threadIdx.x);
+    __syncthreads();
+    return shared_item_ref();
+}
+
 template <bool DYN>
-__device__ __forceinline__ void locate(const BItem *items, const uint32_t *item_of, uint32_t *counter, BItem &it,
-                                       uint32_t &tile)
+__device__ __forceinline__ const BItem &locate(const BItem *items, const uint32_t *item_of, uint32_t *counter,
+                                               uint32_t &tile)
 {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_idx;
@@ -433,8 +450,8 @@ __device__ __forceinline__ void locate(const BItem *items, const uint32_t *item_
         s_tile = (uint32_t)(t - items[idx].tile_base);
     }
     __syncthreads();
-    it = items[s_idx];
     tile = s_tile;
+    return shared_item(items, s_idx);
 }
 
 }  // namespace gtsc

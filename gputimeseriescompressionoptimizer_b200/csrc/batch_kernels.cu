@@ -1116,15 +1116,21 @@ k_bstage(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *c
     constexpr bool DYN = OP == B_SPLIT || OP == B_RLE_HEADS || OP == B_GFC_SCAN;
     __shared__ __align__(16) unsigned char smem[stage_smem(OP)];
     if constexpr (!stage_persistent(OP)) {
-        BItem it;
         uint32_t tile;
-        locate<DYN>(items, item_of, counter, it, tile);
+        const BItem &it = locate<DYN>(items, item_of, counter, tile);
         if (tile >= it.tiles) return;
         run_stage<OP>(it, tile, S, status, smem);
     } else {
         uint32_t t = blockIdx.x;
+        uint32_t cur = 0xffffffffu;  // the item in the shared descriptor
         while (t < total_tiles) {
-            const BItem it = items[item_of[t]];
+            const uint32_t k = item_of[t];
+            if (k != cur) {
+                __syncthreads();  // nobody reads the previous descriptor any more
+                shared_item(items, k);
+                cur = k;
+            }
+            const BItem &it = shared_item_ref();
             const uint32_t tile = t - (uint32_t)it.tile_base;
             if (tile >= stage_extent<OP>(it, S)) {
                 const uint64_t next = it.tile_base + it.tiles;  // the next item's first tile
