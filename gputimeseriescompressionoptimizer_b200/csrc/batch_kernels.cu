@@ -538,19 +538,23 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     uint64_t v[kBVPT];
     load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
     uint32_t bits = 0, codes = 0;
+    if (mode == SPLIT_LOWER) {
 #pragma unroll
-    for (int j = 0; j < (int)kBVPT; j++) {
-        bool f = false;
-        uint32_t code = 0;
-        if (mode == SPLIT_LOWER) f = lt_native(v[j], thr, ES, o);
-        else if (mode == SPLIT_NOT_CONST) f = !bsame(v[j], top[0], o);
-        else {
+        for (int j = 0; j < (int)kBVPT; j++) bits |= (uint32_t)lt_native(v[j], thr, ES, o) << j;
+    } else {
+        // equal bits and not NaN (bsame): NaN-ness once per value, not once per candidate
+        const bool fp = o != ORD_INT;
 #pragma unroll
-            for (int k = 0; k < 4; k++)
-                if (bsame(v[j], top[k], o)) { f = true; code |= (uint32_t)k; }
+        for (int j = 0; j < (int)kBVPT; j++) {
+            const bool nan = fp && is_nan_bits(v[j], o);
+            if (mode == SPLIT_NOT_CONST) {
+                bits |= (uint32_t)(nan || v[j] != top[0]) << j;
+            } else {
+                const uint32_t e0 = v[j] == top[0], e1 = v[j] == top[1], e2 = v[j] == top[2], e3 = v[j] == top[3];
+                bits |= (uint32_t)(!nan && (e0 | e1 | e2 | e3)) << j;
+                codes |= (nan ? 0u : (e1 | (e2 << 1) | (e3 * 3u))) << (2 * j);
+            }
         }
-        bits |= (uint32_t)f << j;
-        codes |= code << (2 * j);
     }
     if (base < n) {
         const uint64_t valid = n - base;
