@@ -599,14 +599,14 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
         uint32_t *words = (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES);
         const uint64_t y0 = yes0 + excl, y1 = y0 + __popc(yes_bits);
         uint32_t acc0 = 0u, acc1 = 0u;  // the first and the second code word of the range
-        uint64_t y = y0;
+        uint32_t r = (uint32_t)(y0 & 15);  // position inside the first word (at most 15 + 16 < 32)
 #pragma unroll
         for (int j = 0; j < (int)kBVPT; j++)
             if ((yes_bits >> j) & 1u) {
-                const uint32_t bits2 = ((codes >> (2 * j)) & 3u) << (2 * (y & 15));
-                if ((y >> 4) == (y0 >> 4)) acc0 |= bits2;
+                const uint32_t bits2 = ((codes >> (2 * j)) & 3u) << (2 * (r & 15));
+                if (r < 16) acc0 |= bits2;
                 else acc1 |= bits2;
-                ++y;
+                ++r;
             }
         if (y1 > y0) {
             for (uint64_t w = y0 >> 4; w <= (y1 - 1) >> 4; w++) {
