@@ -1008,6 +1008,30 @@ __device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool d
     }
 }
 
+// one warp copies n bytes between any addresses: head bytes up to a 4-byte aligned destination,
+// then whole words funnel-shifted out of aligned source words, then the tail
+__device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint64_t n, int lane)
+{
+    const uint64_t head = (4 - ((uintptr_t)dst & 3)) & 3;
+    const uint64_t h = head < n ? head : n;
+    if ((uint64_t)lane < h) dst[lane] = src[lane];
+    if (n <= h) return;
+    uint32_t *d = (uint32_t *)(dst + h);
+    const uint8_t *sp = src + h;
+    const uint64_t words = (n - h) / 4;
+    const uint32_t sh = 8 * (uint32_t)((uintptr_t)sp & 3);
+    const uint32_t *sw = (const uint32_t *)((uintptr_t)sp & ~(uintptr_t)3);
+    if (sh == 0) {
+#pragma unroll 4
+        for (uint64_t k = lane; k < words; k += 32) d[k] = sw[k];
+    } else {
+#pragma unroll 4
+        for (uint64_t k = lane; k < words; k += 32) d[k] = __funnelshift_r(sw[k], sw[k + 1], sh);
+    }
+    const uint64_t tail = (n - h) - 4 * words;
+    if ((uint64_t)lane < tail) ((uint8_t *)d)[4 * words + lane] = sp[4 * words + lane];
+}
+
 template <bool DBL>
 __device__ void p_gfc_compact(const BItem &it, uint32_t tile, StreamDesc *S)
 {
@@ -1026,7 +1050,7 @@ __device__ void p_gfc_compact(const BItem &it, uint32_t tile, StreamDesc *S)
     const uint64_t dst0 = incl[w] - size;
     const uint8_t *src = layout + d_gfc_start(g, w);
     uint8_t *out = S[it.out[2]].ptr;
-    for (uint64_t b = lane; b < size; b += 32) out[dst0 + b] = src[b];
+    warp_copy(out + dst0, src, size, lane);
     if (w == g.warps - 1 && lane == 0) S[it.out[2]].len = incl[w];
 }
 
