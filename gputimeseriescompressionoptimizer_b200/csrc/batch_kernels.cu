@@ -917,10 +917,23 @@ __device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S)
     const uint64_t cb = d_gfc_begin(g, w), ce = d_gfc_cut(g, w);
     const uint64_t start = d_gfc_start(g, w);
     uint64_t off = start, last = 0;
-    for (uint64_t s = cb; s < ce; s += 32) {
-        const uint64_t i = s + lane;
-        uint64_t x = 0;
-        if (i < n) x = view_elem<DBL ? 8 : 4>(it, vc, in.ptr, i);
+    // values of the next 4 subchunks are in flight while one is encoded
+    uint64_t xb[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const uint64_t i = cb + 32 * q + lane;
+        xb[q] = cb + 32 * q < ce && i < n ? view_elem<DBL ? 8 : 4>(it, vc, in.ptr, i) : 0;
+    }
+    for (uint64_t s0 = cb; s0 < ce; s0 += 128)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const uint64_t s = s0 + 32 * q;
+        if (s >= ce) break;
+        const uint64_t x = xb[q];
+        {
+            const uint64_t i = s + 128 + lane;
+            xb[q] = s + 128 < ce && i < n ? view_elem<DBL ? 8 : 4>(it, vc, in.ptr, i) : 0;
+        }
         uint64_t diff;
         uint32_t sign, mb, code;
         if (DBL) {
