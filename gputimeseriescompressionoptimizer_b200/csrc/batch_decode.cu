@@ -262,6 +262,45 @@ __device__ __forceinline__ unsigned long long merge_prefix(const BItem &it, uint
     return total;
 }
 
+// The counting launch of the merges: one warp per tile (512 stencil bytes, 16 per lane), so no
+// block barrier sits between a tile's loads and its count.
+__global__ void __launch_bounds__(kBThreads)
+k_merge_count(const BItem *items, const uint32_t *item_of, StreamDesc *S, const uint32_t *status, uint32_t total_tiles)
+{
+    if (*(volatile const uint32_t *)(status + 1)) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (kBThreads / 32);
+    for (uint32_t t = blockIdx.x * (kBThreads / 32) + (threadIdx.x >> 5); t < total_tiles; t += warps) {
+        const BItem &it = items[item_of[t]];
+        const uint32_t tile = t - (uint32_t)it.tile_base;
+        uint64_t n;
+        const uint8_t *stencil;
+        switch (it.es) {
+        case 1: stencil = merge_stencil<1>(it, S[it.in[0]], n); break;
+        case 2: stencil = merge_stencil<2>(it, S[it.in[0]], n); break;
+        case 4: stencil = merge_stencil<4>(it, S[it.in[0]], n); break;
+        default: stencil = merge_stencil<8>(it, S[it.in[0]], n); break;
+        }
+        const uint64_t e0 = (uint64_t)tile * kBTile + (uint64_t)lane * 128;  // this lane's 128 elements
+        uint32_t c = 0;
+        if (e0 < n) {
+            const uint64_t valid = n - e0 < 128 ? n - e0 : 128;
+            const uint8_t *b = stencil + 1 + e0 / 8;
+            for (uint32_t q = 0; q < (valid + 7) / 8; q++) {
+                uint32_t byte = b[q];
+                const uint64_t left = valid - 8ull * q;
+                if (left < 8) byte &= (1u << left) - 1;
+                c += __popc(byte);
+            }
+        }
+        for (int o = 16; o; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+        if (lane == 0) {
+            merge_counts(it)[tile] = c;
+            if (c) atomicAdd(merge_groups(it) + tile / kMergeGroup, (unsigned long long)c);
+        }
+    }
+}
+
 template <int ES>
 __device__ void p_merge(const BItem &it, uint32_t stile, StreamDesc *S, uint32_t *status, uint8_t *sm)
 {
@@ -1018,7 +1057,15 @@ void launch_batch_decode_stage(int op, const BItem *d_items, const uint32_t *d_i
         GTSC_STAGE(B_DELTA_DEC)
         GTSC_STAGE(B_SCALE_ADD)
         GTSC_STAGE(B_MERGE)
-        GTSC_STAGE(B_MERGE_COUNT)
+    case B_MERGE_COUNT: {
+        int per_sm = 0;
+        GTSC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_merge_count, kBThreads, 0));
+        const uint64_t warps = (total_tiles + kBThreads / 32 - 1) / (kBThreads / 32);
+        const uint64_t resident = (uint64_t)std::max(per_sm, 1) * (uint64_t)sm_count();
+        const unsigned g = (unsigned)std::min<uint64_t>(warps, resident);
+        k_merge_count<<<g, kBThreads, 0, s>>>(d_items, d_item_of, d_streams, d_status, (uint32_t)total_tiles);
+        break;
+    }
         GTSC_STAGE(B_RLE_SCAN)
         GTSC_STAGE(B_RLE_EXPAND)
         GTSC_STAGE(B_F2I_DEC)
