@@ -405,42 +405,35 @@ __device__ void p_merge(const BItem &it, uint32_t stile, StreamDesc *S, uint32_t
         bad |= ok < nn32;
         stage_view<ES>(v2, no0, ok, sm, ny32);
     }
+    // every thread's 16 stencil bits and the matches before them, for the striped assembly below
+    __shared__ uint16_t s_bits[kBThreads], s_excl[kBThreads];
+    s_bits[threadIdx.x] = (uint16_t)bits;
+    s_excl[threadIdx.x] = (uint16_t)excl;
     __syncthreads();
-    if (base < n) {
-        uint32_t ly = (uint32_t)excl, ln = threadIdx.x * kBVPT - (uint32_t)excl;
-        uint64_t v[kBVPT];
-        if (mode == SPLIT_DICT) {
-            // match k of the tile is code (yes0 + k) of the stream: word ((yes0 & 15) + k) / 16 of s_codes
-            const uint32_t y0 = (uint32_t)(yes0 & 15);
-            const uint32_t lim = yes_cap > yes0 ? (uint32_t)(yes_cap - yes0 < kBTile ? yes_cap - yes0 : kBTile) : 0u;
-#pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) {
-                v[j] = 0;
-                if ((bits >> j) & 1u) {
-                    bad |= ly >= lim;
-                    const uint32_t y = y0 + ly;
-                    const uint32_t c = (s_codes[y >> 4] >> (2 * (y & 15))) & 3u;  // select, not an indexed array
-                    v[j] = c == 0 ? top[0] : c == 1 ? top[1] : c == 2 ? top[2] : top[3];
-                    ++ly;
-                } else if ((valid_mask >> j) & 1u) {
-                    v[j] = ld_elem_sm<ES>(sm, ny32 + ln);
-                    ++ln;
-                }
+    // step j writes elements j * 256 + t: consecutive threads read consecutive staged values (no
+    // bank conflicts) and store consecutive outputs (coalesced)
+    const uint32_t y0 = (uint32_t)(yes0 & 15);
+    const uint32_t lim = yes_cap > yes0 ? (uint32_t)(yes_cap - yes0 < kBTile ? yes_cap - yes0 : kBTile) : 0u;
+    uint8_t *dst = out.ptr + tile_base * ES;
+#pragma unroll 4
+    for (uint32_t e = threadIdx.x; e < (uint32_t)tile_n; e += kBThreads) {
+        const uint32_t o = e >> 4, q = e & 15;
+        const uint32_t bb = s_bits[o];
+        const uint32_t r = s_excl[o] + __popc(bb & ((1u << q) - 1));  // matches before e in the tile
+        uint64_t val;
+        if ((bb >> q) & 1u) {
+            if (mode == SPLIT_DICT) {
+                bad |= r >= lim;
+                const uint32_t y = y0 + r;
+                const uint32_t c = (s_codes[y >> 4] >> (2 * (y & 15))) & 3u;  // select, not an indexed array
+                val = c == 0 ? top[0] : c == 1 ? top[1] : c == 2 ? top[2] : top[3];
+            } else {
+                val = ld_elem_sm<ES>(sm, r);
             }
         } else {
-#pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) {
-                v[j] = 0;
-                if ((bits >> j) & 1u) {
-                    v[j] = ld_elem_sm<ES>(sm, ly);
-                    ++ly;
-                } else if ((valid_mask >> j) & 1u) {
-                    v[j] = mode == SPLIT_NOT_CONST ? top[0] : ld_elem_sm<ES>(sm, ny32 + ln);
-                    ++ln;
-                }
-            }
+            val = mode == SPLIT_NOT_CONST ? top[0] : ld_elem_sm<ES>(sm, ny32 + (e - r));
         }
-        store_run<ES, kBVPT>(out.ptr, base, n, v);
+        st_elem<ES>(dst, e, val);
     }
     __syncthreads();  // the next tile restages the shared buffers
     }
