@@ -1150,7 +1150,7 @@ constexpr bool stage_persistent(int op)
 // the others are persistent: an occupancy-sized grid strides over the tiles, skipping from a tile
 // past its item's real extent straight to its first tile of the next item.
 template <int OP>
-__global__ void __launch_bounds__(kBThreads, 3)
+__global__ void __launch_bounds__(kBThreads, 4)
 k_bstage(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status,
          uint32_t total_tiles)
 {
