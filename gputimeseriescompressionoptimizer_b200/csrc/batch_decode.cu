@@ -790,7 +790,7 @@ constexpr bool dec_persistent(int op)
 // One launch of a decode pass over every item: look-back passes one tile per block in claim order,
 // the others persistent over the tiles (see k_bstage).
 template <int OP>
-__global__ void __launch_bounds__(kBThreads, 4)
+__global__ void __launch_bounds__(kBThreads, 5)
 k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status,
        uint32_t total_tiles)
 {

@@ -1149,8 +1149,11 @@ constexpr bool stage_persistent(int op)
 // One launch of a pass over every item.  Look-back passes take one tile per block in claim order;
 // the others are persistent: an occupancy-sized grid strides over the tiles, skipping from a tile
 // past its item's real extent straight to its first tile of the next item.
+// resident blocks per SM the compiler keeps registers for (measured per pass on the mixed workload)
+constexpr int stage_min_blocks(int op) { return op == B_SPLIT || op == B_GFC_COMPRESS || op == B_TOPK ? 4 : 5; }
+
 template <int OP>
-__global__ void __launch_bounds__(kBThreads, 4)
+__global__ void __launch_bounds__(kBThreads, stage_min_blocks(OP))
 k_bstage(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *counter, uint32_t *status,
          uint32_t total_tiles)
 {
