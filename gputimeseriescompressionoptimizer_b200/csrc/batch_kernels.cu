@@ -305,8 +305,11 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         if (threadIdx.x == 0) s_ones = 0;
         __syncthreads();
         const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
+        // the next element's load is in flight while this one is inserted
+        unsigned long long next = t0 + threadIdx.x < end ? view_elem<ES>(it, vc, in.ptr, t0 + threadIdx.x) : 0ull;
         for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
-            const unsigned long long key = view_elem<ES>(it, vc, in.ptr, i);
+            const unsigned long long key = next;
+            if (i + kBThreads < end) next = view_elem<ES>(it, vc, in.ptr, i + kBThreads);
             if (is_nan_bits(key, o)) {
                 unsigned long long k = order_key(key, ES, o);
 #pragma unroll
