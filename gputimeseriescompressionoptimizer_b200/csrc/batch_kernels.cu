@@ -501,6 +501,8 @@ __device__ void p_topk(const BItem &it, uint32_t tile, StreamDesc *S, unsigned c
 }
 
 // ------------------------------------------------------------------------------- split
+__device__ __forceinline__ uint32_t spad(uint32_t x) { return x + (x >> 4); }
+
 template <int ES>
 __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, unsigned char *sm)
 {
@@ -584,15 +586,18 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     const uint64_t tile_n = tile_base < n ? (n - tile_base < kBTile ? n - tile_base : kBTile) : 0;
     const uint64_t ny = total, nn = tile_n - ny;
     const uint64_t yes0 = s_prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
-    uint64_t ly = excl, ln = (uint64_t)threadIdx.x * kBVPT - excl;
+    // staged at spad(position): one spare slot per 16, so the runs of consecutive threads (16 apart
+    // when most values match) fall into different banks
+    uint32_t ly = (uint32_t)excl, ln = threadIdx.x * kBVPT - (uint32_t)excl;
+    const uint32_t ny32 = (uint32_t)ny;
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) {
         if (!((valid_mask >> j) & 1u)) break;
         if ((yes_bits >> j) & 1u) {
-            if (mode != SPLIT_DICT) st_elem<ES>(sm, ly, v[j]);
+            if (mode != SPLIT_DICT) st_elem<ES>(sm, spad(ly), v[j]);
             ++ly;
         } else {
-            st_elem<ES>(sm, ny + ln, v[j]);
+            st_elem<ES>(sm, spad(ny32 + ln), v[j]);
             ++ln;
         }
     }
@@ -621,12 +626,14 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     }
     __syncthreads();
     if (mode != SPLIT_DICT) {
-        uint8_t *yes = S[it.out[1]].ptr;
-        for (uint64_t i = threadIdx.x; i < ny; i += kBThreads) st_elem<ES>(yes, yes0 + i, ld_elem_sm<ES>(sm, i));
+        uint8_t *yes = S[it.out[1]].ptr + yes0 * ES;
+        for (uint32_t i = threadIdx.x; i < ny32; i += kBThreads) st_elem<ES>(yes, i, ld_elem_sm<ES>(sm, spad(i)));
     }
     if (mode != SPLIT_NOT_CONST) {
-        uint8_t *no = S[it.out[2]].ptr;
-        for (uint64_t i = threadIdx.x; i < nn; i += kBThreads) st_elem<ES>(no, no0 + i, ld_elem_sm<ES>(sm, ny + i));
+        uint8_t *no = S[it.out[2]].ptr + no0 * ES;
+        const uint32_t nn32 = (uint32_t)nn;
+        for (uint32_t i = threadIdx.x; i < nn32; i += kBThreads)
+            st_elem<ES>(no, i, ld_elem_sm<ES>(sm, spad(ny32 + i)));
     }
     const uint64_t yes_pos = yes0 + ny;
     if (base < n && base + kBVPT >= n) {  // the thread holding the last element: lengths and headers
@@ -1102,7 +1109,7 @@ constexpr size_t stage_smem(int op)
     return op == B_AFL_PACK ? 8 * (kBTile + kBTile / 16 + 8)
          : op == B_HIST     ? 8 * kBHistPacked + 8 * 4 * (kBThreads / 32)
          : op == B_TOPK     ? sizeof(Cand) * kBThreads * 4
-         : op == B_SPLIT    ? 8 * kBTile
+         : op == B_SPLIT    ? 8 * (kBTile + kBTile / 16)
                             : 16;
 }
 
