@@ -649,8 +649,10 @@ __device__ void p_gfc_sizes(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     }
 }
 
+constexpr uint32_t kGfcDecWin = 512 + 16;  // bytes of a warp's GFC decode window
+
 template <bool DBL>
-__device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+__device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, uint8_t *sm)
 {
     const StreamDesc meta = S[it.in[0]], payload = S[it.in[2]];
     StreamDesc &out = S[it.out[0]];
@@ -678,13 +680,29 @@ __device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
     }
     const uint64_t cb = d_gfc_begin(g, w), ce = d_gfc_cut(g, w);
     uint64_t pos = end - size, last = 0;
-    const uint8_t *pl = payload.ptr;
+    // the chunk is read through a 512-byte window of this warp's shared memory, refilled with one
+    // coalesced load whenever less than a largest subchunk (16 + 32 * 8 bytes) is left in it
+    uint32_t *win = (uint32_t *)(sm + (threadIdx.x >> 5) * kGfcDecWin);
+    const uintptr_t mis = (uintptr_t)payload.ptr & 3;
+    const StreamReader rd{(const uint32_t *)(payload.ptr - mis), payload.len + mis};
+    uint64_t wbase = ~0ull;  // stream byte (counting from the aligned base) held by win[0]
     for (uint64_t s = cb; s < ce; s += 32) {
         if (pos + 16 > end) {
             if (lane == 0) set_status(status, GTSC_ERR_FORMAT);
             return;
         }
-        const uint32_t nib = ((uint32_t)pl[pos + (lane >> 1)] >> (4 * (lane & 1))) & 15u;
+        const uint64_t p0 = pos + mis;
+        if (wbase == ~0ull || p0 + 272 > wbase + 512) {
+            __syncwarp();
+            const uint64_t w0 = p0 >> 2;
+#pragma unroll
+            for (int k = 0; k < 4; k++) win[k * 32 + lane] = rd.word(w0 + k * 32 + lane);
+            wbase = w0 << 2;
+            __syncwarp();
+        }
+        const uint32_t off = (uint32_t)(p0 - wbase);  // below 512 - 272
+        const uint32_t hb = off + (lane >> 1);
+        const uint32_t nib = (win[hb >> 2] >> (8 * (hb & 3) + 4 * (lane & 1))) & 15u;
         const uint32_t code = nib & 7u;
         uint32_t mb = DBL ? (code >= 2 ? code + 1 : code) : code;
         if (!DBL && mb > 4) {
@@ -702,9 +720,12 @@ __device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
             if (lane == 0) set_status(status, GTSC_ERR_FORMAT);
             return;
         }
-        const uint8_t *src = pl + pos + 16 + (inc - mb);
-        uint64_t diff = 0;
-        for (int b = (int)mb - 1; b >= 0; b--) diff = (diff << 8) | src[b];
+        // the lane's mb little-endian bytes from three window words (the window has 4 words of slack
+        // past its 512 bytes; bytes past mb are masked off)
+        const uint32_t q = off + 16 + (inc - mb), sh = 8 * (q & 3);
+        const uint32_t w0 = win[q >> 2], w1 = win[(q >> 2) + 1], w2 = win[(q >> 2) + 2];
+        uint64_t diff = ((uint64_t)__funnelshift_r(w1, w2, sh) << 32) | __funnelshift_r(w0, w1, sh);
+        diff = mb ? diff & (~0ull >> (64 - 8 * mb)) : 0ull;
         if (nib & 8u) diff = 0ull - diff;
         uint64_t x = last + diff;
         if (!DBL) x &= 0xffffffffull;
@@ -795,7 +816,7 @@ k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *cou
        uint32_t total_tiles)
 {
     constexpr bool DYN = OP == B_DELTA_DEC || OP == B_RLE_SCAN;
-    __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : 16];
+    __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : OP == B_GFC_DEC ? kGfcDecWin * (kBThreads / 32) : 16];
     if (*(volatile uint32_t *)(status + 1)) return;
     if constexpr (!dec_persistent(OP)) {
         uint32_t tile;
@@ -849,8 +870,8 @@ __device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDe
     else if constexpr (OP == B_F2I_DEC) { GTSC_ES_SWITCH(p_f2i_dec<E>(it, tile, S, status)) }
     else if constexpr (OP == B_GFC_SIZES) p_gfc_sizes(it, tile, S, status);
     else if constexpr (OP == B_GFC_DEC) {
-        if (it.es == 8) p_gfc_dec<true>(it, tile, S, status);
-        else p_gfc_dec<false>(it, tile, S, status);
+        if (it.es == 8) p_gfc_dec<true>(it, tile, S, status, smem);
+        else p_gfc_dec<false>(it, tile, S, status, smem);
     }
 #undef GTSC_ES_SWITCH
 }
