@@ -649,7 +649,20 @@ __device__ void p_gfc_sizes(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     }
 }
 
-constexpr uint32_t kGfcDecWin = 512 + 16;  // bytes of a warp's GFC decode window
+// A warp's GFC decode reads its chunk through a ring of four 512-byte segments in shared memory,
+// filled by cp.async (16 bytes a lane) up to three segments ahead of the subchunk being parsed.
+constexpr uint32_t kGfcSeg = 512, kGfcRing = 4 * kGfcSeg;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t n)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 template <bool DBL>
 __device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, uint8_t *sm)
@@ -680,29 +693,44 @@ __device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
     }
     const uint64_t cb = d_gfc_begin(g, w), ce = d_gfc_cut(g, w);
     uint64_t pos = end - size, last = 0;
-    // the chunk is read through a 512-byte window of this warp's shared memory, refilled with one
-    // coalesced load whenever less than a largest subchunk (16 + 32 * 8 bytes) is left in it
-    uint32_t *win = (uint32_t *)(sm + (threadIdx.x >> 5) * kGfcDecWin);
-    const uintptr_t mis = (uintptr_t)payload.ptr & 3;
-    const StreamReader rd{(const uint32_t *)(payload.ptr - mis), payload.len + mis};
-    uint64_t wbase = ~0ull;  // stream byte (counting from the aligned base) held by win[0]
+    const uint32_t mis = (uint32_t)((uintptr_t)payload.ptr & 15);
+    const uint8_t *base = payload.ptr - mis;  // 16-byte aligned; stream bytes count from here
+    const uint64_t nbytes = payload.len + mis, seg0 = (pos + mis) & ~15ull, lim = end + mis;
+    uint32_t *ring = (uint32_t *)(sm + (threadIdx.x >> 5) * kGfcRing);
+    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
+    uint32_t issued = 0;  // segments requested (one commit group each, empty past the chunk)
+    auto issue = [&]() {
+        const uint64_t sb = seg0 + (uint64_t)issued * kGfcSeg;
+        if (sb < lim) {
+            const uint64_t b = sb + 16 * lane;
+            const uint32_t n = b >= nbytes ? 0u : (uint32_t)min((uint64_t)16, nbytes - b);
+            cp_async16(ring_s + (issued & 3) * kGfcSeg + 16 * lane, n ? base + b : base, n);
+        }
+        cp_async_commit();
+        issued++;
+    };
+    issue();
+    issue();
+    issue();
     for (uint64_t s = cb; s < ce; s += 32) {
         if (pos + 16 > end) {
             if (lane == 0) set_status(status, GTSC_ERR_FORMAT);
+            cp_async_wait<0>();
             return;
         }
-        const uint64_t p0 = pos + mis;
-        if (wbase == ~0ull || p0 + 272 > wbase + 512) {
-            __syncwarp();
-            const uint64_t w0 = p0 >> 2;
-#pragma unroll
-            for (int k = 0; k < 4; k++) win[k * 32 + lane] = rd.word(w0 + k * 32 + lane);
-            wbase = w0 << 2;
-            __syncwarp();
-        }
-        const uint32_t off = (uint32_t)(p0 - wbase);  // below 512 - 272
-        const uint32_t hb = off + (lane >> 1);
-        const uint32_t nib = (win[hb >> 2] >> (8 * (hb & 3) + 4 * (lane & 1))) & 15u;
+        // a subchunk reads ring bytes [rel, rel + 284): its 16-byte header, at most 32 x 8 payload
+        // bytes and the two words after the last one
+        const uint32_t rel = (uint32_t)(pos + mis - seg0), kcur = rel / kGfcSeg, kneed = (rel + 283) / kGfcSeg;
+        __syncwarp();  // the segments before kcur are no longer read: their slots can be refilled
+        while (issued < kcur + 4) issue();
+        const uint32_t pend = issued - 1 - kneed;  // groups newer than the last one needed
+        if (pend >= 3) cp_async_wait<3>();
+        else if (pend == 2) cp_async_wait<2>();
+        else if (pend == 1) cp_async_wait<1>();
+        else cp_async_wait<0>();
+        __syncwarp();
+        const uint32_t hb = rel + (lane >> 1);
+        const uint32_t nib = (ring[(hb >> 2) & 511] >> (8 * (hb & 3) + 4 * (lane & 1))) & 15u;
         const uint32_t code = nib & 7u;
         uint32_t mb = DBL ? (code >= 2 ? code + 1 : code) : code;
         if (!DBL && mb > 4) {
@@ -718,12 +746,12 @@ __device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
         const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
         if (pos + 16 + total > end) {
             if (lane == 0) set_status(status, GTSC_ERR_FORMAT);
+            cp_async_wait<0>();
             return;
         }
-        // the lane's mb little-endian bytes from three window words (the window has 4 words of slack
-        // past its 512 bytes; bytes past mb are masked off)
-        const uint32_t q = off + 16 + (inc - mb), sh = 8 * (q & 3);
-        const uint32_t w0 = win[q >> 2], w1 = win[(q >> 2) + 1], w2 = win[(q >> 2) + 2];
+        // the lane's mb little-endian bytes from three ring words (bytes past mb are masked off)
+        const uint32_t q = rel + 16 + (inc - mb), sh = 8 * (q & 3), qw = q >> 2;
+        const uint32_t w0 = ring[qw & 511], w1 = ring[(qw + 1) & 511], w2 = ring[(qw + 2) & 511];
         uint64_t diff = ((uint64_t)__funnelshift_r(w1, w2, sh) << 32) | __funnelshift_r(w0, w1, sh);
         diff = mb ? diff & (~0ull >> (64 - 8 * mb)) : 0ull;
         if (nib & 8u) diff = 0ull - diff;
@@ -733,6 +761,7 @@ __device__ void p_gfc_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
         pos += 16 + total;
         if (s == cb) last = __shfl_sync(0xffffffffu, x, 31);
     }
+    cp_async_wait<0>();
     if (lane == 0 && pos != end) set_status(status, GTSC_ERR_FORMAT);
 }
 
@@ -816,7 +845,7 @@ k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *cou
        uint32_t total_tiles)
 {
     constexpr bool DYN = OP == B_DELTA_DEC || OP == B_RLE_SCAN;
-    __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : OP == B_GFC_DEC ? kGfcDecWin * (kBThreads / 32) : 16];
+    __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : OP == B_GFC_DEC ? kGfcRing * (kBThreads / 32) : 16];
     if (*(volatile uint32_t *)(status + 1)) return;
     if constexpr (!dec_persistent(OP)) {
         uint32_t tile;
