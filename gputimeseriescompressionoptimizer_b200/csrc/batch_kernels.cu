@@ -897,8 +897,27 @@ __device__ void p_f2i_raw(const BItem &it, uint32_t tile, StreamDesc *S)
 
 // ------------------------------------------------------------------------------- GFC
 // node scratch of GFC: p[0] look-back, p[1] chunk sizes (int32), p[2] inclusive ends (u64), p[3] layout
+
+// A double chunk is built in a 1 KB ring of the warp's shared memory and stored in 512-byte blocks,
+// 16 bytes a lane (its payload bytes, up to 8 a lane, would otherwise be that many partial global
+// stores); a float chunk, at most 4 bytes a lane, is stored directly.  Positions count bytes from
+// the 16-byte aligned address at or below the chunk's start; only the bytes in [lo, hi) are stored.
+constexpr uint32_t kGfcStage = 1024;
+
+__device__ __forceinline__ void gfc_flush(uint8_t *al, const uint8_t *ring, uint32_t b, uint32_t lo, uint32_t hi,
+                                          int lane)
+{
+    const uint32_t p = b + 16 * (uint32_t)lane;
+    if (p >= lo && p + 16 <= hi) {
+        *(uint4 *)(al + p) = *(const uint4 *)(ring + (p & (kGfcStage - 1)));
+    } else {
+        for (uint32_t k = 0; k < 16; k++)
+            if (p + k >= lo && p + k < hi) al[p + k] = ring[(p + k) & (kGfcStage - 1)];
+    }
+}
+
 template <bool DBL>
-__device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S)
+__device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S, uint8_t *sm)
 {
     const StreamDesc in = S[it.in[0]];
     const ViewCtx vc = view_ctx<DBL ? 8 : 4>(it, in);
@@ -926,7 +945,11 @@ __device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S)
     int32_t *ends = (int32_t *)S[it.out[1]].ptr;
     const uint64_t cb = d_gfc_begin(g, w), ce = d_gfc_cut(g, w);
     const uint64_t start = d_gfc_start(g, w);
-    uint64_t off = start, last = 0;
+    uint64_t last = 0;
+    uint8_t *ring = sm + (threadIdx.x >> 5) * kGfcStage;
+    const uint32_t mis = (uint32_t)((uintptr_t)(layout + start) & 15);
+    uint8_t *al = layout + start - mis;
+    uint32_t fr = mis, flushed = 0;  // positions: the next subchunk's header, the bytes stored
     // values of the next 4 subchunks are in flight while one is encoded
     uint64_t xb[4];
 #pragma unroll
@@ -970,15 +993,29 @@ __device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S)
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
         const uint32_t prev_nib = __shfl_up_sync(0xffffffffu, nib, 1);
-        if (lane & 1) layout[off + (lane >> 1)] = (uint8_t)(prev_nib | (nib << 4));
-        uint8_t *dst = layout + off + 16 + (incl - mb);
-        for (uint32_t b = 0; b < mb; b++) dst[b] = (uint8_t)(diff >> (8 * b));
-        off += 16 + total;
+        const uint32_t pl = fr + 16 + (incl - mb);
+        if constexpr (DBL) {
+            if (lane & 1) ring[(fr + (lane >> 1)) & (kGfcStage - 1)] = (uint8_t)(prev_nib | (nib << 4));
+            for (uint32_t b = 0; b < mb; b++) ring[(pl + b) & (kGfcStage - 1)] = (uint8_t)(diff >> (8 * b));
+        } else {
+            if (lane & 1) al[fr + (lane >> 1)] = (uint8_t)(prev_nib | (nib << 4));
+            for (uint32_t b = 0; b < mb; b++) al[pl + b] = (uint8_t)(diff >> (8 * b));
+        }
+        fr += 16 + total;  // at most 272 bytes a subchunk: the ring holds [flushed, fr) below 784 bytes
         if (s == cb) last = __shfl_sync(0xffffffffu, x, 31);
+        if constexpr (DBL) {
+            __syncwarp();
+            if (fr - flushed >= 512) {
+                gfc_flush(al, ring, flushed, mis, 0xffffffffu, lane);
+                flushed += 512;
+                __syncwarp();
+            }
+        }
     }
+    if (DBL && flushed < fr) gfc_flush(al, ring, flushed, mis, fr, lane);
     if (lane == 31) {
-        ends[w] = (int32_t)off;
-        sizes[w] = (int32_t)(off - start);
+        ends[w] = (int32_t)(start + fr - mis);
+        sizes[w] = (int32_t)(fr - mis);
     }
 }
 
@@ -1032,7 +1069,9 @@ __device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool d
 }
 
 // one warp copies n bytes between any addresses: head bytes up to a 4-byte aligned destination,
-// then whole words funnel-shifted out of aligned source words, then the tail
+// then whole words funnel-shifted out of aligned source words, then the tail.  The source is read
+// through the read-only path (it was written by an earlier launch), so the unrolled loads are all
+// in flight together.
 __device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint64_t n, int lane)
 {
     const uint64_t head = (4 - ((uintptr_t)dst & 3)) & 3;
@@ -1046,10 +1085,10 @@ __device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint
     const uint32_t *sw = (const uint32_t *)((uintptr_t)sp & ~(uintptr_t)3);
     if (sh == 0) {
 #pragma unroll 4
-        for (uint64_t k = lane; k < words; k += 32) d[k] = sw[k];
+        for (uint64_t k = lane; k < words; k += 32) d[k] = __ldg(sw + k);
     } else {
 #pragma unroll 4
-        for (uint64_t k = lane; k < words; k += 32) d[k] = __funnelshift_r(sw[k], sw[k + 1], sh);
+        for (uint64_t k = lane; k < words; k += 32) d[k] = __funnelshift_r(__ldg(sw + k), __ldg(sw + k + 1), sh);
     }
     const uint64_t tail = (n - h) - 4 * words;
     if ((uint64_t)lane < tail) ((uint8_t *)d)[4 * words + lane] = sp[4 * words + lane];
@@ -1110,6 +1149,7 @@ constexpr size_t stage_smem(int op)
          : op == B_HIST     ? 8 * kBHistPacked + 8 * 4 * (kBThreads / 32)
          : op == B_TOPK     ? sizeof(Cand) * kBThreads * 4
          : op == B_SPLIT    ? 8 * (kBTile + kBTile / 16)
+         : op == B_GFC_COMPRESS ? kGfcStage * (kBThreads / 32)
                             : 16;
 }
 
@@ -1224,8 +1264,8 @@ __device__ __forceinline__ void run_stage(const BItem &it, uint32_t tile, Stream
     else if constexpr (OP == B_F2I_ENC) { GTSC_ES_SWITCH(p_f2i_enc<E>(it, tile, S)) }
     else if constexpr (OP == B_F2I_RAW) { GTSC_ES_SWITCH(p_f2i_raw<E>(it, tile, S)) }
     else if constexpr (OP == B_GFC_COMPRESS) {
-        if (it.es == 8) p_gfc_compress<true>(it, tile, S);
-        else p_gfc_compress<false>(it, tile, S);
+        if (it.es == 8) p_gfc_compress<true>(it, tile, S, smem);
+        else p_gfc_compress<false>(it, tile, S, smem);
     } else if constexpr (OP == B_GFC_SCAN) {
         p_gfc_scan(it, tile, S, it.es == 8, it.mode != 0);
     } else if constexpr (OP == B_GFC_COMPACT) {
