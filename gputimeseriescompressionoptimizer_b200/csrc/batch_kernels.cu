@@ -27,15 +27,50 @@ __device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
     const uint64_t end = n < t0 + kBMinMaxTile ? n : t0 + kBMinMaxTile;
     const Order o = (Order)it.order;
     uint64_t kmin = ~0ull, kmax = 0;
-    for (uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT; base < end; base += (uint64_t)kBThreads * kBVPT) {
-        uint64_t v[kBVPT];
-        load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+    if constexpr (ES <= 4) {
+        // 32-bit keys of the same order (sign bit flipped for integers, order_key's map for floats),
+        // turned into the accumulator's 64-bit keys once per thread
+        const bool f32 = o == ORD_F32;
+        constexpr uint32_t SH = 32 - 8 * ES;
+        uint32_t k32min = ~0u, k32max = 0;
+        bool seen = false;
+        auto key32 = [&](uint32_t u) {
+            if (f32) return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+            return (uint32_t)((int32_t)(u << SH) >> SH) ^ 0x80000000u;
+        };
+        for (uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT; base < end; base += (uint64_t)kBThreads * kBVPT) {
+            uint64_t v[kBVPT];
+            load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+            const uint32_t cnt = end - base < kBVPT ? (uint32_t)(end - base) : kBVPT;
 #pragma unroll
-        for (int j = 0; j < (int)kBVPT; j++) {
-            if (base + j >= end || is_nan_bits(v[j], o)) continue;
-            const uint64_t k = order_key(v[j], ES, o);
-            kmin = k < kmin ? k : kmin;
-            kmax = k > kmax ? k : kmax;
+            for (int j = 0; j < (int)kBVPT; j++) {
+                const uint32_t u = (uint32_t)v[j];
+                const bool ok = (uint32_t)j < cnt && !(f32 && (u & 0x7fffffffu) > 0x7f800000u);
+                const uint32_t k = key32(u);
+                k32min = ok && k < k32min ? k : k32min;
+                k32max = ok && k > k32max ? k : k32max;
+                seen |= ok;
+            }
+        }
+        if (seen) {
+            const uint32_t umin = f32 ? ((k32min & 0x80000000u) ? (k32min ^ 0x80000000u) : ~k32min)
+                                      : (k32min ^ 0x80000000u);
+            const uint32_t umax = f32 ? ((k32max & 0x80000000u) ? (k32max ^ 0x80000000u) : ~k32max)
+                                      : (k32max ^ 0x80000000u);
+            kmin = order_key(umin, 4, o);  // umin / umax are sign-extended to 32 bits
+            kmax = order_key(umax, 4, o);
+        }
+    } else {
+        for (uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT; base < end; base += (uint64_t)kBThreads * kBVPT) {
+            uint64_t v[kBVPT];
+            load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+#pragma unroll
+            for (int j = 0; j < (int)kBVPT; j++) {
+                if (base + j >= end || is_nan_bits(v[j], o)) continue;
+                const uint64_t k = order_key(v[j], ES, o);
+                kmin = k < kmin ? k : kmin;
+                kmax = k > kmax ? k : kmax;
+            }
         }
     }
     block_minmax(kmin, kmax);
@@ -159,6 +194,55 @@ __device__ void p_afl_pack(const BItem &it, uint32_t tile, StreamDesc *S, unsign
     const uint64_t t0 = (uint64_t)tile * kBTile;
     if (t0 >= n) return;
     uint8_t *out = S[it.out[1]].ptr;
+    if constexpr (ES <= 4) {
+        // b <= 32.  Thread t packs its 16 values (tile bits [16 b t, 16 b (t + 1))) into a register
+        // and stores whole words to the tile's words in shared memory; the word it shares with the
+        // thread before it (a start inside a word) and the one it shares with the thread after it
+        // (an end inside a word) are or-ed in.  Word w sits at w + w / 32, so that threads storing
+        // b / 2 words apart spread over the banks.  A tile's output starts on a word: 4096 b / 32.
+        uint32_t *ow = (uint32_t *)sv;
+        auto slot = [](uint32_t w) { return w + (w >> 5); };
+        const uint32_t vmask32 = b >= 32 ? ~0u : ((1u << b) - 1);
+        uint64_t v[kBVPT];
+        const uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT;
+        load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+        const uint32_t bit0 = threadIdx.x * kBVPT * (uint32_t)b;
+        if (bit0 & 31) ow[slot(bit0 >> 5)] = 0;
+        __syncthreads();
+        uint32_t wi = bit0 >> 5, fill = bit0 & 31;
+        bool shared_first = fill != 0;
+        uint64_t acc = 0;
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++) {
+            const uint32_t u = base + j < n ? ((uint32_t)v[j] & vmask32) : 0u;
+            acc |= (uint64_t)u << fill;
+            fill += (uint32_t)b;
+            if (fill >= 32) {
+                if (shared_first) atomicOr(&ow[slot(wi)], (uint32_t)acc);
+                else ow[slot(wi)] = (uint32_t)acc;
+                shared_first = false;
+                ++wi;
+                acc >>= 32;
+                fill -= 32;
+            }
+        }
+        if (fill) atomicOr(&ow[slot(wi)], (uint32_t)acc);
+        __syncthreads();
+        const uint64_t total_words = (out_bytes + 3) / 4;
+        const uint64_t w0 = t0 * (uint64_t)b / 32;
+        uint64_t w_end = w0 + 128u * (uint32_t)b;
+        if (w_end > total_words) w_end = total_words;
+        for (uint64_t w = w0 + threadIdx.x; w < w_end; w += kBThreads) {
+            const uint32_t word = ow[slot((uint32_t)(w - w0))];
+            if (4 * w + 4 <= out_bytes) {
+                reinterpret_cast<uint32_t *>(out)[w] = word;
+            } else {
+                for (int k = 0; k < 4; k++)
+                    if (4 * w + k < out_bytes) out[4 * w + k] = (uint8_t)(word >> (8 * k));
+            }
+        }
+        return;
+    }
     const uint64_t vmask = b >= 64 ? ~0ull : ((1ull << b) - 1);
     const uint64_t cnt = n - t0 < kBTile ? n - t0 : kBTile;
     // the tile's values in shared memory, skewed by one slot per 16 values (afl_slot) so that a
