@@ -38,15 +38,27 @@ __device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
             if (f32) return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
             return (uint32_t)((int32_t)(u << SH) >> SH) ^ 0x80000000u;
         };
-        for (uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT; base < end; base += (uint64_t)kBThreads * kBVPT) {
+        // the tile's two runs of 16 values a thread are both loaded before either is reduced
+        static_assert(kBMinMaxTile == 2 * kBThreads * kBVPT, "a min/max tile is two runs a thread");
+        const uint64_t b0 = t0 + (uint64_t)threadIdx.x * kBVPT, b1 = b0 + (uint64_t)kBThreads * kBVPT;
+        uint32_t u[2][kBVPT];
+        {
             uint64_t v[kBVPT];
-            load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
-            const uint32_t cnt = end - base < kBVPT ? (uint32_t)(end - base) : kBVPT;
+            load_view<ES, kBVPT>(it, vc, in.ptr, b0, v);
+#pragma unroll
+            for (int j = 0; j < (int)kBVPT; j++) u[0][j] = (uint32_t)v[j];
+            if (b1 < end) load_view<ES, kBVPT>(it, vc, in.ptr, b1, v);
+#pragma unroll
+            for (int j = 0; j < (int)kBVPT; j++) u[1][j] = (uint32_t)v[j];
+        }
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const uint64_t base = r ? b1 : b0;
+            const uint32_t cnt = base >= end ? 0u : end - base < kBVPT ? (uint32_t)(end - base) : kBVPT;
 #pragma unroll
             for (int j = 0; j < (int)kBVPT; j++) {
-                const uint32_t u = (uint32_t)v[j];
-                const bool ok = (uint32_t)j < cnt && !(f32 && (u & 0x7fffffffu) > 0x7f800000u);
-                const uint32_t k = key32(u);
+                const bool ok = (uint32_t)j < cnt && !(f32 && (u[r][j] & 0x7fffffffu) > 0x7f800000u);
+                const uint32_t k = key32(u[r][j]);
                 k32min = ok && k < k32min ? k : k32min;
                 k32max = ok && k > k32max ? k : k32max;
                 seen |= ok;
