@@ -27,8 +27,10 @@ LIB_PATH = os.path.join(HERE, "libgtsc.so")
 CHAR, SHORT, INT, TIME, FLOAT, DOUBLE = range(6)
 # EncodingType codes (compression/encoding_type.hpp:17-30)
 DELTA, AFL, SCALE, RLE, DICT, UNIQUE, PATCH, NONE, FLOAT_TO_INT, CONST, GFC = range(11)
+# the outside variant of the patch encoding (PatchType::outside); serialised as PATCH
+PATCH_OUTSIDE = 11
 ENCODING_NAMES = ["delta", "afl", "scale", "rle", "dict", "unique", "patch", "none", "floatToInt",
-                  "constData", "gfc"]
+                  "constData", "gfc", "patch(outside)"]
 NP_TYPES = {CHAR: np.int8, SHORT: np.int16, INT: np.int32, TIME: np.int64, FLOAT: np.float32,
             DOUBLE: np.float64}
 

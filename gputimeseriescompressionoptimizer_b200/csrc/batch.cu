@@ -82,7 +82,7 @@ int view_ops(const int8_t *vop)
 bool view_consumer(int enc)
 {
     return enc == GTSC_AFL || enc == GTSC_GFC || enc == GTSC_DICT || enc == GTSC_CONST || enc == GTSC_PATCH ||
-           enc == GTSC_RLE || enc == GTSC_DELTA || enc == GTSC_SCALE;
+           enc == GTSC_PATCH_OUTSIDE || enc == GTSC_RLE || enc == GTSC_DELTA || enc == GTSC_SCALE;
 }
 
 struct Launch {
@@ -192,7 +192,7 @@ void BatchEngine::build_node(const Tree &t, int &k, int col, int parent, int in_
     case GTSC_RLE: cap[0] = 4; cap[1] = 4 * n; cap[2] = in_cap; break;
     case GTSC_DICT: cap[0] = 2 + cdiv(n, 8); cap[1] = 20 + 4 * es + 4 * cdiv(n, 16); cap[2] = in_cap; break;
     case GTSC_CONST: cap[0] = es + 2 + cdiv(n, 8); cap[1] = in_cap; break;
-    case GTSC_PATCH: cap[0] = 2 + cdiv(n, 8); cap[1] = in_cap; cap[2] = in_cap; break;
+    case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: cap[0] = 2 + cdiv(n, 8); cap[1] = in_cap; cap[2] = in_cap; break;
     case GTSC_FLOAT_TO_INT: cap[0] = 4; cap[1] = std::max<uint64_t>(4 * n, in_cap); break;
     case GTSC_GFC:
         if (is_fp(me.dt)) {
@@ -240,7 +240,7 @@ void BatchEngine::plan_passes()
         const uint64_t n = nd.in_cap / nd.es;
         uint64_t c = 64;
         switch (nd.enc) {
-        case GTSC_PATCH:
+        case GTSC_PATCH: case GTSC_PATCH_OUTSIDE:
             nd.split_tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
             c = 64 + align_up(lookback_bytes(nd.split_tiles), 256);
             break;
@@ -278,7 +278,7 @@ void BatchEngine::plan_passes()
         uint64_t d = 0;
         const uint64_t tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
         switch (nd.enc) {
-        case GTSC_DELTA: case GTSC_PATCH: case GTSC_DICT: case GTSC_CONST:
+        case GTSC_DELTA: case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: case GTSC_DICT: case GTSC_CONST:
             nd.dlb_off = nd.c_bytes;
             d = align_up(lookback_bytes(tiles), 256);
             break;
@@ -359,7 +359,7 @@ void BatchEngine::plan_passes()
             add(pk);
             break;
         }
-        case GTSC_PATCH: {
+        case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: {
             BItem mm = base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile));
             mm.order = (int16_t)native_order(nd.dt);
             add(mm);
@@ -367,6 +367,7 @@ void BatchEngine::plan_passes()
             sp.order = (int16_t)native_order(nd.dt);
             sp.mode = SPLIT_LOWER;
             sp.p[0] = 64;
+            sp.p[1] = nd.enc == GTSC_PATCH_OUTSIDE;  // the outside variant's stencil
             add(sp);
             break;
         }
@@ -459,6 +460,7 @@ void BatchEngine::plan_passes()
             const HNode &par = nodes[nd.parent];
             const int slot = (int)(std::find(par.kids.begin(), par.kids.end(), id) - par.kids.begin()) + 1;
             const bool consumer = par.enc == GTSC_DELTA || par.enc == GTSC_SCALE || par.enc == GTSC_PATCH ||
+                                  par.enc == GTSC_PATCH_OUTSIDE ||
                                   par.enc == GTSC_CONST || par.enc == GTSC_RLE || par.enc == GTSC_FLOAT_TO_INT ||
                                   (par.enc == GTSC_DICT && slot == 2);
             if (consumer && nd.enc == GTSC_AFL && nd.kids.size() == 1 && nodes[nd.kids[0]].enc == GTSC_NONE) {
@@ -512,9 +514,9 @@ void BatchEngine::plan_passes()
         case GTSC_AFL: ps.push_back(ditem(B_AFL_UNPACK, t2k)); break;
         case GTSC_DELTA: { BItem it = ditem(B_DELTA_DEC, t2k); it.p[0] = nd.dlb_off; ps.push_back(it); break; }
         case GTSC_SCALE: ps.push_back(ditem(B_SCALE_ADD, t2k)); break;
-        case GTSC_PATCH: case GTSC_DICT: case GTSC_CONST: {
+        case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: case GTSC_DICT: case GTSC_CONST: {
             BItem it = ditem(B_MERGE, cdiv(t2k, kBMergeSub));
-            it.mode = (int16_t)(nd.enc == GTSC_PATCH ? SPLIT_LOWER : nd.enc == GTSC_DICT ? SPLIT_DICT : SPLIT_NOT_CONST);
+            it.mode = (int16_t)(nd.enc == GTSC_PATCH || nd.enc == GTSC_PATCH_OUTSIDE ? SPLIT_LOWER : nd.enc == GTSC_DICT ? SPLIT_DICT : SPLIT_NOT_CONST);
             it.p[0] = nd.dlb_off;
             it.p[1] = t2k;
             // the stencil counts need only the node's metadata, parsed before the first level: one
@@ -669,7 +671,7 @@ void BatchEngine::layout(cudaStream_t s)
         const uint64_t n = nd.in_cap / nd.es;
         const uint64_t t2k = std::max<uint64_t>(1, cdiv(n, kBTile));
         switch (nd.enc) {
-        case GTSC_DELTA: case GTSC_PATCH: case GTSC_DICT: case GTSC_CONST: case GTSC_RLE:
+        case GTSC_DELTA: case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: case GTSC_DICT: case GTSC_CONST: case GTSC_RLE:
             zr(zero_d, sc + nd.dlb_off, lookback_zero_bytes(t2k));
             break;
         case GTSC_GFC:
@@ -687,8 +689,9 @@ void BatchEngine::layout(cudaStream_t s)
         for (size_t id = 0; id < nodes.size(); id++) {
             if (nodes[id].col != (int)c) continue;
             const HNode &nd = nodes[id];
-            BNodeDev a{nd.enc, nd.dt, nd.enc == GTSC_NONE ? -1 : nd.out_sid[0], nd.enc == GTSC_NONE ? nd.in_sid : -1, 0, 0};
-            BNodeDev b{nd.enc, nd.dt, nd.dec_meta_sid, nd.dec_data_sid, 0, 0};
+            const int henc = nd.enc == GTSC_PATCH_OUTSIDE ? GTSC_PATCH : nd.enc;  // the serialised type
+            BNodeDev a{henc, nd.dt, nd.enc == GTSC_NONE ? -1 : nd.out_sid[0], nd.enc == GTSC_NONE ? nd.in_sid : -1, 0, 0};
+            BNodeDev b{henc, nd.dt, nd.dec_meta_sid, nd.dec_data_sid, 0, 0};
             nodes_c.push_back(a);
             nodes_d.push_back(b);
             cnt++;

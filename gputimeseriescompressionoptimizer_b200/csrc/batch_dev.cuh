@@ -158,6 +158,20 @@ __device__ __forceinline__ uint64_t d_patch_threshold(uint64_t mnb, uint64_t mxb
     return d_cast_double_to_T(__dsub_rn(dmax, __dmul_rn(0.1, ddist)), dt, es);
 }
 
+// OutsidePatchEncoding::GetOperator<T> (outside_patch_encoding.cu:22-31), factor 0.1, x86 casts:
+// low = (T)(min + 0.1 * dist), high = (T)(max - 0.1 * dist) with T dist = max - min
+__device__ __forceinline__ void d_outside_patch_bounds(uint64_t mnb, uint64_t mxb, int dt, int es, uint64_t &lo,
+                                                       uint64_t &hi)
+{
+    const double dmin = d_T_to_double(mnb, dt, es), dmax = d_T_to_double(mxb, dt, es);
+    const uint64_t dist_bits = d_cast_double_to_T(__dsub_rn(dmax, dmin), dt, es);
+    const double ddist = (dt == GTSC_FLOAT || dt == GTSC_DOUBLE) ? d_T_to_double(dist_bits, dt, es)
+                                                                   : (double)sext(dist_bits, es);
+    const double prod = __dmul_rn(0.1, ddist);
+    lo = d_cast_double_to_T(__dadd_rn(dmin, prod), dt, es);
+    hi = d_cast_double_to_T(__dsub_rn(dmax, prod), dt, es);
+}
+
 // (int)(logf(10^k) / logf(10)) with CUDA's logf (cuda_array_statistics.cu:43)
 __device__ __forceinline__ int d_precision_of(int steps)
 {

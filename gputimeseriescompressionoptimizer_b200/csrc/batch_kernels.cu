@@ -613,11 +613,13 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     // stencil location and the values matched against
     uint8_t *meta = S[it.out[0]].ptr;
     uint8_t *stencil = mode == SPLIT_NOT_CONST ? meta + ES + 1 : meta + 1;
-    uint64_t top[4] = {0, 0, 0, 0}, thr = 0;
+    uint64_t top[4] = {0, 0, 0, 0}, thr = 0, lo = 0;
+    const bool outside = mode == SPLIT_LOWER && it.p[1] != 0;
     if (mode == SPLIT_LOWER) {
         uint64_t mnb = 0, mxb = 0;
         if (!acc_minmax((const MinMaxAcc *)it.scratch, ES, o, mnb, mxb) && n) mnb = mxb = view_elem<ES>(it, vc, in.ptr, 0);
-        thr = d_patch_threshold(mnb, mxb, it.dt, ES);
+        if (outside) d_outside_patch_bounds(mnb, mxb, it.dt, ES, lo, thr);  // thr: the high bound
+        else thr = d_patch_threshold(mnb, mxb, it.dt, ES);
     } else if (mode == SPLIT_NOT_CONST) {
         top[0] = ld_elem<ES>(meta, 0);
     } else {
@@ -639,7 +641,12 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     uint64_t v[kBVPT];
     load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
     uint32_t bits = 0, codes = 0;
-    if (mode == SPLIT_LOWER) {
+    if (mode == SPLIT_LOWER && outside) {
+        // OutsideOperator (stencil_operators.hpp:14-25): false when x > high or x < low
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++)
+            bits |= (uint32_t)!(lt_native(thr, v[j], ES, o) || lt_native(v[j], lo, ES, o)) << j;
+    } else if (mode == SPLIT_LOWER) {
 #pragma unroll
         for (int j = 0; j < (int)kBVPT; j++) bits |= (uint32_t)lt_native(v[j], thr, ES, o) << j;
     } else {

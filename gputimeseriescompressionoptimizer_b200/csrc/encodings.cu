@@ -575,7 +575,25 @@ uint64_t lower_patch_threshold(uint64_t mnb, uint64_t mxb, int dt)
     return cast_double_to_T(t, dt);
 }
 
-Parts patch_encode(int dt, View in, cudaStream_t s)
+// OutsidePatchEncoding::GetOperator<T> (compression/patch/outside_patch_encoding.cu:22-31), factor
+// 0.1: T dist = _max - _min; low = (T)(_min + 0.1 * dist), high = (T)(_max - 0.1 * dist)
+void outside_patch_bounds(uint64_t mnb, uint64_t mxb, int dt, uint64_t *lo, uint64_t *hi)
+{
+    volatile double dmin = T_to_double(mnb, dt), dmax = T_to_double(mxb, dt);
+    volatile double span = dmax - dmin;
+    const uint64_t dist_bits = cast_double_to_T(span, dt);
+    double ddist = is_fp(dt) ? T_to_double(dist_bits, dt) : (double)sext(dist_bits, dtype_size(dt));
+    volatile double prod = 0.1 * ddist;
+    volatile double l = dmin + prod, h = dmax - prod;
+    *lo = cast_double_to_T(l, dt);
+    *hi = cast_double_to_T(h, dt);
+}
+
+// LowerPatchEncoding::Encode (lower_patch_encoding.cu:33-67) and, with `outside`,
+// OutsidePatchEncoding::Encode (outside_patch_encoding.cu:33-60): the stencil is x < t, or the
+// OutsideOperator's low <= x <= high (stencil_operators.hpp:14-25; NaN counts as inside); meta = the
+// packed stencil, out1 = the stencil-true values, out2 = the rest, both in order
+Parts patch_encode(int dt, View in, cudaStream_t s, bool outside)
 {
     const int es = dtype_size(dt);
     const uint64_t n = in.bytes / es;
@@ -595,6 +613,8 @@ Parts patch_encode(int dt, View in, cudaStream_t s)
     SplitArgs a;
     a.order = native_order(dt);
     a.thr = thr;
+    a.outside = outside;
+    if (outside) outside_patch_bounds(mnb, mxb, dt, &a.lo, &a.hi);
     a.stencil = meta.get() + 1;
     a.yes = out1.get();
     a.no = out2.get();
@@ -856,7 +876,7 @@ int n_results(int enc)
     switch (enc) {
     case GTSC_DELTA: case GTSC_AFL: case GTSC_SCALE: case GTSC_UNIQUE: case GTSC_FLOAT_TO_INT: case GTSC_CONST:
         return 1;
-    case GTSC_RLE: case GTSC_DICT: case GTSC_PATCH: case GTSC_GFC: return 2;
+    case GTSC_RLE: case GTSC_DICT: case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: case GTSC_GFC: return 2;
     case GTSC_NONE: return 0;
     default: return -1;
     }
@@ -881,7 +901,8 @@ Parts encode(int enc, int dt, View in, cudaStream_t s)
     case GTSC_RLE: return rle_encode(dt, in, s);
     case GTSC_DICT: return dict_encode(dt, in, s);
     case GTSC_CONST: return const_encode(dt, in, s);
-    case GTSC_PATCH: return patch_encode(dt, in, s);
+    case GTSC_PATCH: return patch_encode(dt, in, s, false);
+    case GTSC_PATCH_OUTSIDE: return patch_encode(dt, in, s, true);
     case GTSC_FLOAT_TO_INT: return f2i_encode(dt, in, s);
     case GTSC_GFC: return gfc_encode(dt, in, s);
     case GTSC_UNIQUE: return unique_encode(dt, in, s);
@@ -902,7 +923,7 @@ DevBuf decode(int enc, int dt, const std::vector<View> &in, cudaStream_t s)
     case GTSC_RLE: return rle_decode(dt, v[0], v[1], v[2], s);
     case GTSC_DICT: return dict_decode(dt, v[0], v[1], v[2], s);
     case GTSC_CONST: return const_decode(dt, v[0], v[1], s);
-    case GTSC_PATCH: return patch_decode(dt, v[0], v[1], v[2], s);
+    case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: return patch_decode(dt, v[0], v[1], v[2], s);
     case GTSC_FLOAT_TO_INT: return f2i_decode(dt, v[0], v[1], s);
     case GTSC_GFC: return gfc_decode(dt, v[0], v[1], v[2], s);
     case GTSC_UNIQUE: return unique_decode(dt, v[0], v[1], s);

@@ -38,6 +38,8 @@ enum SplitMode : int { SPLIT_LOWER = 0, SPLIT_NOT_CONST = 1, SPLIT_DICT = 2 };
 struct SplitArgs {
     Order order = ORD_INT;
     uint64_t thr = 0;                        // SPLIT_LOWER: threshold bits (x < thr in T order)
+    bool outside = false;                    // SPLIT_LOWER of the outside patch: !(x > hi || x < lo)
+    uint64_t lo = 0, hi = 0;                 //   its bounds (bits, T order)
     const uint8_t *top = nullptr;            // NOT_CONST: 1 value, DICT: 4 values (device, any alignment)
     uint8_t *stencil = nullptr;              // packed stencil bytes (after the rest byte)
     uint8_t *yes = nullptr, *no = nullptr;   // ordered outputs (yes unused for DICT, no for NOT_CONST)

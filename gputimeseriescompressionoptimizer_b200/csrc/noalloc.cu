@@ -7,14 +7,15 @@
 // the caller and keeps the scan's scratch in the file-scope array below instead.
 //
 // The array is reserved in every GPU that loads this library, for the life of the process.  Its
-// device address is looked up once per device, on that device's first call (the first call on a
-// device should therefore come before any stream capture).  Every call shares the array: the
-// bytes that must start at zero are cleared at the start of each call, and two calls whose GPU
-// work overlaps -- on different streams, or on different host threads -- race on it.
+// device address is looked up with cudaGetSymbolAddress on every call, with the caller's device
+// current: the lookup allocates nothing, and a cached address would go stale if the caller reset
+// the device (cudaDeviceReset reloads the module, and the array can move).  The first call on a
+// device also loads the library's module there, so it should come before any stream capture.
+// Every call shares the array: the bytes that must start at zero are cleared at the start of each
+// call, and two calls whose GPU work overlaps -- on different streams, or on different host
+// threads -- race on it.
 #include "kernels.hpp"
 #include "scan.cuh"
-
-#include <mutex>
 
 namespace gtsc {
 
@@ -27,23 +28,12 @@ constexpr uint64_t kNoAllocScratchBytes = lookback_bytes(kNoAllocTiles);
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-uint8_t *g_scratch_addr[kMaxDevices] = {};
-
-// device address of g_noalloc_scratch for the current device (set up on first use)
+// device address of g_noalloc_scratch on the current device
 uint8_t *scratch_for_current_device()
 {
-    int dev = 0;
-    GTSC_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) fail(GTSC_ERR_ARG, "device index out of range");
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        GTSC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_scratch_addr[dev] = (uint8_t *)p;
-    }
-    return g_scratch_addr[dev];
+    void *p = nullptr;
+    GTSC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    return (uint8_t *)p;
 }
 
 }  // namespace

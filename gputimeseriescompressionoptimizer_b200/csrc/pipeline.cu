@@ -108,7 +108,12 @@ void pipeline_compress_host(Pipeline *p, const void *const *host_cols, uint8_t *
         sizes[g] = 0;
         if (!p->eng[g]) continue;
         const uint64_t nb = batch_output_bytes(p->eng[g], p->st[g]);  // waits for this group only
-        if (off + nb > cap) fail(GTSC_ERR_CAPACITY, "pipeline: host framed buffer too small");
+        if (off + nb > cap) {
+            // earlier groups' copies into host_framed (and their decodes) are in flight: let them
+            // finish so that nothing writes the caller's buffer after the error returns
+            for (int h = 0; h < G; h++) cudaStreamSynchronize(p->st[h]);
+            fail(GTSC_ERR_CAPACITY, "pipeline: host framed buffer too small");
+        }
         p->framed[g] = batch_output(p->eng[g]);
         p->framed_bytes[g] = nb;
         GTSC_CUDA(cudaMemcpyAsync(host_framed + off, p->framed[g], nb, cudaMemcpyDeviceToHost, p->st[g]));

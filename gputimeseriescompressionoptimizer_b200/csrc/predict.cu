@@ -157,7 +157,7 @@ SizePrediction predict_sizes(int enc, int dt, View in, cudaStream_t s)
     case GTSC_DELTA: return {(uint64_t)es, bytes - es};
     case GTSC_SCALE: return {(uint64_t)es, bytes};
     case GTSC_FLOAT_TO_INT: return {4, bytes};
-    case GTSC_PATCH: return {stencil, bytes};
+    case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: return {stencil, bytes};
     case GTSC_RLE: return {4, count_heads(in, es, o, s) * (4 + es)};
     case GTSC_DICT: {
         const uint64_t top = count_top(in, es, o, 4, s);

@@ -80,7 +80,8 @@ k_split(const uint8_t *__restrict__ in, uint64_t n, SplitArgs a, Lookback lb)
         bool f = false;
         uint32_t code = 0;
         if (MODE == SPLIT_LOWER) {
-            f = lt_native(v[j], a.thr, ES, a.order);
+            f = a.outside ? !(lt_native(a.hi, v[j], ES, a.order) || lt_native(v[j], a.lo, ES, a.order))
+                          : lt_native(v[j], a.thr, ES, a.order);
         } else if (MODE == SPLIT_NOT_CONST) {
             f = !same_val(v[j], top[0], a.order);
         } else {  // SPLIT_DICT

@@ -115,7 +115,8 @@ void compress_rec(const Tree &t, int &i, View in, std::vector<Seg> &segs, std::v
     const size_t seg0 = segs.size();
     ++i;
     auto push_hdr = [&](int32_t meta_len) {
-        int16_t h[2] = {(int16_t)enc, (int16_t)dt};
+        // both patch variants serialise as EncodingType::patch
+        int16_t h[2] = {(int16_t)(enc == GTSC_PATCH_OUTSIDE ? GTSC_PATCH : enc), (int16_t)dt};
         size_t off = hdrs.size();
         hdrs.resize(off + 8);
         memcpy(hdrs.data() + off, h, 4);
@@ -298,7 +299,7 @@ uint64_t predicted_metadata_size(int enc, int dt, View in, cudaStream_t s)
         if (dt == GTSC_FLOAT) return 9;
         fail(GTSC_ERR_UNSUPPORTED, "afl: no metadata-size predictor for this type");
     case GTSC_DICT: return (elems + 7) / 8 + 1;                          // dict_encoding.hpp:44-48
-    case GTSC_PATCH: return bytes ? (elems + 7) / 8 + 1 : 0;
+    case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: return bytes ? (elems + 7) / 8 + 1 : 0;
     case GTSC_CONST: return bytes ? (elems + 7) / 8 + es + 1 : 0;
     case GTSC_GFC: return 12;
     default: (void)s; fail(GTSC_ERR_UNSUPPORTED, "no metadata-size predictor for this encoding");

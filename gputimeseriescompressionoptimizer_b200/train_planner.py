@@ -16,6 +16,7 @@ import argparse
 import collections
 import concurrent.futures as cf
 import json
+import os
 import time
 
 import numpy as np
@@ -137,7 +138,7 @@ def main():
         "holdout_ratio_exhaustive": round(raw / size_ex, 4), "holdout_ratio_learned": round(raw / size_ln, 4),
         "holdout_ratio_gap": round(1 - (raw / size_ln) / (raw / size_ex), 4),
         "generate_s": round(t_gen, 1), "label_s": round(t_label, 1), "train_s": round(t_train, 1),
-        "model": args.out, "model_bytes": len(P.save()),
+        "model": os.path.basename(args.out), "model_bytes": len(P.save()),
     }), flush=True)
     del buf
 

@@ -40,7 +40,14 @@ enum { GTSC_CHAR = 0, GTSC_SHORT = 1, GTSC_INT = 2, GTSC_TIME = 3, GTSC_FLOAT = 
 /* EncodingType -- compression/encoding_type.hpp:17-30 */
 enum {
     GTSC_DELTA = 0, GTSC_AFL = 1, GTSC_SCALE = 2, GTSC_RLE = 3, GTSC_DICT = 4, GTSC_UNIQUE = 5,
-    GTSC_PATCH = 6, GTSC_NONE = 7, GTSC_FLOAT_TO_INT = 8, GTSC_CONST = 9, GTSC_GFC = 10
+    GTSC_PATCH = 6, GTSC_NONE = 7, GTSC_FLOAT_TO_INT = 8, GTSC_CONST = 9, GTSC_GFC = 10,
+    /* The outside variant of the patch encoding: PatchEncodingFactory<T>(dt, PatchType::outside)
+     * (compression/patch/patch_encoding_factory.hpp:47-55) building an OutsidePatchEncoding
+     * (outside_patch_encoding.cu:22-60).  GTSC_PATCH is the lower variant, the one
+     * DefaultEncodingFactory uses (default_encoding_factory.hpp:48-60).  Accepted by gtsc_encode /
+     * gtsc_decode and in tree node lists; a serialised tree records it as GTSC_PATCH (6), as the
+     * reference does, and both variants decode alike. */
+    GTSC_PATCH_OUTSIDE = 11
 };
 
 typedef struct {
@@ -389,8 +396,10 @@ gtsc_status gtsc_optimal_tree_destroy(gtsc_optimal_tree *t);
  * deltas) into d_out, which the caller provides with room for n_deltas + 1 values (16-byte aligned;
  * d_deltas aligned to the element size).  The scan's scratch is a static device array of ~128 KB,
  * reserved on every GPU that loads the library until exit, so at most 2^24 values are decoded per
- * call (GTSC_ERR_CAPACITY beyond).  The first call on a device looks up that array's address and
- * should come before any stream capture.  Calls share the array: calls whose GPU work overlaps race.
+ * call (GTSC_ERR_CAPACITY beyond).  Each call looks up that array's address on the current device
+ * (so a cudaDeviceReset in between is harmless); the first call on a device also loads the library's
+ * module there and should come before any stream capture.  Calls share the array: calls whose GPU
+ * work overlaps race.
  * Synchronises the stream before returning.
  */
 gtsc_status gtsc_delta_decode_noalloc(int32_t dtype, const void *d_first, const void *d_deltas,

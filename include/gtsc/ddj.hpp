@@ -155,14 +155,16 @@ inline SharedCudaPtr<char> adopt(const gtsc_buffer &b)
 
 class Encoding {
 public:
-    Encoding(EncodingType t) : _type(t) {}
+    Encoding(EncodingType t) : _type(t), _code((int32_t)t) {}
+    // `code`: the library's encoding code when it differs from the type (GTSC_PATCH_OUTSIDE)
+    Encoding(EncodingType t, int32_t code) : _type(t), _code(code) {}
     virtual ~Encoding() = default;
 
     SharedCudaPtrVector<char> Encode(SharedCudaPtr<char> data, DataType type, void *stream = nullptr)
     {
         gtsc_buffer out[3];
         uint32_t n = 0;
-        Check(gtsc_encode((int32_t)_type, (int32_t)type, data ? data->get() : nullptr, data ? data->bytes() : 0, out,
+        Check(gtsc_encode(_code, (int32_t)type, data ? data->get() : nullptr, data ? data->bytes() : 0, out,
                           &n, stream),
               "Encode");
         SharedCudaPtrVector<char> r;
@@ -176,7 +178,7 @@ public:
         const uint32_t n = (uint32_t)std::min<size_t>(input.size(), 3);
         for (uint32_t i = 0; i < n; i++) in[i] = gtsc_buffer{input[i]->get(), input[i]->bytes()};
         gtsc_buffer out{};
-        Check(gtsc_decode((int32_t)_type, (int32_t)type, in, n, &out, stream), "Decode");
+        Check(gtsc_decode(_code, (int32_t)type, in, n, &out, stream), "Decode");
         return detail::adopt(out);
     }
 
@@ -200,7 +202,7 @@ public:
     size_t GetMetadataSize(SharedCudaPtr<char> data, DataType type, void *stream = nullptr)
     {
         uint64_t m = 0, d = 0;
-        Check(gtsc_predict_sizes((int32_t)_type, (int32_t)type, data->get(), data->bytes(), &m, &d, stream),
+        Check(gtsc_predict_sizes(_code, (int32_t)type, data->get(), data->bytes(), &m, &d, stream),
               "GetMetadataSize");
         return m;
     }
@@ -208,7 +210,7 @@ public:
     size_t GetCompressedSize(SharedCudaPtr<char> data, DataType type, void *stream = nullptr)
     {
         uint64_t m = 0, d = 0;
-        Check(gtsc_predict_sizes((int32_t)_type, (int32_t)type, data->get(), data->bytes(), &m, &d, stream),
+        Check(gtsc_predict_sizes(_code, (int32_t)type, data->get(), data->bytes(), &m, &d, stream),
               "GetCompressedSize");
         return d;
     }
@@ -220,9 +222,12 @@ public:
     }
 
     EncodingType GetType() const { return _type; }
+    // the code this encoding passes to the library (the tree node list entry for it)
+    int32_t GetCode() const { return _code; }
 
 private:
     EncodingType _type;
+    int32_t _code;
 };
 
 using SharedEncodingPtr = std::shared_ptr<Encoding>;
@@ -231,19 +236,40 @@ class EncodingFactory {
 public:
     EncodingFactory(DataType dt, EncodingType et) : dataType(dt), encodingType(et) {}
     virtual ~EncodingFactory() = default;
-    SharedEncodingPtr Get() { return std::make_shared<Encoding>(encodingType); }
-    // the reference picks a patch variant from the data; only the lower variant exists here
-    SharedEncodingPtr Get(SharedCudaPtr<char>) { return Get(); }
+    virtual SharedEncodingPtr Get() { return std::make_shared<Encoding>(encodingType); }
+    virtual SharedEncodingPtr Get(SharedCudaPtr<char>) { return Get(); }
     DataType dataType;
     EncodingType encodingType;
 };
 
 using SharedEncodingFactoryPtr = std::shared_ptr<EncodingFactory>;
 
+// compression/patch/patch_type.hpp
+enum class PatchType { outside, lower };
+
+// PatchEncodingFactory<T> (compression/patch/patch_encoding_factory.hpp:20-57).  The encoding's
+// bounds come from the data's min / max, which the library computes on the device inside
+// gtsc_encode, so Get(data) only picks the variant.  Get() without data is the reference's
+// OutsidePatchEncoding(0, 0, 0) placeholder: use it to decode (both variants decode alike).
+class PatchEncodingFactory : public EncodingFactory {
+public:
+    PatchEncodingFactory(DataType dt, PatchType pt) : EncodingFactory(dt, EncodingType::patch), patchType(pt) {}
+    SharedEncodingPtr Get() override { return std::make_shared<Encoding>(EncodingType::patch, GTSC_PATCH_OUTSIDE); }
+    SharedEncodingPtr Get(SharedCudaPtr<char> data) override
+    {
+        if (!data || data->bytes() == 0) return Get();
+        return std::make_shared<Encoding>(EncodingType::patch,
+                                          patchType == PatchType::outside ? GTSC_PATCH_OUTSIDE : GTSC_PATCH);
+    }
+    PatchType patchType;
+};
+
 class DefaultEncodingFactory {
 public:
+    // default_encoding_factory.hpp:36-82: patch is the lower variant
     static SharedEncodingFactoryPtr Get(EncodingType encodingType, DataType dataType)
     {
+        if (encodingType == EncodingType::patch) return std::make_shared<PatchEncodingFactory>(dataType, PatchType::lower);
         return std::make_shared<EncodingFactory>(dataType, encodingType);
     }
 };
@@ -296,7 +322,7 @@ public:
     std::string ToString() const
     {
         static const char *names[] = {"delta", "afl", "scale", "rle", "dict", "unique", "patch", "none",
-                                      "floatToInt", "constData", "gfc"};
+                                      "floatToInt", "constData", "gfc", "patch"};
         std::string s;
         for (size_t i = 0; i < _nodes.size(); i += 2) s += std::string(names[_nodes[i]]) + ",";
         return s;

@@ -18,11 +18,12 @@ REF_PATH = os.path.join(HERE, "_ref", "libref_afl.so")
 # data types and encodings (compression/encoding_type.hpp:17-30)
 CHAR, SHORT, INT, TIME, FLOAT, DOUBLE = range(6)
 DELTA, AFL, SCALE, RLE, DICT, UNIQUE, PATCH, NONE, FLOAT2INT, CONST, GFC = range(11)
+PATCH_OUTSIDE = 11  # PatchType::outside (patch_encoding_factory.hpp:47-55), serialised as PATCH
 NP_TYPES = {CHAR: np.int8, SHORT: np.int16, INT: np.int32, TIME: np.int64,
             FLOAT: np.float32, DOUBLE: np.float64}
 DTYPE_OF = {np.dtype(v): k for k, v in NP_TYPES.items()}
 ENC_NAMES = ["delta", "afl", "scale", "rle", "dict", "unique", "patch", "none", "floatToInt",
-             "constData", "gfc"]
+             "constData", "gfc", "patch(outside)"]
 
 
 class OracleError(RuntimeError):
@@ -40,11 +41,16 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
 
 
+# the reference's source tree (read only when building oracle/_ref; absent on machines that only
+# run the prebuilt files)
+REF_SRC = os.environ.get("GTSC_REFERENCE_SRC", "/root/reference/src")
+
+
 def build_ref():
     """Compile the reference AFL host path; returns False when the reference tree is absent."""
-    if not os.path.isdir("/root/reference/src"):
+    if not os.path.isdir(REF_SRC):
         return os.path.exists(REF_PATH)
-    subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
     return True
 
 

@@ -756,18 +756,39 @@ static uint64_t lower_patch_threshold(uint64_t mnb, uint64_t mxb, int dt)
     return cast_double_to_T(t, dt);
 }
 
+/* bounds of OutsidePatchEncoding::GetOperator<T> (outside_patch_encoding.cu:22-31), factor 0.1:
+ * T dist = _max - _min; low = static_cast<T>(_min + 0.1 * dist), high = static_cast<T>(_max - 0.1 * dist) */
+static void outside_patch_bounds(uint64_t mnb, uint64_t mxb, int dt, uint64_t *lo, uint64_t *hi)
+{
+    double dmin = T_to_double(mnb, dt), dmax = T_to_double(mxb, dt);
+    uint64_t dist_bits = cast_double_to_T(dmax - dmin, dt);
+    double ddist = T_to_double(dist_bits, dt);
+    if (dt != OR_FLOAT && dt != OR_DOUBLE) ddist = (double)sext(dist_bits, es_of(dt));
+    double prod = 0.1 * ddist;
+    *lo = cast_double_to_T(dmin + prod, dt);
+    *hi = cast_double_to_T(dmax - prod, dt);
+}
+
 /* PatchEncodingFactory<T>::Get(data) (patch_encoding_factory.hpp:40-57) + LowerPatchEncoding
  * (lower_patch_encoding.cu:33-94): stencil x < t, meta = packed stencil, out1 = x < t values,
- * out2 = the rest, both in order. */
-static int patch_encode(int dt, const uint8_t *in, uint64_t n, uint8_t *meta, uint8_t *o1, uint8_t *o2, uint64_t ob[3])
+ * out2 = the rest, both in order.  With `outside`, OutsidePatchEncoding::Encode
+ * (outside_patch_encoding.cu:33-60): stencil = OutsideOperator (stencil_operators.hpp:14-25),
+ * true unless x > high or x < low (so NaN is true), same three outputs.  Empty input: three empty
+ * buffers for both variants. */
+static int patch_encode(int dt, const uint8_t *in, uint64_t n, uint8_t *meta, uint8_t *o1, uint8_t *o2, uint64_t ob[3],
+                        int outside)
 {
     int es = es_of(dt);
     if (n == 0) { ob[0] = ob[1] = ob[2] = 0; return OR_OK; }
     uint64_t mnb, mxb;
     or_minmax_bits(in, dt, n, &mnb, &mxb);
-    uint64_t t = lower_patch_threshold(mnb, mxb, dt);
+    uint64_t t = lower_patch_threshold(mnb, mxb, dt), lo = 0, hi = 0;
+    if (outside) outside_patch_bounds(mnb, mxb, dt, &lo, &hi);
     int32_t *st = (int32_t *)malloc(n * sizeof(int32_t));
-    for (uint64_t i = 0; i < n; i++) st[i] = lt_bits(ld_u(in, es, i), t, dt);
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t x = ld_u(in, es, i);
+        st[i] = outside ? !(lt_bits(hi, x, dt) || lt_bits(x, lo, dt)) : lt_bits(x, t, dt);
+    }
     uint64_t ny, nn;
     or_split(in, es, n, st, o1, &ny, o2, &nn);
     ob[0] = or_stencil_pack(st, n, meta);
@@ -942,7 +963,8 @@ int or_encode(int enc, int dt, const uint8_t *in, uint64_t in_bytes,
     case OR_DICT: *n_out = 3; return dict_encode(dt, in, n, o0, o1, o2, ob);
     case OR_UNIQUE: *n_out = 2; return unique_encode(dt, in, n, o0, o1, ob);
     case OR_CONST: *n_out = 2; return const_encode(dt, in, n, o0, o1, ob);
-    case OR_PATCH: *n_out = 3; return patch_encode(dt, in, n, o0, o1, o2, ob);
+    case OR_PATCH: *n_out = 3; return patch_encode(dt, in, n, o0, o1, o2, ob, 0);
+    case OR_PATCH_OUTSIDE: *n_out = 3; return patch_encode(dt, in, n, o0, o1, o2, ob, 1);
     case OR_FLOAT2INT: *n_out = 2; return f2i_encode(dt, in, n, o0, o1, ob);
     case OR_GFC:
         if (!is_fp(dt)) {
@@ -974,7 +996,7 @@ int or_decode(int enc, int dt, const uint8_t *i0, uint64_t b0, const uint8_t *i1
     case OR_DICT: return dict_decode(dt, i0, b0, i1, b1, i2, b2, out, cap, ob);
     case OR_UNIQUE: return unique_decode(dt, i0, b0, i1, b1, out, cap, ob);
     case OR_CONST: return const_decode(dt, i0, b0, i1, b1, out, cap, ob);
-    case OR_PATCH: return patch_decode(dt, i0, b0, i1, b1, i2, b2, out, cap, ob);
+    case OR_PATCH: case OR_PATCH_OUTSIDE: return patch_decode(dt, i0, b0, i1, b1, i2, b2, out, cap, ob);
     case OR_FLOAT2INT: return f2i_decode(dt, i0, b0, i1, b1, out, cap, ob);
     case OR_GFC:
         if (!is_fp(dt)) return afl_decode(dt, i0, b0, i1, b1, out, cap, ob);

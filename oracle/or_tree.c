@@ -13,7 +13,7 @@ static int nres(int enc)
 {
     switch (enc) {
     case OR_DELTA: case OR_AFL: case OR_SCALE: case OR_UNIQUE: case OR_FLOAT2INT: case OR_CONST: return 1;
-    case OR_RLE: case OR_DICT: case OR_PATCH: case OR_GFC: return 2;
+    case OR_RLE: case OR_DICT: case OR_PATCH: case OR_PATCH_OUTSIDE: case OR_GFC: return 2;
     case OR_NONE: return 0;
     default: return -1;
     }
@@ -86,7 +86,8 @@ static int compress_rec(cursor_t *c, const uint8_t *in, uint64_t in_bytes, uint8
         if (*w + 8 + ob[0] > cap) e = OR_ERR_CAP;
     }
     if (!e) {
-        int16_t hdr16[2] = {(int16_t)enc, (int16_t)dt};
+        /* both patch variants serialise as EncodingType::patch */
+        int16_t hdr16[2] = {(int16_t)(enc == OR_PATCH_OUTSIDE ? OR_PATCH : enc), (int16_t)dt};
         int32_t ml = (int32_t)ob[0];
         memcpy(out + *w, hdr16, 4);
         memcpy(out + *w + 4, &ml, 4);
@@ -226,7 +227,7 @@ static int meta_size(int enc, int dt, const uint8_t *in, uint64_t bytes, uint64_
         if (dt == OR_FLOAT) { *ms = 9; return OR_OK; }
         return OR_ERR_UNSUPPORTED;
     case OR_DICT: *ms = (elems + 7) / 8 + 1; return OR_OK;               /* dict_encoding.hpp:44-48 */
-    case OR_PATCH: *ms = bytes ? (elems + 7) / 8 + 1 : 0; return OR_OK;
+    case OR_PATCH: case OR_PATCH_OUTSIDE: *ms = bytes ? (elems + 7) / 8 + 1 : 0; return OR_OK;
     case OR_CONST: *ms = bytes ? (elems + 7) / 8 + es + 1 : 0; return OR_OK;
     case OR_GFC: *ms = 12; return OR_OK;
     case OR_UNIQUE: {

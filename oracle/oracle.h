@@ -33,7 +33,10 @@ enum or_dtype { OR_CHAR = 0, OR_SHORT = 1, OR_INT = 2, OR_TIME = 3, OR_FLOAT = 4
 /* compression/encoding_type.hpp:17-30 */
 enum or_enc {
     OR_DELTA = 0, OR_AFL = 1, OR_SCALE = 2, OR_RLE = 3, OR_DICT = 4, OR_UNIQUE = 5,
-    OR_PATCH = 6, OR_NONE = 7, OR_FLOAT2INT = 8, OR_CONST = 9, OR_GFC = 10
+    OR_PATCH = 6, OR_NONE = 7, OR_FLOAT2INT = 8, OR_CONST = 9, OR_GFC = 10,
+    /* PatchEncodingFactory(dt, PatchType::outside) (patch_encoding_factory.hpp:47-55): encoded by
+     * OutsidePatchEncoding, serialised and decoded as patch (6) */
+    OR_PATCH_OUTSIDE = 11
 };
 
 enum or_status {

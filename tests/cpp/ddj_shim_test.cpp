@@ -66,6 +66,18 @@ int main()
         EXPECT(same(enc->Decode(enc->Encode(data, DataType::d_float), DataType::d_float), floats));
     }
 
+    // PatchEncodingFactory with either patch type (patch_encoding_factory.hpp:40-57): Get(data)
+    // encodes, Get() decodes either variant
+    for (PatchType pt : {PatchType::outside, PatchType::lower}) {
+        PatchEncodingFactory f(DataType::d_int, pt);
+        auto data = CastSharedCudaPtr<int, char>(device(ints));
+        auto enc = f.Get(data);
+        EXPECT(enc->GetType() == EncodingType::patch);
+        auto encoded = enc->Encode(data, DataType::d_int);
+        EXPECT(encoded.size() == 3);
+        EXPECT(same(f.Get()->Decode(encoded, DataType::d_int), ints));
+    }
+
     // TestGetMetadataSize / TestGetCompressedSize (test/compression_unittest_base.hpp:32-54)
     for (EncodingType et : {EncodingType::rle, EncodingType::dict, EncodingType::constData, EncodingType::delta,
                             EncodingType::afl, EncodingType::unique}) {

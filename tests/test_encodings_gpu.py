@@ -81,7 +81,7 @@ def test_elementwise_encodings(G, O, rng, enc, dt, npt, n):
 
 
 @pytest.mark.parametrize("dt,npt", ALL_TYPES)
-@pytest.mark.parametrize("enc", [OR.RLE, OR.DICT, OR.CONST, OR.PATCH])
+@pytest.mark.parametrize("enc", [OR.RLE, OR.DICT, OR.CONST, OR.PATCH, OR.PATCH_OUTSIDE])
 @pytest.mark.parametrize("n", SIZES)
 def test_split_and_run_encodings(G, O, rng, enc, dt, npt, n):
     for kind in KINDS:

@@ -140,3 +140,49 @@ def test_afl_config1_sizes(O, rng):
     assert data.size == 1441792
     if OR.build_ref():
         assert np.array_equal(O.ref_afl_compress(OR.INT, x, 11), data)
+
+
+# ---- outside patch (outside_patch_encoding.cu:22-60, stencil_operators.hpp:14-25) -----------
+def _stencil_bits(st):
+    """Stencil::pack layout: rest byte, then LSB-first bits, the tail repeating the last element."""
+    n = st.size
+    pad = (-n) % 8
+    full = np.concatenate([st, np.full(pad, st[-1])]).astype(np.uint8)
+    return np.concatenate([[n % 8], np.packbits(full, bitorder="little")]).astype(np.uint8)
+
+
+def test_outside_patch_kat(O, rng):
+    """low = (int)(min + 0.1 * dist), high = (int)(max - 0.1 * dist); elements in [low, high] go to
+    out1, the others (both tails) to out2, in order."""
+    x = rng.integers(-1000, 1000, 5000).astype(np.int32)
+    x[7], x[9] = -1000, 999
+    mn, mx = int(x.min()), int(x.max())
+    dist = mx - mn
+    lo, hi = int(mn + 0.1 * dist), int(mx - 0.1 * dist)   # truncation toward zero, as static_cast<int>
+    inside = (x >= lo) & (x <= hi)
+    meta, o1, o2 = O.encode(OR.PATCH_OUTSIDE, OR.INT, x)
+    assert np.array_equal(o1.view(np.int32), x[inside])
+    assert np.array_equal(o2.view(np.int32), x[~inside])
+    assert np.array_equal(meta, _stencil_bits(inside))
+    assert np.array_equal(O.decode(OR.PATCH_OUTSIDE, OR.INT, [meta, o1, o2]).view(np.int32), x)
+    assert np.array_equal(O.decode(OR.PATCH, OR.INT, [meta, o1, o2]).view(np.int32), x)
+
+
+def test_outside_patch_nan_is_inside(O):
+    """OutsideOperator returns true unless x > high or x < low: NaN compares false both ways."""
+    x = np.array([0.0, 100.0, 50.0, np.nan, 5.0, 95.0], np.float64)
+    meta, o1, o2 = O.encode(OR.PATCH_OUTSIDE, OR.DOUBLE, x)
+    # min/max skip NaN: 0 and 100, bounds 10 and 90
+    got = o1.view(np.float64)
+    assert got.size == 2 and got[0] == 50.0 and np.isnan(got[1])
+    assert np.array_equal(o2.view(np.float64), [0.0, 100.0, 5.0, 95.0])
+
+
+def test_outside_patch_tree_serialises_as_patch(O, rng):
+    """A tree with an outside patch node records EncodingType::patch (6) in its header and decodes."""
+    x = rng.integers(0, 1 << 12, 3000).astype(np.int32)
+    nodes = O.tree_from_path([OR.PATCH_OUTSIDE, OR.AFL, OR.NONE, OR.AFL, OR.NONE], OR.INT)
+    blob = O.tree_compress(nodes, x)
+    assert blob[:2].view(np.int16)[0] == OR.PATCH
+    out, dt = O.tree_decompress(blob, x.nbytes)
+    assert dt == OR.INT and np.array_equal(out.view(np.int32), x)

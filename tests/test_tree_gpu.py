@@ -77,6 +77,10 @@ TREES = [
     ([OR.PATCH, OR.DELTA, OR.SCALE, OR.AFL, OR.NONE, OR.DELTA, OR.SCALE, OR.AFL, OR.NONE], OR.INT, "b"),
     ([OR.GFC, OR.NONE, OR.NONE], OR.DOUBLE, "prec3"),
     ([OR.DELTA, OR.GFC, OR.NONE, OR.NONE], OR.DOUBLE, "prec3"),
+    # ComplexTree_Patch (compression_tree_unittest.cpp:124-150): an outside patch root
+    ([OR.PATCH_OUTSIDE, OR.DICT, OR.DELTA, OR.NONE, OR.SCALE, OR.NONE, OR.DELTA, OR.NONE], OR.INT, "int"),
+    ([OR.PATCH_OUTSIDE, OR.AFL, OR.NONE, OR.AFL, OR.NONE], OR.INT, "ts"),
+    ([OR.SCALE, OR.PATCH_OUTSIDE, OR.GFC, OR.NONE, OR.NONE, OR.NONE], OR.DOUBLE, "prec3"),
 ]
 
 
