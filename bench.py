@@ -10,7 +10,8 @@ framed buffer and decompress it again, with the columns resident in HBM; `value`
 GB/s.  Beside it: the plain path (one column at a time through gtsc_tree_compress /
 gtsc_tree_decompress, host-synchronising as the reference's per-column calls do), the planners'
 cost, the dominant kernel against the HBM roofline, an end-to-end step from pinned host memory,
-and the CPU oracle on a bounded sample.
+the CPU oracle on the same workload, and each benchmark configuration (AFL alone, the int32
+chains, GFC) measured alone.
 
 N > 1 runs N independent replicas (one process per GPU, launched by torchrun): the columns are
 independent and the path has no exchange step, so `value` is the work of all ranks over the
@@ -35,7 +36,6 @@ PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 N_COLUMNS = int(os.environ.get("GTSC_BENCH_COLUMNS", "512"))
 MAX_LEN = 1 << int(os.environ.get("GTSC_BENCH_MAX_LOG2", "24"))
-CPU_SAMPLE_LEN = 1 << 18     # CPU legs: every column cut to its first 2^18 values
 MIN_CONFIDENCE = 0.5         # learned planner: below this softmax probability the exhaustive search decides
 TICK_CHUNKS = 4              # streaming tick table: 40 columns x 2^20 rows per chunk
 E2E_GROUPS = 8               # end to end: column groups pipelined over their own streams
@@ -130,22 +130,40 @@ def gen_columns(specs, max_len=None, threads=None):
 
 
 # ------------------------------------------------------------------------------- CPU legs
+def cpu_model():
+    """The host CPU's model name and the number of hardware threads."""
+    name = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    name = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return name, os.cpu_count() or 1
+
+
 def cpu_roundtrip(cols, trees, threads):
-    """The oracle's CompressionTree::Compress + Decompress of every column (one task per column,
-    `threads` host threads; ctypes releases the GIL).  Returns (seconds, input bytes, blob bytes)."""
+    """The oracle's CompressionTree::Compress + Decompress of every column: one task per column,
+    largest columns first, `threads` host threads (ctypes releases the GIL).  A column's blob depends
+    on the whole column (its min / max, histogram and run boundaries), so a column is one task.
+    Returns (seconds, input bytes, blob bytes)."""
     import oracle
+
+    order = sorted(range(len(cols)), key=lambda i: -cols[i].nbytes)
 
     def work(i):
         blob = oracle.tree_compress(trees[i], cols[i])
         out, _ = oracle.tree_decompress(blob, cols[i].nbytes)
-        return blob.size, out.size
+        return blob.size, out.size, cols[i].nbytes
 
     t = time.perf_counter()
     with cf.ThreadPoolExecutor(threads) as ex:
-        res = list(ex.map(work, range(len(cols))))
+        res = list(ex.map(work, order))
     dt = time.perf_counter() - t
-    assert all(o == c.nbytes for (_, o), c in zip(res, cols))
-    return dt, sum(c.nbytes for c in cols), sum(b for b, _ in res)
+    assert all(o == c for _, o, c in res)
+    return dt, sum(c.nbytes for c in cols), sum(b for b, _, _ in res)
 
 
 def oracle_check(cols, trees, blobs, threads=None):
@@ -178,13 +196,18 @@ def cpu_trees(cols, specs):
 
 
 def run_reference(args, world, rank):
-    """The reference's CPU implementation of the path (the oracle restatement: no part of the
-    reference's own tree code compiles here), all host threads, on a bounded sample per step."""
+    """The reference's CPU implementation of the path on the same workload: no part of the
+    reference's own tree code compiles here (boost, log4cplus, a missing submodule), so this is the
+    oracle restatement built -O3 -march=native on this host, with every host thread, over the full
+    512-column workload per step, with the trees the exhaustive planner picks."""
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
+    import oracle
+
+    build = oracle.select_native()
+    model, threads = cpu_model()
     specs = workload_specs()
-    cols = gen_columns(specs, CPU_SAMPLE_LEN)
+    cols = gen_columns(specs)
     trees = cpu_trees(cols, specs)
     for _ in range(max(args.warmup, 1)):
         cpu_roundtrip(cols, trees, threads)
@@ -194,7 +217,8 @@ def run_reference(args, world, rank):
         times.append(t)
     t = sum(times) / len(times)
     gbs = in_bytes / t / 1e9
-    sample = f"all {len(cols)} columns cut to their first 2^18 values ({in_bytes} B), trees planned on them"
+    sample = (f"the full workload each step: all {len(cols)} columns ({in_bytes} B), trees from the exhaustive "
+              f"planner on each column's sample; {build}; {threads} threads on {model}")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t, 3), "higher_is_better": True,
@@ -203,7 +227,8 @@ def run_reference(args, world, rank):
         "config": {"workload": WORKLOAD, "inputs": "host memory",
                    "step": "CompressionTree::Compress + Decompress of every column (CPU restatement)",
                    "compression_ratio": round(in_bytes / blob_bytes, 4)},
-        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample,
+                         "cpu_model": model},
         "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -276,6 +301,98 @@ def tick_table(g, torch, planner, st, stream, sp):
             "fallback_rate": round(sum(r["fallbacks"] for r in res) / (40.0 * len(res)), 4),
             "planning_speedup": round(sum(r["plan_exhaustive_ms"] for r in res) /
                                       max(sum(r["plan_learned_ms"] for r in res), 1e-9), 1)}
+
+
+# the benchmark configurations measured one by one beside the mixed workload: (name, generator,
+# data type, values, compression tree as a pre-order encoding list)
+CONFIG_COLUMNS = [
+    ("1 afl", "uniform11", 2, 1 << 20, [1, 7]),
+    ("2a delta-afl", "walk", 2, 1 << 26, [0, 1, 7]),
+    ("2a delta-scale-afl", "walk", 2, 1 << 26, [0, 2, 1, 7]),
+    ("2b rle-afl-afl", "runs", 2, 1 << 26, [3, 1, 7, 1, 7]),
+    ("2c dict-afl-afl", "zipf", 2, 1 << 26, [4, 1, 7, 1, 7]),
+    ("2d const-afl", "const", 2, 1 << 26, [9, 1, 7]),
+    ("2e patch-afl-afl", "outliers", 2, 1 << 26, [6, 1, 7, 1, 7]),
+    ("3 gfc double", "price", 5, 1 << 26, [10, 7, 7]),
+    ("3 gfc float", "price", 4, 1 << 26, [10, 7, 7]),
+]
+
+
+def config_column(k):
+    from gputimeseriescompressionoptimizer_b200 import workloads as W
+    name, kind, dt, n, _ = CONFIG_COLUMNS[k]
+    if kind == "uniform11":
+        return np.random.default_rng(0xB201).integers(0, 1 << 11, n).astype(np.int32)
+    return W.column(kind, dt, n, 0xB202 + (k if kind != "price" else 8))
+
+
+def per_config(g, torch, st, stream, peak, reps):
+    """Each benchmark configuration alone as a one-column batch (its tree's compress and decompress
+    steps, CUDA graphs, device-resident input): CUDA-event time per step (median of `reps`, the L2
+    flushed before each step when the column fits in it), GB/s of uncompressed input and the
+    fraction of the HBM peak on algorithmic bytes (n*s + C each way).  Config 1 also times the AFL
+    pack / unpack kernels alone at its bit width 11 (run_afl_compress_gpu / run_afl_decompress_gpu)."""
+    with cf.ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        cols = list(ex.map(config_column, range(len(CONFIG_COLUMNS))))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def med_time(fn, small):
+        ts = []
+        for _ in range(reps + 2):
+            if small:
+                flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return statistics.median(ts[2:])
+
+    out = []
+    for k, (name, kind, dt, n, path) in enumerate(CONFIG_COLUMNS):
+        x = cols[k]
+        dev = torch.from_numpy(x.view(np.uint8)).to("cuda")
+        dv = DevView(dev)
+        small = x.nbytes < (128 << 20)
+        nodes = g.tree_from_path(path, dt)
+        b = g.Batch([dv], [dt], [nodes], st)
+        o = torch.empty_like(dev)
+        ov = [DevView(o)]
+        b.compress()
+        b.status()
+        p, nb = b.output()
+        b.decompress(p, nb, ov)
+        b.status()
+        assert torch.equal(o, dev), f"config {name}: round trip differs"
+        blob = int(b.blob_sizes()[0])
+        tc = med_time(b.compress, small)
+        td = med_time(lambda: b.decompress(p, nb, ov), small)
+        b.status()
+        alg = x.nbytes + blob
+        row = {"config": name, "values": n, "input_bytes": x.nbytes, "blob_bytes": blob,
+               "ratio": round(x.nbytes / blob, 4), "compress_ms": round(1e3 * tc, 4),
+               "decompress_ms": round(1e3 * td, 4), "compress_GBps": round(x.nbytes / tc / 1e9, 1),
+               "decompress_GBps": round(x.nbytes / td / 1e9, 1),
+               "compress_hbm_frac": round(alg / tc / 1e9 / peak, 4),
+               "decompress_hbm_frac": round(alg / td / 1e9 / peak, 4),
+               "launches": [b.launches(True), b.launches(False)]}
+        if k == 0:  # the AFL kernels alone at b = 11
+            L = g.lib()
+            words = (n * 11 + 31) // 32
+            packed = torch.empty(words * 4, dtype=torch.uint8, device="cuda")
+            back = torch.empty_like(dev)
+            tp = med_time(lambda: g.check(L.gtsc_afl_compress_gpu(dt, 11, dv.ptr, n, packed.data_ptr(), words * 4,
+                                                                   st.handle), "afl"), small)
+            tu = med_time(lambda: g.check(L.gtsc_afl_decompress_gpu(dt, 11, packed.data_ptr(), words * 4,
+                                                                     back.data_ptr(), n, st.handle), "afl"), small)
+            assert torch.equal(back, dev)
+            row["afl_kernels_b11"] = {"pack_ms": round(1e3 * tp, 4), "unpack_ms": round(1e3 * tu, 4),
+                                      "pack_GBps": round((x.nbytes + words * 4) / tp / 1e9, 1),
+                                      "unpack_GBps": round((x.nbytes + words * 4) / tu / 1e9, 1)}
+        out.append(row)
+        del b, o, ov, dev, dv
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -456,14 +573,17 @@ def run_ours(args, world, rank, local):
     alg_step = 2 * (in_bytes + blob_bytes + 8 + 8 * len(cols))
     value = world * in_bytes / t_step / 1e9
 
-    # CPU baseline: the oracle on a bounded sample (same trees), all host threads
-    threads = os.cpu_count() or 1
-    scols = gen_columns(specs, CPU_SAMPLE_LEN)
-    cpu_roundtrip(scols, trees, threads)
-    ct, cin, _ = min((cpu_roundtrip(scols, trees, threads) for _ in range(2)), key=lambda r: r[0])
+    # CPU baseline: the oracle (built -O3 -march=native here) on the same workload and trees, all
+    # host threads, best of two after a warm-up
+    import oracle
+    cpu_build = oracle.select_native()
+    model, threads = cpu_model()
+    cpu_roundtrip(cols, trees, threads)
+    ct, cin, _ = min((cpu_roundtrip(cols, trees, threads) for _ in range(2)), key=lambda r: r[0])
     cpu_gbs = cin / ct / 1e9
 
     tick = tick_table(g, torch, planner, st, stream, sp) if rank == 0 else None
+    configs = per_config(g, torch, st, stream, peak, max(3, args.steps)) if rank == 0 else None
     tree_names = {}
     for t in trees:
         k = "-".join(g.tree_names(t))
@@ -501,8 +621,9 @@ def run_ours(args, world, rank, local):
                      "timing": "CUDA events around each launch of one step replayed launch by launch"},
         "launches": {k: [[x[0], round(x[1], 4), x[2], x[3]] for x in v] for k, v in prof.items()},
         "cpu_baseline": {"value": round(cpu_gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"all {len(scols)} columns cut to their first 2^18 values ({cin} B), same trees, "
-                                   "oracle tree compress + decompress"},
+                         "sample": f"the full workload: all {len(cols)} columns ({cin} B), the same trees, oracle "
+                                   f"tree compress + decompress, best of 2; {cpu_build}",
+                         "cpu_model": model},
         "e2e": {"value": round(world * in_bytes / t_e2e / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": in_bytes,
                 "d2h_bytes_per_step": e2e_bytes["d2h"],
                 "path": f"gtsc_pipeline_roundtrip_host: {E2E_GROUPS} column groups, pinned host columns in, "
@@ -512,6 +633,7 @@ def run_ours(args, world, rank, local):
                    "what": "every batched blob of the first step byte-compared with the oracle's "
                            "CompressionTree::Compress of its column; every column's round trip bit-exact"},
         "tick_table": tick,
+        "configs": configs,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

@@ -58,44 +58,61 @@ _lib = None
 _ref = None
 
 
+NATIVE_PATH = os.path.join(HERE, "_native", "liboracle.so")
+
+
+def select_native():
+    """Build the oracle -O3 -march=native for this host (oracle/_native, never shipped elsewhere)
+    and route every later call through it.  Used only by the timed CPU legs of bench.py; parity
+    checks run on the default build.  Returns a description of the build."""
+    global _lib
+    subprocess.run(["make", "-s", "-C", HERE, "native"], check=True)
+    _lib = _bind(ctypes.CDLL(NATIVE_PATH))
+    return "C oracle, gcc -O3 -march=native -ffp-contract=off"
+
+
 def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
-        L = ctypes.CDLL(LIB_PATH)
-        u8p = ctypes.POINTER(ctypes.c_uint8)
-        u64p = ctypes.POINTER(ctypes.c_uint64)
-        L.or_encode.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
-                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
-                                u64p, ctypes.POINTER(ctypes.c_int)]
-        L.or_decode.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
-                                ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
-                                ctypes.c_void_p, ctypes.c_uint64, u64p]
-        L.or_bitlen.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64]
-        L.or_alt_bitlen.argtypes = [ctypes.c_int]
-        L.or_stats.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Stats)]
-        L.or_rl_metric.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int]
-        L.or_rl_metric.restype = ctypes.c_float
-        L.or_float_precision.argtypes = [ctypes.c_float]
-        L.or_stencil_pack.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
-        L.or_stencil_pack.restype = ctypes.c_uint64
-        L.or_stencil_unpack.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64]
-        L.or_stencil_unpack.restype = ctypes.c_int64
-        L.or_tree_from_path.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
-        L.or_tree_compress.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
-                                       ctypes.c_void_p, ctypes.c_uint64, u64p]
-        L.or_tree_decompress.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
-                                         u64p, ctypes.POINTER(ctypes.c_int)]
-        L.or_tree_predict_size.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, u64p]
-        for f in (L.or_plan_exhaustive, L.or_optimize_tree):
-            f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int,
-                          ctypes.POINTER(ctypes.c_int), u64p]
-        L.or_sample_bytes.argtypes = [ctypes.c_int, ctypes.c_uint64]
-        L.or_sample_bytes.restype = ctypes.c_uint64
-        del u8p
-        _lib = L
+        _lib = _bind(ctypes.CDLL(LIB_PATH))
     return _lib
+
+
+def _bind(L):
+    """Declare the argument and result types of the oracle's C functions on a loaded library."""
+    u8p = ctypes.POINTER(ctypes.c_uint8)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    L.or_encode.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                            u64p, ctypes.POINTER(ctypes.c_int)]
+    L.or_decode.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                            ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
+                            ctypes.c_void_p, ctypes.c_uint64, u64p]
+    L.or_bitlen.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64]
+    L.or_alt_bitlen.argtypes = [ctypes.c_int]
+    L.or_stats.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Stats)]
+    L.or_rl_metric.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int]
+    L.or_rl_metric.restype = ctypes.c_float
+    L.or_float_precision.argtypes = [ctypes.c_float]
+    L.or_stencil_pack.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    L.or_stencil_pack.restype = ctypes.c_uint64
+    L.or_stencil_unpack.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64]
+    L.or_stencil_unpack.restype = ctypes.c_int64
+    L.or_tree_from_path.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+    L.or_tree_compress.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                   ctypes.c_void_p, ctypes.c_uint64, u64p]
+    L.or_tree_decompress.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
+                                     u64p, ctypes.POINTER(ctypes.c_int)]
+    L.or_tree_predict_size.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, u64p]
+    for f in (L.or_plan_exhaustive, L.or_optimize_tree):
+        f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int,
+                      ctypes.POINTER(ctypes.c_int), u64p]
+    L.or_sample_bytes.argtypes = [ctypes.c_int, ctypes.c_uint64]
+    L.or_sample_bytes.restype = ctypes.c_uint64
+    del u8p
+    return L
 
 
 def ref():

@@ -129,17 +129,19 @@ void or_radix_sort_u64(uint64_t *keys, uint64_t n)
     if (n < 2) return;
     uint64_t *tmp = (uint64_t *)malloc(n * sizeof(uint64_t));
     uint64_t *src = keys, *dst = tmp;
+    uint64_t *cnt = (uint64_t *)malloc(65536 * sizeof(uint64_t));
     for (int pass = 0; pass < 4; pass++) {
         int sh = 16 * pass;
-        uint64_t *cnt = (uint64_t *)calloc(65536, sizeof(uint64_t));
+        memset(cnt, 0, 65536 * sizeof(uint64_t));
         for (uint64_t i = 0; i < n; i++) cnt[(src[i] >> sh) & 0xffff]++;
+        if (cnt[(src[0] >> sh) & 0xffff] == n) continue;  /* one digit value: the order stands */
         uint64_t s = 0;
         for (int d = 0; d < 65536; d++) { uint64_t c = cnt[d]; cnt[d] = s; s += c; }
         for (uint64_t i = 0; i < n; i++) dst[cnt[(src[i] >> sh) & 0xffff]++] = src[i];
-        free(cnt);
         uint64_t *t = src; src = dst; dst = t;
     }
-    /* 4 passes: result is back in keys */
+    if (src != keys) memcpy(keys, src, n * sizeof(uint64_t));
+    free(cnt);
     free(tmp);
 }
 
@@ -206,12 +208,16 @@ static int afl_encode(int dt, const uint8_t *in, uint64_t n, uint8_t *meta, uint
     meta[0] = (uint8_t)b; meta[1] = (uint8_t)rest; meta[2] = 0; meta[3] = 0;
     memset(out, 0, bytes);
     uint64_t mask = b >= 64 ? ~0ULL : ((1ULL << b) - 1);
+    /* the bitstream in byte order: whole bytes leave a 128-bit accumulator as soon as they fill */
+    unsigned __int128 acc = 0;
+    int fill = 0;
+    uint8_t *o = out;
     for (uint64_t i = 0; i < n; i++) {
-        uint64_t v = ld_u(in, es, i) & mask;
-        uint64_t pos = i * (uint64_t)b;
-        for (int k = 0; k < b; k++, pos++)
-            if ((v >> k) & 1) out[pos >> 3] |= (uint8_t)(1u << (pos & 7));
+        acc |= (unsigned __int128)(ld_u(in, es, i) & mask) << fill;
+        fill += b;
+        while (fill >= 8) { *o++ = (uint8_t)acc; acc >>= 8; fill -= 8; }
     }
+    if (fill > 0) *o = (uint8_t)acc;
     ob[0] = 4; ob[1] = bytes;
     return OR_OK;
 }
@@ -229,11 +235,14 @@ static int afl_decode(int dt, const uint8_t *meta, uint64_t mb, const uint8_t *d
     if (bits < 0) return OR_ERR_FORMAT;
     uint64_t n = (uint64_t)bits / b;
     if (n * es > cap) return OR_ERR_CAP;
+    uint64_t mask = b >= 64 ? ~0ULL : ((1ULL << b) - 1);
     for (uint64_t i = 0; i < n; i++) {
-        uint64_t v = 0, pos = i * (uint64_t)b;
-        for (int k = 0; k < b; k++, pos++)
-            if ((data[pos >> 3] >> (pos & 7)) & 1) v |= 1ULL << k;
-        st_u(out, es, i, v);
+        /* bits [pos, pos + b) of the LSB-first stream: up to 9 bytes from byte pos / 8 */
+        uint64_t pos = i * (uint64_t)b, first = pos >> 3;
+        unsigned __int128 w = 0;
+        int nbytes = (int)((((pos & 7) + (uint64_t)b) + 7) >> 3);
+        for (int k = 0; k < nbytes; k++) w |= (unsigned __int128)data[first + k] << (8 * k);
+        st_u(out, es, i, (uint64_t)(w >> (pos & 7)) & mask);
     }
     *ob = n * es;
     return OR_OK;
