@@ -337,9 +337,22 @@ def per_config(g, torch, st, stream, peak, reps):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def med_time(fn, small):
+        """Columns that fit in L2: each call timed alone after a 256 MB write on the same stream
+        (it evicts the column from L2 and keeps the GPU busy while the host issues the call); larger
+        columns: `reps` calls back to back between two events, after two warm-up calls."""
+        if not small:
+            for _ in range(2):
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / 1e3 / reps
         ts = []
         for _ in range(reps + 2):
-            if small:
+            with torch.cuda.stream(stream):
                 flush.fill_(1)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)

@@ -135,6 +135,8 @@ def lib():
         L.gtsc_batch_decompress.argtypes = [vp, vp, u64, ctypes.POINTER(vp), vp]
         L.gtsc_batch_status.argtypes = [vp, vp]
         L.gtsc_batch_launches.argtypes = [vp, i32]
+        L.gtsc_batch_set_schedule.argtypes = [vp, i32]
+        L.gtsc_batch_schedule.argtypes = [vp]
         L.gtsc_batch_destroy.argtypes = [vp]
         L.gtsc_batch_profile.argtypes = [vp, i32, i32p, ctypes.POINTER(ctypes.c_float), u64p, u64p, i32, i32p, vp]
         L.gtsc_pipeline_create.argtypes = [ctypes.POINTER(Column), u32, i16p, i32p, i32, ctypes.POINTER(vp)]
@@ -393,7 +395,7 @@ PASS_NAMES = dict(enumerate(
      "delta_dec", "scale_add", "merge", "rle_scan", "rle_expand", "f2i_dec", "gfc_sizes", "gfc_dec", "vmeta",
      "merge_count"]))
 PASS_NAMES.update({-1: "set_streams", -2: "zero", -3: "frame_sizes", -4: "frame_layout", -5: "frame_copy",
-                   -6: "parse_frames"})
+                   -6: "parse_frames", -7: "persistent"})
 
 
 class Batch:
@@ -448,6 +450,13 @@ class Batch:
 
     def launches(self, compress=True):
         return lib().gtsc_batch_launches(self.handle, 1 if compress else 0)
+
+    def set_schedule(self, persistent):
+        """Replay the steps as one persistent launch per step (True) or per level (False)."""
+        check(lib().gtsc_batch_set_schedule(self.handle, 1 if persistent else 0), "batch_set_schedule")
+
+    def schedule(self):
+        return "persistent" if lib().gtsc_batch_schedule(self.handle) == 1 else "levels"
 
     def profile(self, compress=True):
         """One step launch by launch: [(pass name, ms, bytes moved at least, blocks)]."""

@@ -90,6 +90,7 @@ struct Launch {
     int first, count;
     uint64_t tiles;
     uint64_t map_off;  // this launch's tile -> item table in the item_of array
+    int level;
 };
 
 // passes whose tiles chain through a decoupled look-back (claimed in order from a counter)
@@ -118,7 +119,17 @@ public:
     std::vector<BNodeDev> nodes_c, nodes_d;  // framing (compress) / parse (decode) node tables
     std::vector<Pass> pass_c, pass_d;
     std::vector<BItem> items_c, items_d, items_copy;
+    std::vector<int> item_col_c, item_col_d;  // each item's column
     std::vector<Launch> launch_c, launch_d;
+    // the persistent schedule (batch.hpp, PLaunch) of each phase
+    std::vector<PLaunch> plaunch_c, plaunch_d;
+    std::vector<PItem> pitem_c, pitem_d;
+    uint32_t q_total_c = 0, q_total_d = 0;
+    PLaunch *d_plaunch_c = nullptr, *d_plaunch_d = nullptr;
+    PItem *d_pitem_c = nullptr, *d_pitem_d = nullptr;
+    uint32_t *d_done_c = nullptr, *d_done_d = nullptr, *d_ext_c = nullptr, *d_ext_d = nullptr;
+    uint32_t *d_queue = nullptr;  // [0] compress claim counter, [1] decode claim counter
+    bool persistent = false;      // the schedule the step graphs replay
     std::vector<uint32_t> item_of;           // tile -> item tables of every launch, back to back
     uint64_t copy_map_off = 0;
     uint32_t *d_item_of = nullptr;
@@ -139,7 +150,7 @@ public:
     uint32_t *d_status = nullptr, *d_counters = nullptr;
     uint8_t *d_framed = nullptr;
     int n_counters = 0;
-    cudaGraphExec_t graph_c = nullptr, graph_d = nullptr;
+    cudaGraphExec_t graph_c[2] = {nullptr, nullptr}, graph_d[2] = {nullptr, nullptr};  // [persistent]
 
     int new_stream(uint64_t cap)
     {
@@ -149,11 +160,16 @@ public:
 
     void build_node(const Tree &t, int &k, int col, int parent, int in_sid, uint64_t in_cap, int depth,
                     const int8_t *in_vop, const int *in_vnode);
+    int folded_minmax(int id) const;
     void plan_passes();
     void layout(cudaStream_t s);
     void capture(cudaStream_t s);
-    void record_compress(cudaStream_t s, const std::function<void(int)> &mark);
-    void record_decompress(cudaStream_t s, const std::function<void(int)> &mark);
+    void record_compress(cudaStream_t s, const std::function<void(int)> &mark, bool pers);
+    void record_decompress(cudaStream_t s, const std::function<void(int)> &mark, bool pers);
+    void plan_persistent(const std::vector<Launch> &launches, const std::vector<BItem> &items,
+                         const std::vector<int> &item_col, std::vector<PLaunch> &pl, std::vector<PItem> &pi,
+                         uint32_t &total);
+    PersistArgs persist_args(bool compress) const;
 };
 
 // ---------------------------------------------------------------------------------- compile
@@ -231,6 +247,25 @@ void BatchEngine::build_node(const Tree &t, int &k, int col, int parent, int in_
         return;
     }
     for (int j = 0; j < r; j++) build_node(t, k, col, id, nodes[id].out_sid[j + 1], cap[j + 1], depth + 1, nullptr, nullptr);
+}
+
+// A node packed by AFL whose min / max its parent's split accumulates while it writes the child's
+// input stream, so that the child needs no min/max pass of its own (one read of that stream less):
+// the patch outputs, the const node's unmatched values and the dictionary's unmatched values.
+// Returns the parent's split output (1 = the matches, 2 = the rest) or 0.
+int BatchEngine::folded_minmax(int id) const
+{
+    const HNode &nd = nodes[id];
+    if (nd.parent < 0 || nd.virt || view_ops(nd.vop) != 0) return 0;
+    if (!(nd.enc == GTSC_AFL || (nd.enc == GTSC_GFC && !is_fp(nd.dt)))) return 0;
+    const HNode &par = nodes[nd.parent];
+    const int slot = (int)(std::find(par.kids.begin(), par.kids.end(), id) - par.kids.begin()) + 1;
+    switch (par.enc) {
+    case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: return slot;
+    case GTSC_CONST: return slot == 1 ? 1 : 0;
+    case GTSC_DICT: return slot == 2 ? 2 : 0;
+    default: return 0;
+    }
 }
 
 void BatchEngine::plan_passes()
@@ -329,6 +364,14 @@ void BatchEngine::plan_passes()
         auto add = [&](BItem it) { ps.push_back(it); };
         const int nops = view_ops(nd.vop);
         const bool scale_view = nops > 0 && nd.vop[nops - 1] == V_SCALE;
+        // split items: p[2] / p[3] = 1 + the node whose min/max the matches / the rest feed (0 =
+        // none); layout() turns them into that node's scratch address
+        auto set_folds = [&](BItem &sp) {
+            for (int kid : nd.kids) {
+                const int slot = folded_minmax(kid);
+                if (slot) sp.p[1 + slot] = (uint64_t)kid + 1;
+            }
+        };
         if (nd.virt) {
             // delta: metadata only, the child can start at once; scale: min/max, then metadata
             BItem vm = base_item(nd, B_VMETA, 1);
@@ -355,7 +398,7 @@ void BatchEngine::plan_passes()
         case GTSC_AFL: {
             BItem pk = base_item(nd, B_AFL_PACK, t2k);
             if (scale_view) pk.vflags |= 1;  // width from the scale's min / max: no min/max pass
-            else add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+            else if (!folded_minmax((int)id)) add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
             add(pk);
             break;
         }
@@ -368,6 +411,7 @@ void BatchEngine::plan_passes()
             sp.mode = SPLIT_LOWER;
             sp.p[0] = 64;
             sp.p[1] = nd.enc == GTSC_PATCH_OUTSIDE;  // the outside variant's stencil
+            set_folds(sp);
             add(sp);
             break;
         }
@@ -388,6 +432,7 @@ void BatchEngine::plan_passes()
             sp.order = (int16_t)native_order(nd.dt);
             sp.mode = (int16_t)(nd.enc == GTSC_DICT ? SPLIT_DICT : SPLIT_NOT_CONST);
             sp.p[0] = 64;
+            set_folds(sp);
             add(sp);
             break;
         }
@@ -433,7 +478,7 @@ void BatchEngine::plan_passes()
             } else {
                 BItem pk = base_item(nd, B_AFL_PACK, t2k);
                 if (scale_view) pk.vflags |= 1;
-                else add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+                else if (!folded_minmax((int)id)) add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
                 add(pk);
             }
             break;
@@ -610,16 +655,20 @@ void BatchEngine::layout(cudaStream_t s)
         }
 
     // items: patch scratch offsets into device addresses, group into launches
-    auto build = [&](std::vector<Pass> &ps, std::vector<BItem> &items, std::vector<Launch> &launches) {
+    auto build = [&](std::vector<Pass> &ps, std::vector<BItem> &items, std::vector<Launch> &launches,
+                     std::vector<int> &item_col) {
         std::stable_sort(ps.begin(), ps.end(), [](const Pass &a, const Pass &b) {
             return std::make_tuple(a.level, a.op) < std::make_tuple(b.level, b.op);
         });
         for (size_t i = 0; i < ps.size();) {
             size_t j = i;
-            Launch L{ps[i].op, (int)items.size(), 0, 0};
+            Launch L{ps[i].op, (int)items.size(), 0, 0, 0, ps[i].level};
             while (j < ps.size() && ps[j].level == ps[i].level && ps[j].op == ps[i].op) {
                 BItem it = ps[j].item;
                 it.scratch = A + nodes[ps[j].node].scratch;
+                if (ps[j].op == B_SPLIT)  // the children whose min / max the split accumulates
+                    for (int q = 2; q < 4; q++)
+                        it.p[q] = it.p[q] ? (uint64_t)(uintptr_t)(A + nodes[it.p[q] - 1].scratch) : 0;
                 if (ps[j].op < B_NONE_COPY || ps[j].op == B_VMETA)  // compress passes: the view's scale nodes
                     for (int v = 0; v < kMaxViewOps; v++) {
                         const int sn = nodes[ps[j].node].vnode[v];
@@ -628,6 +677,7 @@ void BatchEngine::layout(cudaStream_t s)
                 it.tile_base = L.tiles;
                 L.tiles += it.tiles;
                 items.push_back(it);
+                item_col.push_back(nodes[ps[j].node].col);
                 j++;
             }
             L.count = (int)items.size() - L.first;
@@ -654,8 +704,10 @@ void BatchEngine::layout(cudaStream_t s)
             i = j;
         }
     };
-    build(pass_c, items_c, launch_c);
-    build(pass_d, items_d, launch_d);
+    build(pass_c, items_c, launch_c, item_col_c);
+    build(pass_d, items_d, launch_d, item_col_d);
+    plan_persistent(launch_c, items_c, item_col_c, plaunch_c, pitem_c, q_total_c);
+    plan_persistent(launch_d, items_d, item_col_d, plaunch_d, pitem_d, q_total_d);
 
     // zero ranges per step
     auto zr = [](std::vector<unsigned long long> &z, uint8_t *p, uint64_t bytes) {
@@ -743,6 +795,16 @@ void BatchEngine::layout(cudaStream_t s)
     const uint64_t o_status = t_off; t_off += 256;
     const uint64_t o_counters = t_off; t_off += sz(n_counters, 4);
     const uint64_t o_item_of = t_off; t_off += sz(item_of.size(), 4);
+    const uint64_t ncol = col_root.size();
+    const uint64_t o_plc = t_off; t_off += sz(plaunch_c.size(), sizeof(PLaunch));
+    const uint64_t o_pld = t_off; t_off += sz(plaunch_d.size(), sizeof(PLaunch));
+    const uint64_t o_pic = t_off; t_off += sz(pitem_c.size(), sizeof(PItem));
+    const uint64_t o_pid = t_off; t_off += sz(pitem_d.size(), sizeof(PItem));
+    const uint64_t o_done_c = t_off; t_off += sz(ncol, 4);
+    const uint64_t o_done_d = t_off; t_off += sz(ncol, 4);
+    const uint64_t o_ext_c = t_off; t_off += sz(items_c.size(), 4);
+    const uint64_t o_ext_d = t_off; t_off += sz(items_d.size(), 4);
+    const uint64_t o_queue = t_off; t_off += 256;
     tables = dev_alloc(t_off, s);
     uint8_t *T = tables.get();
     GTSC_CUDA(cudaMemsetAsync(T, 0, t_off, s));
@@ -765,11 +827,27 @@ void BatchEngine::layout(cudaStream_t s)
     d_status = (uint32_t *)(T + o_status);
     d_counters = (uint32_t *)(T + o_counters);
     d_item_of = (uint32_t *)(T + o_item_of);
+    d_plaunch_c = (PLaunch *)(T + o_plc);
+    d_plaunch_d = (PLaunch *)(T + o_pld);
+    d_pitem_c = (PItem *)(T + o_pic);
+    d_pitem_d = (PItem *)(T + o_pid);
+    d_done_c = (uint32_t *)(T + o_done_c);
+    d_done_d = (uint32_t *)(T + o_done_d);
+    d_ext_c = (uint32_t *)(T + o_ext_c);
+    d_ext_d = (uint32_t *)(T + o_ext_d);
+    d_queue = (uint32_t *)(T + o_queue);
     // the status word and the counters are zeroed with the other ranges at each step
     zr(zero_c, (uint8_t *)d_status, 8);   // [0] error code, [1] decode: the frames did not parse
     zr(zero_d, (uint8_t *)d_status, 8);
     zr(zero_c, (uint8_t *)d_counters, 4ull * n_counters);
     zr(zero_d, (uint8_t *)d_counters, 4ull * n_counters);
+    // the persistent schedule's per-column progress, extent cache and claim counters
+    zr(zero_c, (uint8_t *)d_done_c, 4 * ncol);
+    zr(zero_d, (uint8_t *)d_done_d, 4 * ncol);
+    zr(zero_c, (uint8_t *)d_ext_c, 4 * std::max<uint64_t>(items_c.size(), 1));
+    zr(zero_d, (uint8_t *)d_ext_d, 4 * std::max<uint64_t>(items_d.size(), 1));
+    zr(zero_c, (uint8_t *)d_queue, 4);
+    zr(zero_d, (uint8_t *)(d_queue + 1), 4);
     auto h2d = [&](void *dst, const void *src, size_t bytes) {
         if (bytes) GTSC_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
     };
@@ -783,13 +861,71 @@ void BatchEngine::layout(cudaStream_t s)
     h2d(d_zero_c, zero_c.data(), zero_c.size() * 8);
     h2d(d_zero_d, zero_d.data(), zero_d.size() * 8);
     h2d(d_item_of, item_of.data(), item_of.size() * 4);
+    h2d(d_plaunch_c, plaunch_c.data(), plaunch_c.size() * sizeof(PLaunch));
+    h2d(d_plaunch_d, plaunch_d.data(), plaunch_d.size() * sizeof(PLaunch));
+    h2d(d_pitem_c, pitem_c.data(), pitem_c.size() * sizeof(PItem));
+    h2d(d_pitem_d, pitem_d.data(), pitem_d.size() * sizeof(PItem));
     GTSC_CUDA(cudaStreamSynchronize(s));
 }
 
-// Launch-sequence markers: the stage op, or one of these for the fixed kernels of a step.
-enum : int { M_SET = -1, M_ZERO = -2, M_FRAME_SIZES = -3, M_FRAME_LAYOUT = -4, M_FRAME_COPY = -5, M_PARSE = -6 };
+// The persistent schedule of one phase (batch.hpp, PLaunch): the level launches end to end as one
+// queue, and per item its column and the number of that column's entries in earlier levels.
+void BatchEngine::plan_persistent(const std::vector<Launch> &launches, const std::vector<BItem> &items,
+                                  const std::vector<int> &item_col, std::vector<PLaunch> &pl,
+                                  std::vector<PItem> &pi, uint32_t &total)
+{
+    const size_t nc = col_root.size();
+    std::vector<uint64_t> tot(nc, 0), before(nc, 0);  // entries so far / in the earlier levels
+    pi.assign(items.size(), PItem{0, 0});
+    uint64_t q = 0;
+    int level = INT32_MIN;
+    for (const Launch &L : launches) {
+        if (L.level != level) {  // launches are sorted by level
+            before = tot;
+            level = L.level;
+        }
+        PLaunch p;
+        p.op = L.op;
+        p.first = L.first;
+        p.tiles = (uint32_t)L.tiles;
+        p.map_off = (uint32_t)L.map_off;
+        p.qstart = (uint32_t)q;
+        p.dyn = dyn_pass(L.op) ? 1 : 0;
+        pl.push_back(p);
+        q += L.tiles;
+        for (int k = L.first; k < L.first + L.count; k++) {
+            const int c = item_col[k];
+            if (before[c] > 0xffffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles for the persistent schedule");
+            pi[k] = PItem{(uint32_t)c, (uint32_t)before[c]};
+            tot[c] += items[k].tiles;
+        }
+    }
+    if (q >= 0xffffffffull - kPersistChunk) fail(GTSC_ERR_CAPACITY, "batch: too many tiles for the persistent schedule");
+    total = (uint32_t)q;
+}
 
-void BatchEngine::record_compress(cudaStream_t s, const std::function<void(int)> &mark)
+PersistArgs BatchEngine::persist_args(bool compress) const
+{
+    PersistArgs a;
+    a.launches = compress ? d_plaunch_c : d_plaunch_d;
+    a.n_launches = (int)(compress ? plaunch_c.size() : plaunch_d.size());
+    a.total = compress ? q_total_c : q_total_d;
+    a.items = compress ? d_items_c : d_items_d;
+    a.pitems = compress ? d_pitem_c : d_pitem_d;
+    a.item_of = d_item_of;
+    a.done = compress ? d_done_c : d_done_d;
+    a.ext = compress ? d_ext_c : d_ext_d;
+    a.qcounter = d_queue + (compress ? 0 : 1);
+    a.S = d_streams;
+    a.status = d_status;
+    return a;
+}
+
+// Launch-sequence markers: the stage op, or one of these for the fixed kernels of a step.
+enum : int { M_SET = -1, M_ZERO = -2, M_FRAME_SIZES = -3, M_FRAME_LAYOUT = -4, M_FRAME_COPY = -5, M_PARSE = -6,
+             M_PERSIST = -7 };
+
+void BatchEngine::record_compress(cudaStream_t s, const std::function<void(int)> &mark, bool pers)
 {
     const int nc = (int)col_root.size();
     k_set_streams<<<(nc + 127) / 128, 128, 0, s>>>(d_set_vals, d_set_sids, nc, d_streams);
@@ -797,11 +933,16 @@ void BatchEngine::record_compress(cudaStream_t s, const std::function<void(int)>
     mark(M_SET);
     launch_zero_ranges(d_zero_c, (int)zero_c.size() / 2, s);
     mark(M_ZERO);
-    int ctr = 0;
-    for (auto &L : launch_c) {
-        launch_batch_stage(L.op, d_items_c + L.first, d_item_of + L.map_off, L.count, L.tiles, d_streams,
-                           d_counters + ctr++, d_status, s);
-        mark(L.op);
+    if (pers) {
+        launch_batch_persistent_c(persist_args(true), s);
+        mark(M_PERSIST);
+    } else {
+        int ctr = 0;
+        for (auto &L : launch_c) {
+            launch_batch_stage(L.op, d_items_c + L.first, d_item_of + L.map_off, L.count, L.tiles, d_streams,
+                               d_counters + ctr++, d_status, s);
+            mark(L.op);
+        }
     }
     launch_frame_sizes(d_cols, nc, d_nodes_c, d_streams, d_col_off, d_total, d_framed, s);
     mark(M_FRAME_SIZES);
@@ -812,7 +953,7 @@ void BatchEngine::record_compress(cudaStream_t s, const std::function<void(int)>
     mark(M_FRAME_COPY);
 }
 
-void BatchEngine::record_decompress(cudaStream_t s, const std::function<void(int)> &mark)
+void BatchEngine::record_decompress(cudaStream_t s, const std::function<void(int)> &mark, bool pers)
 {
     const int nc = (int)col_root.size();
     k_set_streams<<<(nc + 127) / 128, 128, 0, s>>>(d_set_vals + 2 * nc, d_set_sids + nc, nc, d_streams);
@@ -823,6 +964,11 @@ void BatchEngine::record_decompress(cudaStream_t s, const std::function<void(int
     launch_parse_frames(d_cols, nc, d_nodes_d, d_streams, d_col_off_d, (const uint8_t *const *)d_frame_ptr,
                         d_frame_len, d_status, s);
     mark(M_PARSE);
+    if (pers) {
+        launch_batch_persistent_d(persist_args(false), s);
+        mark(M_PERSIST);
+        return;
+    }
     int ctr = (int)launch_c.size();
     for (auto &L : launch_d) {
         launch_batch_stage(L.op, d_items_d + L.first, d_item_of + L.map_off, L.count, L.tiles, d_streams,
@@ -833,12 +979,13 @@ void BatchEngine::record_decompress(cudaStream_t s, const std::function<void(int
 
 void BatchEngine::capture(cudaStream_t s)
 {
-    for (int which = 0; which < 2; which++) {
+    for (int which = 0; which < 4; which++) {
+        const bool comp = which % 2 == 0, pers = which >= 2;
         cudaGraph_t g;
         GTSC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         try {
-            if (which == 0) record_compress(s, [](int) {});
-            else record_decompress(s, [](int) {});
+            if (comp) record_compress(s, [](int) {}, pers);
+            else record_decompress(s, [](int) {}, pers);
         } catch (...) {
             cudaGraph_t junk;
             cudaStreamEndCapture(s, &junk);
@@ -849,7 +996,7 @@ void BatchEngine::capture(cudaStream_t s)
         cudaGraphExec_t ex;
         GTSC_CUDA(cudaGraphInstantiate(&ex, g, 0));
         cudaGraphDestroy(g);
-        (which == 0 ? graph_c : graph_d) = ex;
+        (comp ? graph_c : graph_d)[pers ? 1 : 0] = ex;
     }
 }
 
@@ -903,12 +1050,17 @@ void batch_destroy(BatchEngine *e)
     cudaDeviceSynchronize();
     e->arena.release_on_default_stream();
     e->tables.release_on_default_stream();
-    if (e->graph_c) cudaGraphExecDestroy(e->graph_c);
-    if (e->graph_d) cudaGraphExecDestroy(e->graph_d);
+    for (int k = 0; k < 2; k++) {
+        if (e->graph_c[k]) cudaGraphExecDestroy(e->graph_c[k]);
+        if (e->graph_d[k]) cudaGraphExecDestroy(e->graph_d[k]);
+    }
     delete e;
 }
 
-void batch_compress(BatchEngine *e, cudaStream_t s) { GTSC_CUDA(cudaGraphLaunch(e->graph_c, s)); }
+void batch_compress(BatchEngine *e, cudaStream_t s) { GTSC_CUDA(cudaGraphLaunch(e->graph_c[e->persistent], s)); }
+
+void batch_set_schedule(BatchEngine *e, bool persistent) { e->persistent = persistent; }
+bool batch_schedule(const BatchEngine *e) { return e->persistent; }
 
 void batch_set_inputs(BatchEngine *e, const std::vector<const void *> &inputs, cudaStream_t s)
 {
@@ -956,7 +1108,7 @@ void batch_decompress(BatchEngine *e, const uint8_t *framed, uint64_t framed_byt
     GTSC_CUDA(cudaMemcpyAsync(e->d_set_vals + 2 * nc, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, s));
     unsigned long long fr[2] = {(unsigned long long)(uintptr_t)framed, framed_bytes};
     GTSC_CUDA(cudaMemcpyAsync(e->d_frame_ptr, fr, 16, cudaMemcpyHostToDevice, s));
-    GTSC_CUDA(cudaGraphLaunch(e->graph_d, s));
+    GTSC_CUDA(cudaGraphLaunch(e->graph_d[e->persistent], s));
 }
 
 // Bytes a pass must move at least: its inputs read and its outputs written (from the stream table
@@ -1008,8 +1160,8 @@ std::vector<BatchLaunchProfile> batch_profile(BatchEngine *e, bool compress, cud
             marks.push_back(m);
             GTSC_CUDA(cudaEventRecord(new_event(), s));
         };
-        if (compress) e->record_compress(s, mark);
-        else e->record_decompress(s, mark);
+        if (compress) e->record_compress(s, mark, e->persistent);
+        else e->record_decompress(s, mark, e->persistent);
         GTSC_CUDA(cudaStreamSynchronize(s));
         std::vector<StreamDesc> S(e->streams.size());
         d2h(S.data(), e->d_streams, S.size() * sizeof(StreamDesc), s);
@@ -1029,6 +1181,9 @@ std::vector<BatchLaunchProfile> batch_profile(BatchEngine *e, bool compress, cud
             } else if (marks[k] == M_FRAME_COPY) {
                 p.bytes = 2 * total;
                 p.blocks = e->copy_tiles;
+            } else if (marks[k] == M_PERSIST) {  // every pass of the step in one launch
+                for (const BItem &it : compress ? e->items_c : e->items_d) p.bytes += item_bytes(it, S);
+                p.blocks = compress ? e->q_total_c : e->q_total_d;
             }
             out.push_back(p);
         }
@@ -1051,6 +1206,7 @@ int batch_launches(BatchEngine *e, bool compress)
 {
     // compress: set streams, zero, stages, frame sizes / layout / copy; decompress: set streams,
     // zero, parse directory + frames, stages
+    if (e->persistent) return compress ? 6 : 4;
     return compress ? (int)e->launch_c.size() + 5 : (int)e->launch_d.size() + 4;
 }
 

@@ -141,6 +141,10 @@ void batch_decompress(BatchEngine *e, const uint8_t *framed, uint64_t framed_byt
 gtsc_status batch_status(BatchEngine *e, cudaStream_t s);
 // number of kernel launches in one compress / decompress step
 int batch_launches(BatchEngine *e, bool compress);
+// the schedule the steps replay: a launch per (level, pass kind), or one persistent launch per step
+// pulling tiles from a device queue (both are captured at creation; the default is the levels)
+void batch_set_schedule(BatchEngine *e, bool persistent);
+bool batch_schedule(const BatchEngine *e);
 // one step run launch by launch with events between launches: per launch its pass kind (a BOp, or
 // a negative code for the fixed kernels), its time and the bytes it must move at least
 struct BatchLaunchProfile {
@@ -164,6 +168,48 @@ gtsc_status pipeline_decompress(Pipeline *p);
 const void *pipeline_column_input(Pipeline *p, int c);
 const void *pipeline_column_output(Pipeline *p, int c);
 
+// ---- the persistent schedule: one launch per step whose blocks pull work from a device queue
+//
+// The queue is the level schedule laid end to end: entry e belongs to launch L when
+// qstart[L] <= e < qstart[L] + tiles[L], and names that launch's tile (or, for look-back passes,
+// its claim-order tile) exactly as the stage launch would.  A block claims kPersistChunk
+// consecutive entries at a time and runs them in order.  An item waits, before its first tile,
+// until its column has finished every entry of the earlier levels (done[col] >= wait): passes of
+// different columns never depend on one another, and a level only follows levels of its own
+// column, so small columns run ahead instead of waiting at every level for the largest ones.
+// Every entry depends only on lower entries (look-back predecessors come earlier in claim order,
+// earlier levels earlier in the queue), so the lowest unfinished entry can always run and the
+// resident blocks always make progress; each wait is still bounded (GTSC_ERR_TIMEOUT).
+struct PLaunch {
+    int32_t op;
+    int32_t first;      // first item of the launch in the phase's item table
+    uint32_t tiles;     // entries (the launch's tiles)
+    uint32_t map_off;   // its tile -> item table in item_of; look-back passes: claim order after it
+    uint32_t qstart;    // its first queue entry
+    int32_t dyn;        // a look-back pass (tiles in claim order)
+};
+struct PItem {
+    uint32_t col;       // the item's column
+    uint32_t wait;      // entries of that column in earlier levels
+};
+struct PersistArgs {
+    const PLaunch *launches;
+    int n_launches;
+    uint32_t total;     // queue entries
+    const BItem *items;
+    const PItem *pitems;
+    const uint32_t *item_of;
+    uint32_t *done;     // per column: entries finished (zeroed each step)
+    uint32_t *ext;      // per item: 1 + its extent in tiles once a block computed it (zeroed)
+    uint32_t *qcounter; // the claim counter (zeroed)
+    StreamDesc *S;
+    uint32_t *status;
+};
+constexpr uint32_t kPersistChunk = 4;  // queue entries claimed at a time
+// one persistent launch of a whole compress (batch_kernels.cu) or decode (batch_decode.cu) step
+void launch_batch_persistent_c(const PersistArgs &a, cudaStream_t s);
+void launch_batch_persistent_d(const PersistArgs &a, cudaStream_t s);
+
 // stage launcher (batch_kernels.cu / batch_decode.cu): one launch of `total_tiles` blocks;
 // d_item_of[t] = the item (index into d_items) of tile t
 void launch_batch_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items, uint64_t total_tiles,
@@ -178,6 +224,7 @@ constexpr uint32_t kBMergeSub = 4;      // kBTile tiles per block of the merge p
 constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
 constexpr uint32_t kBHistSmem = 2048;    // shared hash slots of a histogram block (8-byte values)
 constexpr uint32_t kBHistPacked = 4096;  // the same for values of up to 4 bytes (packed slots)
+constexpr int kBHistPackedLog2 = 12;
 
 // scratch layout of a histogram item
 struct BHistHdr {

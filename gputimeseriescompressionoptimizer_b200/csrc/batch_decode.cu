@@ -4,7 +4,11 @@
 // Framed output: for every column, a uint64 blob length followed by the column's serialized tree
 // (the reference's per-column-chunk file framing, optimizer/compression_task.cpp:35-40, with
 // the blob of CompressionTree::Compress).
+// the persistent kernels here read, in later passes, what earlier passes of the same launch wrote
+#define GTSC_COHERENT_LOADS 1
 #include "batch_dev.cuh"
+
+#include <algorithm>
 
 namespace gtsc {
 
@@ -28,10 +32,10 @@ __device__ void block_copy(uint8_t *dst, const uint8_t *src, uint64_t n)
     uint32_t *dw = (uint32_t *)d;
     if (sh == 0) {
 #pragma unroll 4
-        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = __ldg(sw + k);
+        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = ldg(sw + k);
     } else {
 #pragma unroll 4
-        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = __funnelshift_r(__ldg(sw + k), __ldg(sw + k + 1), sh);
+        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = __funnelshift_r(ldg(sw + k), ldg(sw + k + 1), sh);
     }
     const uint64_t tail = (n - h) - 4 * words;
     if (threadIdx.x < tail) d[4 * words + threadIdx.x] = sp[4 * words + threadIdx.x];
@@ -301,6 +305,13 @@ k_merge_count(const BItem *items, const uint32_t *item_of, StreamDesc *S, const 
     }
 }
 
+// Shared staging of the merge and the RLE expansion, declared once at file scope: a __shared__
+// array inside a function template is one array per instantiation (per element size), which a
+// kernel running every pass kind for every element size could not hold.
+static __shared__ uint32_t s_merge_codes[kBTile / 16 + 2];              // the tile's dictionary code words
+static __shared__ uint16_t s_merge_bits[kBThreads], s_merge_excl[kBThreads];  // stencil bits, matches before
+static __shared__ uint16_t s_rle_end[kBTile + 2];                       // the tile's run ends
+
 template <int ES>
 __device__ void p_merge(const BItem &it, uint32_t stile, StreamDesc *S, uint32_t *status, uint8_t *sm)
 {
@@ -382,7 +393,7 @@ __device__ void p_merge(const BItem &it, uint32_t stile, StreamDesc *S, uint32_t
     const uint64_t ny = total, nn = tile_n - ny;
     const uint64_t yes0 = prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
     // dictionary: the code words of the tile's matches, staged once (coalesced, whole words)
-    __shared__ uint32_t s_codes[kBTile / 16 + 2];
+    uint32_t *s_codes = s_merge_codes;
     const uint64_t w0 = yes0 >> 4;
     if (mode == SPLIT_DICT && ny) {
         const uint64_t nw = ((yes0 + ny + 15) >> 4) - w0;
@@ -390,7 +401,7 @@ __device__ void p_merge(const BItem &it, uint32_t stile, StreamDesc *S, uint32_t
         const bool al = ((uintptr_t)codes & 3) == 0;
         for (uint64_t k = threadIdx.x; k < nw; k += kBThreads) {
             const uint64_t w = w0 + k;
-            s_codes[k] = w >= avail ? 0u : al ? __ldg((const uint32_t *)codes + w) : (uint32_t)ld_unaligned<4>(codes + 4 * w);
+            s_codes[k] = w >= avail ? 0u : al ? ldg((const uint32_t *)codes + w) : (uint32_t)ld_unaligned<4>(codes + 4 * w);
         }
     }
     // in-tile counts fit 32 bits; a stream position past the stream's end is corrupt input
@@ -406,7 +417,7 @@ __device__ void p_merge(const BItem &it, uint32_t stile, StreamDesc *S, uint32_t
         stage_view<ES>(v2, no0, ok, sm, ny32);
     }
     // every thread's 16 stencil bits and the matches before them, for the striped assembly below
-    __shared__ uint16_t s_bits[kBThreads], s_excl[kBThreads];
+    uint16_t *s_bits = s_merge_bits, *s_excl = s_merge_excl;
     s_bits[threadIdx.x] = (uint16_t)bits;
     s_excl[threadIdx.x] = (uint16_t)excl;
     __syncthreads();
@@ -508,7 +519,7 @@ template <int ES>
 __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
 {
     // the tile's run ends relative to its first element, clamped to kBTile (at most kBTile + 1 runs)
-    __shared__ uint16_t s_end[kBTile + 2];
+    uint16_t *s_end = s_rle_end;
     bool ok;
     const DViewCtx values = dview_ctx<ES>(it, S, 2, ok);
     StreamDesc &out = S[it.out[0]];
@@ -905,6 +916,49 @@ __device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDe
 #undef GTSC_ES_SWITCH
 }
 
+// ------------------------------------------------------------------------------- persistent step
+constexpr size_t kPersistSmemD = 8 * kBTile > kGfcRing * (kBThreads / 32) ? 8 * kBTile : kGfcRing * (kBThreads / 32);
+
+__device__ __forceinline__ uint32_t persist_extent_d(int op, const BItem &it, const StreamDesc *S)
+{
+    switch (op) {
+    case B_AFL_UNPACK: return dec_extent<B_AFL_UNPACK>(it, S);
+    case B_SCALE_ADD: return dec_extent<B_SCALE_ADD>(it, S);
+    case B_F2I_DEC: return dec_extent<B_F2I_DEC>(it, S);
+    case B_RLE_EXPAND: return dec_extent<B_RLE_EXPAND>(it, S);
+    case B_MERGE_COUNT: return dec_extent<B_MERGE_COUNT>(it, S);
+    default: return it.tiles;
+    }
+}
+
+// The whole decode step in one launch (batch.hpp, PLaunch); the merges' counting pass is the
+// queue's first launch.
+__global__ void __launch_bounds__(kBThreads, 4) k_bpersist_d(PersistArgs a)
+{
+    __shared__ __align__(16) unsigned char smem[kPersistSmemD];
+    if (*(volatile uint32_t *)(a.status + 1)) return;  // the frames did not parse
+    persist_loop(
+        a, [](int op, const BItem &it, const StreamDesc *S) { return persist_extent_d(op, it, S); },
+        [&](int op, const BItem &it, uint32_t tile) {
+            switch (op) {
+#define GTSC_RUN(OPC) case OPC: run_dec<OPC>(it, tile, a.S, a.status, smem); break;
+                GTSC_RUN(B_NONE_COPY)
+                GTSC_RUN(B_AFL_UNPACK)
+                GTSC_RUN(B_DELTA_DEC)
+                GTSC_RUN(B_SCALE_ADD)
+                GTSC_RUN(B_MERGE)
+                GTSC_RUN(B_MERGE_COUNT)
+                GTSC_RUN(B_RLE_SCAN)
+                GTSC_RUN(B_RLE_EXPAND)
+                GTSC_RUN(B_F2I_DEC)
+                GTSC_RUN(B_GFC_SIZES)
+                GTSC_RUN(B_GFC_DEC)
+#undef GTSC_RUN
+            default: set_status(a.status, GTSC_ERR_ARG); break;
+            }
+        });
+}
+
 // ------------------------------------------------------------------------------- framing
 // Framed buffer: uint64 column count C, uint64 blob bytes of every column (the directory), then the
 // C blobs back to back.  The directory lets decode find every column without walking the blobs.
@@ -1151,6 +1205,17 @@ void launch_parse_frames(const BColumnDev *cols, int ncols, const BNodeDev *node
     k_parse_directory<<<1, kBThreads, 0, s>>>(ncols, col_off, framed_p, framed_bytes_p, status);
     GTSC_CUDA(cudaGetLastError());
     k_parse_frames<<<(ncols + 127) / 128, 128, 0, s>>>(cols, ncols, nodes, S, col_off, framed_p, status);
+    GTSC_CUDA(cudaGetLastError());
+}
+
+void launch_batch_persistent_d(const PersistArgs &a, cudaStream_t s)
+{
+    if (a.total == 0) return;
+    int per_sm = 0;
+    GTSC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bpersist_d, kBThreads, 0));
+    const uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * (uint64_t)sm_count(),
+                                             (a.total + kPersistChunk - 1) / kPersistChunk);
+    k_bpersist_d<<<(unsigned)grid, kBThreads, 0, s>>>(a);
     GTSC_CUDA(cudaGetLastError());
 }
 

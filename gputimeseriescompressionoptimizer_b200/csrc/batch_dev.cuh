@@ -444,9 +444,103 @@ __device__ __forceinline__ const BItem &shared_item(const BItem *items, uint32_t
     static_assert(sizeof(BItem) % 8 == 0, "BItem is copied in 8-byte words");
     constexpr int W = (int)(sizeof(BItem) / 8);
     if (threadIdx.x < W)
-        s_item_words[threadIdx.x] = __ldg((const unsigned long long *)(items + k) + threadIdx.x);
+        s_item_words[threadIdx.x] = ldg((const unsigned long long *)(items + k) + threadIdx.x);
     __syncthreads();
     return shared_item_ref();
+}
+
+// ------------------------------------------------------------------------------- persistent step
+// Helpers of the persistent kernels (batch.hpp, PLaunch); all of them run on thread 0 of a block.
+
+// the launch holding queue entry e: the last launch whose first entry is <= e
+__device__ __forceinline__ int persist_launch_of(const PersistArgs &a, uint32_t e)
+{
+    int lo = 0, hi = a.n_launches - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.launches[mid].qstart <= e) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// waits until the item's column has finished the entries of its earlier levels; bounded: gives up
+// with GTSC_ERR_TIMEOUT after kSpinLimit polls, or at once when another block recorded an error
+__device__ __forceinline__ void persist_wait(const PersistArgs &a, const PItem &pi)
+{
+    uint32_t spins = 0;
+    while (*(volatile const uint32_t *)(a.done + pi.col) < pi.wait) {
+        if (*(volatile const uint32_t *)a.status != 0u) break;
+        if (++spins > kSpinLimit) {
+            set_status(a.status, GTSC_ERR_TIMEOUT);
+            break;
+        }
+        __nanosleep(spins < 64 ? 32 : 256);
+    }
+    __threadfence();  // acquire: what the earlier levels wrote is visible to this block from here
+}
+
+// counts `pend` finished entries of `item` (after the block's barrier behind its last tile)
+__device__ __forceinline__ void persist_flush(const PersistArgs &a, int item, uint32_t &pend)
+{
+    if (item >= 0 && pend) {
+        __threadfence();  // release: this block's writes before the count
+        atomicAdd(a.done + a.pitems[item].col, pend);
+    }
+    pend = 0;
+}
+
+// The persistent loop shared by the compress and the decode kernel.  EXTENT(op, item, S) gives an
+// item's tiles that do work (the level schedule's persistent passes skip the others), RUN(op,
+// item, tile) runs one tile.
+template <class Extent, class Run>
+__device__ __forceinline__ void persist_loop(const PersistArgs &a, Extent extent, Run run)
+{
+    __shared__ uint32_t s_e0, s_tile, s_ext;
+    __shared__ int s_item, s_op, s_new;
+    int cur = -1;       // thread 0: the item whose entries it is counting
+    uint32_t pend = 0;  // thread 0: finished entries of cur not counted yet
+    for (;;) {
+        if (threadIdx.x == 0) s_e0 = atomicAdd(a.qcounter, kPersistChunk);
+        __syncthreads();
+        const uint32_t e0 = s_e0;
+        if (e0 >= a.total) break;
+        const uint32_t e1 = e0 + kPersistChunk < a.total ? e0 + kPersistChunk : a.total;
+        for (uint32_t e = e0; e < e1; e++) {
+            if (threadIdx.x == 0) {
+                const PLaunch &pl = a.launches[persist_launch_of(a, e)];
+                const uint32_t local = e - pl.qstart;
+                const uint32_t t = pl.dyn ? a.item_of[pl.map_off + pl.tiles + local] : local;
+                const int gi = pl.first + (int)a.item_of[pl.map_off + t];
+                s_new = gi != cur;
+                if (gi != cur) {
+                    persist_flush(a, cur, pend);
+                    persist_wait(a, a.pitems[gi]);
+                    cur = gi;
+                }
+                s_item = gi;
+                s_op = pl.op;
+                s_tile = t - (uint32_t)a.items[gi].tile_base;
+            }
+            __syncthreads();
+            if (s_new) shared_item(a.items, (uint32_t)s_item);
+            const BItem &it = shared_item_ref();
+            if (threadIdx.x == 0) {
+                // the extent is cached per item (a stale read only recomputes the same value)
+                uint32_t x = a.ext[s_item];
+                if (x == 0) {
+                    x = 1 + extent(s_op, it, a.S);
+                    a.ext[s_item] = x;
+                }
+                s_ext = x - 1;
+            }
+            __syncthreads();
+            if (s_tile < s_ext && s_tile < it.tiles) run(s_op, it, s_tile);
+            __syncthreads();  // the next entry reuses the shared memory and the descriptor
+            if (threadIdx.x == 0) ++pend;
+        }
+    }
+    if (threadIdx.x == 0) persist_flush(a, cur, pend);
 }
 
 template <bool DYN>

@@ -6,6 +6,8 @@
 // look-back of scan.cuh, per item.  Every pass reads its input length from the stream table and
 // writes its outputs' lengths there; tile 0 (or the tile that ends the input) writes metadata.
 // Byte layouts are the per-encoding ones of encodings.cu (and of the reference).
+// the persistent kernels here read, in later passes, what earlier passes of the same launch wrote
+#define GTSC_COHERENT_LOADS 1
 #include "batch_dev.cuh"
 
 #include <algorithm>
@@ -340,7 +342,7 @@ __device__ __forceinline__ HTab htab(const BItem &it)
     return t;
 }
 
-__device__ void g_insert(const HTab &t, unsigned long long key, unsigned int c, uint32_t *status)
+__device__ __noinline__ void g_insert(const HTab &t, unsigned long long key, unsigned int c, uint32_t *status)
 {
     constexpr unsigned long long EMPTY = ~0ull;
     if (key == EMPTY) {
@@ -387,7 +389,8 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         for (uint64_t w = t0 / 16 + threadIdx.x; w < (e_end + 15) / 16; w += kBThreads) words[w] = 0u;
     }
     unsigned long long nan_min[4] = {EMPTY, EMPTY, EMPTY, EMPTY};
-    if (ES <= 4 && t0 < n) {
+    if constexpr (ES <= 4) {
+      if (t0 < n) {
         // values of up to 4 bytes: 32-bit keys and counts (twice the slots of the layout below); a
         // value already in the table costs a plain key read and one 32-bit atomicAdd.  0xffffffff
         // marks an empty slot, so that value itself is counted apart.
@@ -401,55 +404,97 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         if (threadIdx.x == 0) s_ones = 0;
         __syncthreads();
         const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
-        // the next element's load is in flight while this one is inserted
-        unsigned long long next = t0 + threadIdx.x < end ? view_elem<ES>(it, vc, in.ptr, t0 + threadIdx.x) : 0ull;
-        for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
-            const unsigned long long key = next;
-            if (i + kBThreads < end) next = view_elem<ES>(it, vc, in.ptr, i + kBThreads);
-            if (is_nan_bits(key, o)) {
-                unsigned long long k = order_key(key, ES, o);
+        // rounds of 8 consecutive values per thread (16 for bytes, one 16-byte vector): all of a
+        // round's loads (16-byte vectors where the stream allows) are issued before the first
+        // insert, so each thread keeps a whole run in flight instead of one element
+        constexpr int V = ES == 1 ? 16 : 8;
+        for (uint64_t r0 = t0; r0 < end; r0 += (uint64_t)kBThreads * V) {
+            const uint64_t b = r0 + (uint64_t)threadIdx.x * V;
+            uint32_t cur[V];
+            {
+                uint64_t w[V];
+                load_view<ES, V>(it, vc, in.ptr, b, w);
 #pragma unroll
-                for (int j = 0; j < 4; j++)
-                    if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
-                continue;
+                for (int j = 0; j < V; j++) cur[j] = (uint32_t)w[j];
             }
-            const uint32_t kk = (uint32_t)key;
-            if (kk == 0xffffffffu) {
-                atomicAdd(&s_ones, 1u);
-                continue;
+            // equal neighbours within the thread's run are counted once (constant and run-heavy
+            // columns would otherwise serialise on one shared counter): run lengths from the right
+            uint32_t runlen[V];
+#pragma unroll
+            for (int j = V - 1; j >= 0; j--) {
+                const bool more = j + 1 < V && b + j + 1 < end && cur[j + 1] == cur[j];
+                runlen[j] = more ? runlen[j + 1 < V ? j + 1 : j] + 1 : 1u;
             }
-            uint32_t h = (uint32_t)bhash(key) & (kBHistPacked - 1);
-            bool done = false;
-            for (int p = 0; p < 8; p++) {
-                uint32_t cur = ((volatile uint32_t *)k32)[h];
-                if (cur == 0xffffffffu) cur = atomicCAS(&k32[h], 0xffffffffu, kk);
-                if (cur == 0xffffffffu || cur == kk) {
-                    atomicAdd(&c32[h], 1u);
-                    done = true;
-                    break;
+#pragma unroll
+            for (int j = 0; j < V; j++) {
+                if (b + j >= end || (j > 0 && cur[j] == cur[j - 1])) continue;  // past the end / inside a run
+                const uint32_t kk = cur[j], c = runlen[j];
+                if (is_nan_bits(kk, o)) {
+                    for (uint32_t r = 0; r < c; r++) {
+                        unsigned long long k = order_key(kk, ES, o);
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            if (k < nan_min[q]) { const unsigned long long x = nan_min[q]; nan_min[q] = k; k = x; }
+                    }
+                    continue;
                 }
-                h = (h + 1) & (kBHistPacked - 1);
+                if (kk == 0xffffffffu) {
+                    atomicAdd(&s_ones, c);
+                    continue;
+                }
+                // multiplicative (Fibonacci) hash: the product's top 12 bits pick the slot
+                uint32_t h = (kk * 0x9E3779B1u) >> (32 - kBHistPackedLog2);
+                bool done = false;
+                for (int p = 0; p < 8; p++) {
+                    uint32_t cs = ((volatile uint32_t *)k32)[h];
+                    if (cs == 0xffffffffu) cs = atomicCAS(&k32[h], 0xffffffffu, kk);
+                    if (cs == 0xffffffffu || cs == kk) {
+                        atomicAdd(&c32[h], c);
+                        done = true;
+                        break;
+                    }
+                    h = (h + 1) & (kBHistPacked - 1);
+                }
+                if (!done) g_insert(t, (unsigned long long)kk, c, status);
             }
-            if (!done) g_insert(t, key, 1u, status);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < (int)kBHistPacked; i += kBThreads)
             if (k32[i] != 0xffffffffu) g_insert(t, (unsigned long long)k32[i], c32[i], status);
         if (threadIdx.x == 0 && s_ones) g_insert(t, 0xffffffffull, s_ones, status);
-    } else if (t0 < n) {
+      }
+    } else {
+      if (t0 < n) {
         for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads) {
             skeys[i] = EMPTY;
             scounts[i] = 0;
         }
         __syncthreads();
         const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
-        for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
-            const unsigned long long key = view_elem<ES>(it, vc, in.ptr, i);
-            if (is_nan_bits(key, o)) {
-                unsigned long long k = order_key(key, ES, o);
+        // rounds of 8 consecutive values per thread, loaded before the first insert
+        constexpr int V = 8;
+        for (uint64_t r0 = t0; r0 < end; r0 += (uint64_t)kBThreads * V) {
+          const uint64_t b = r0 + (uint64_t)threadIdx.x * V;
+          uint64_t cur[V];
+          load_view<ES, V>(it, vc, in.ptr, b, cur);
+          uint32_t runlen[V];  // equal neighbours are counted once (as in the narrow path)
 #pragma unroll
-                for (int j = 0; j < 4; j++)
-                    if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
+          for (int j = V - 1; j >= 0; j--) {
+            const bool more = j + 1 < V && b + j + 1 < end && cur[j + 1] == cur[j];
+            runlen[j] = more ? runlen[j + 1 < V ? j + 1 : j] + 1 : 1u;
+          }
+#pragma unroll
+          for (int j = 0; j < V; j++) {
+            if (b + j >= end || (j > 0 && cur[j] == cur[j - 1])) continue;
+            const unsigned long long key = cur[j];
+            const uint32_t c = runlen[j];
+            if (is_nan_bits(key, o)) {
+                for (uint32_t r = 0; r < c; r++) {
+                    unsigned long long k = order_key(key, ES, o);
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (k < nan_min[q]) { const unsigned long long x = nan_min[q]; nan_min[q] = k; k = x; }
+                }
                 continue;
             }
             bool done = false;
@@ -458,18 +503,20 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
                 for (int p = 0; p < 8; p++) {
                     const unsigned long long prev = atomicCAS(&skeys[h], EMPTY, key);
                     if (prev == EMPTY || prev == key) {
-                        atomicAdd(&scounts[h], 1u);
+                        atomicAdd(&scounts[h], c);
                         done = true;
                         break;
                     }
                     h = (h + 1) & (kBHistSmem - 1);
                 }
             }
-            if (!done) g_insert(t, key, 1u, status);
+            if (!done) g_insert(t, key, c, status);
+          }
         }
         __syncthreads();
         for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads)
             if (skeys[i] != EMPTY) g_insert(t, skeys[i], scounts[i], status);
+      }
     }
     // this tile's 4 smallest NaN sort keys
     for (int off = 16; off > 0; off >>= 1) {
@@ -676,6 +723,27 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     }
     const uint32_t valid_mask = base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
     const uint32_t yes_bits = bits & valid_mask;
+    if (it.p[2] | it.p[3]) {
+        // min / max of the matches and of the rest, for the AFL children that read them (integer
+        // order, as their own min/max pass would compute it)
+        uint64_t ymin = ~0ull, ymax = 0, nmin = ~0ull, nmax = 0;
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++) {
+            const uint64_t k = order_key(v[j], ES, ORD_INT);
+            const bool in = (valid_mask >> j) & 1u, y = (yes_bits >> j) & 1u;
+            if (in && y) { ymin = k < ymin ? k : ymin; ymax = k > ymax ? k : ymax; }
+            if (in && !y) { nmin = k < nmin ? k : nmin; nmax = k > nmax ? k : nmax; }
+        }
+        block_minmax(ymin, ymax);
+        block_minmax(nmin, nmax);
+        if (threadIdx.x == 0) {
+            MinMaxAcc *ay = (MinMaxAcc *)it.p[2], *an = (MinMaxAcc *)it.p[3];
+            if (ay && ymin != ~0ull) atomicMax(&ay->nkmin, (unsigned long long)~ymin);
+            if (ay && ymax != 0) atomicMax(&ay->kmax, (unsigned long long)ymax);
+            if (an && nmin != ~0ull) atomicMax(&an->nkmin, (unsigned long long)~nmin);
+            if (an && nmax != 0) atomicMax(&an->kmax, (unsigned long long)nmax);
+        }
+    }
     unsigned long long total;
     const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(yes_bits), ws, total);
     if (threadIdx.x < 32) {
@@ -1188,10 +1256,10 @@ __device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint
     const uint32_t *sw = (const uint32_t *)((uintptr_t)sp & ~(uintptr_t)3);
     if (sh == 0) {
 #pragma unroll 4
-        for (uint64_t k = lane; k < words; k += 32) d[k] = __ldg(sw + k);
+        for (uint64_t k = lane; k < words; k += 32) d[k] = ldg(sw + k);
     } else {
 #pragma unroll 4
-        for (uint64_t k = lane; k < words; k += 32) d[k] = __funnelshift_r(__ldg(sw + k), __ldg(sw + k + 1), sh);
+        for (uint64_t k = lane; k < words; k += 32) d[k] = __funnelshift_r(ldg(sw + k), ldg(sw + k + 1), sh);
     }
     const uint64_t tail = (n - h) - 4 * words;
     if ((uint64_t)lane < tail) ((uint8_t *)d)[4 * words + lane] = sp[4 * words + lane];
@@ -1303,7 +1371,7 @@ constexpr bool stage_persistent(int op)
 // the others are persistent: an occupancy-sized grid strides over the tiles, skipping from a tile
 // past its item's real extent straight to its first tile of the next item.
 // resident blocks per SM the compiler keeps registers for (measured per pass on the mixed workload)
-constexpr int stage_min_blocks(int op) { return op == B_SPLIT || op == B_GFC_COMPRESS || op == B_TOPK ? 4 : 5; }
+constexpr int stage_min_blocks(int op) { return op == B_SPLIT || op == B_GFC_COMPRESS || op == B_TOPK || op == B_HIST ? 4 : 5; }
 
 template <int OP>
 __global__ void __launch_bounds__(kBThreads, stage_min_blocks(OP))
@@ -1378,7 +1446,75 @@ __device__ __forceinline__ void run_stage(const BItem &it, uint32_t tile, Stream
 #undef GTSC_ES_SWITCH
 }
 
+// ------------------------------------------------------------------------------- persistent step
+constexpr size_t persist_smem_c()
+{
+    size_t m = 16;
+    for (int op = 0; op <= B_GFC_COMPACT; op++) m = stage_smem(op) > m ? stage_smem(op) : m;
+    return m;
+}
+
+// tiles of an item that do work: the streaming passes skip tiles past the real length, as their
+// stage launches do; every other pass runs all its tiles
+__device__ __forceinline__ uint32_t persist_extent_c(int op, const BItem &it, const StreamDesc *S)
+{
+    switch (op) {
+    case B_MINMAX: return stage_extent<B_MINMAX>(it, S);
+    case B_DELTA_ENC: return stage_extent<B_DELTA_ENC>(it, S);
+    case B_SCALE_SUB: return stage_extent<B_SCALE_SUB>(it, S);
+    case B_AFL_PACK: return stage_extent<B_AFL_PACK>(it, S);
+    case B_F2I_STATS: return stage_extent<B_F2I_STATS>(it, S);
+    case B_F2I_ENC: return stage_extent<B_F2I_ENC>(it, S);
+    case B_F2I_RAW: return stage_extent<B_F2I_RAW>(it, S);
+    case B_RLE_LENGTHS: return stage_extent<B_RLE_LENGTHS>(it, S);
+    default: return it.tiles;
+    }
+}
+
+// The whole compress step in one launch: every pass kind behind one switch, tiles pulled from the
+// queue of batch.hpp (PLaunch).
+__global__ void __launch_bounds__(kBThreads, 4) k_bpersist_c(PersistArgs a)
+{
+    __shared__ __align__(16) unsigned char smem[persist_smem_c()];
+    persist_loop(
+        a, [](int op, const BItem &it, const StreamDesc *S) { return persist_extent_c(op, it, S); },
+        [&](int op, const BItem &it, uint32_t tile) {
+        switch (op) {
+#define GTSC_RUN(OPC) case OPC: run_stage<OPC>(it, tile, a.S, a.status, smem); break;
+            GTSC_RUN(B_MINMAX)
+            GTSC_RUN(B_DELTA_ENC)
+            GTSC_RUN(B_SCALE_SUB)
+            GTSC_RUN(B_AFL_PACK)
+            GTSC_RUN(B_HIST)
+            GTSC_RUN(B_TOPK)
+            GTSC_RUN(B_SPLIT)
+            GTSC_RUN(B_RLE_HEADS)
+            GTSC_RUN(B_RLE_LENGTHS)
+            GTSC_RUN(B_F2I_STATS)
+            GTSC_RUN(B_F2I_ENC)
+            GTSC_RUN(B_F2I_RAW)
+            GTSC_RUN(B_GFC_COMPRESS)
+            GTSC_RUN(B_GFC_SCAN)
+            GTSC_RUN(B_GFC_COMPACT)
+            GTSC_RUN(B_VMETA)
+#undef GTSC_RUN
+        default: set_status(a.status, GTSC_ERR_ARG); break;
+        }
+    });
+}
+
 }  // namespace
+
+void launch_batch_persistent_c(const PersistArgs &a, cudaStream_t s)
+{
+    if (a.total == 0) return;
+    int per_sm = 0;
+    GTSC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bpersist_c, kBThreads, 0));
+    const uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * (uint64_t)sm_count(),
+                                             (a.total + kPersistChunk - 1) / kPersistChunk);
+    k_bpersist_c<<<(unsigned)grid, kBThreads, 0, s>>>(a);
+    GTSC_CUDA(cudaGetLastError());
+}
 
 void launch_batch_decode_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items,
                                uint64_t total_tiles, StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status,

@@ -305,6 +305,17 @@ gtsc_status gtsc_batch_status(gtsc_batch *b, void *stream)
 
 int32_t gtsc_batch_launches(gtsc_batch *b, int32_t compress) { return b ? batch_launches(b->e, compress != 0) : 0; }
 
+gtsc_status gtsc_batch_set_schedule(gtsc_batch *b, int32_t schedule)
+{
+    return guard([&] {
+        if (!b) fail(GTSC_ERR_ARG, "null batch");
+        if (schedule != GTSC_SCHEDULE_LEVELS && schedule != GTSC_SCHEDULE_PERSISTENT) fail(GTSC_ERR_ARG, "unknown schedule");
+        batch_set_schedule(b->e, schedule == GTSC_SCHEDULE_PERSISTENT);
+    });
+}
+
+int32_t gtsc_batch_schedule(gtsc_batch *b) { return b && batch_schedule(b->e) ? GTSC_SCHEDULE_PERSISTENT : GTSC_SCHEDULE_LEVELS; }
+
 gtsc_status gtsc_batch_profile(gtsc_batch *b, int32_t compress, int32_t *ops, float *ms, uint64_t *bytes,
                                uint64_t *blocks, int32_t cap, int32_t *n, void *stream)
 {

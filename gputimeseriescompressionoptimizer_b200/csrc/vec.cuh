@@ -5,6 +5,26 @@
 
 namespace gtsc {
 
+// Read-only loads.  Data that earlier work of the same kernel may have written must not be read
+// through the non-coherent read-only path (ld.global.nc is only defined for data that no thread
+// writes while the kernel runs).  The batch engine's translation units hold persistent kernels in
+// which later passes read what earlier passes wrote, so they define GTSC_COHERENT_LOADS before
+// including this header and get plain (L1-cached, coherent after an acquire) loads instead.
+// (internal linkage: the two definitions never meet across translation units)
+#ifdef GTSC_COHERENT_LOADS
+template <class T>
+static __device__ __forceinline__ T ldg(const T *p)
+{
+    return *p;
+}
+#else
+template <class T>
+static __device__ __forceinline__ T ldg(const T *p)
+{
+    return __ldg(p);
+}
+#endif
+
 // Element j (of width ES <= 4) of a 16-byte chunk; ES == 8 is specialised below.
 template <int ES>
 __device__ __forceinline__ uint64_t chunk_elem(const uint4 &c, int j)
@@ -27,10 +47,10 @@ __device__ __forceinline__ uint64_t chunk_elem<8>(const uint4 &c, int j)
 template <int ES>
 __device__ __forceinline__ uint64_t ld_elem(const uint8_t *p, uint64_t i)
 {
-    if (ES == 1) return __ldg(p + i);
-    if (ES == 2) return __ldg((const unsigned short *)p + i);
-    if (ES == 4) return __ldg((const unsigned int *)p + i);
-    return __ldg((const unsigned long long *)p + i);
+    if (ES == 1) return ldg(p + i);
+    if (ES == 2) return ldg((const unsigned short *)p + i);
+    if (ES == 4) return ldg((const unsigned int *)p + i);
+    return ldg((const unsigned long long *)p + i);
 }
 
 // Little-endian load of an ES-byte value at any address (metadata fields inside a blob).
@@ -39,7 +59,7 @@ __device__ __forceinline__ uint64_t ld_unaligned(const uint8_t *p)
 {
     uint64_t v = 0;
 #pragma unroll
-    for (int k = 0; k < ES; k++) v |= (uint64_t)__ldg(p + k) << (8 * k);
+    for (int k = 0; k < ES; k++) v |= (uint64_t)ldg(p + k) << (8 * k);
     return v;
 }
 
@@ -54,7 +74,7 @@ __device__ __forceinline__ void st_elem(uint8_t *p, uint64_t i, uint64_t v)
 
 __device__ __forceinline__ uint4 ld_chunk(const uint8_t *p)  // p 16-byte aligned
 {
-    return __ldg((const uint4 *)p);
+    return ldg((const uint4 *)p);
 }
 
 // Pack element values into a 16-byte chunk.
@@ -86,7 +106,7 @@ struct StreamReader {
     __device__ __forceinline__ uint32_t word(uint64_t w) const
     {
         uint64_t b = 4 * w;
-        if (b + 4 <= nbytes) return __ldg(base + w);
+        if (b + 4 <= nbytes) return ldg(base + w);
         uint32_t r = 0;
         const uint8_t *p = (const uint8_t *)base;
         for (int k = 0; k < 4; k++)

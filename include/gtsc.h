@@ -194,9 +194,20 @@ gtsc_status gtsc_batch_status(gtsc_batch *b, void *stream);
 /* kernel launches in one step (compress != 0: compress step) */
 int32_t gtsc_batch_launches(gtsc_batch *b, int32_t compress);
 /*
+ * The schedule later steps replay (both are recorded at creation): GTSC_SCHEDULE_LEVELS = one launch
+ * per (tree level, pass kind) over all columns; GTSC_SCHEDULE_PERSISTENT = one persistent launch per
+ * step whose blocks pull (pass, tile) work from a device queue, each column's levels waiting only for
+ * that column's earlier levels (then a compress step is 6 launches and a decompress step 4).  Both
+ * give the same bytes.  The default is the levels; gtsc_batch_autotune picks by measurement.
+ * No counterpart in the reference (it compresses one column at a time).
+ */
+enum { GTSC_SCHEDULE_LEVELS = 0, GTSC_SCHEDULE_PERSISTENT = 1 };
+gtsc_status gtsc_batch_set_schedule(gtsc_batch *b, int32_t schedule);
+int32_t gtsc_batch_schedule(gtsc_batch *b);
+/*
  * One step run launch by launch with CUDA events between the launches (not the graph): per launch
  * its pass kind (ops[i] >= 0, or -1 stream setup, -2 scratch zeroing, -3/-4/-5 frame sizes / layout
- * / copy, -6 frame parse), its time in ms, the bytes it must read and write at least (its input and
+ * / copy, -6 frame parse, -7 the persistent launch of every pass), its time in ms, the bytes it must read and write at least (its input and
  * output streams) and its blocks.  Writes at most cap entries and the count to *n.  Synchronises.
  * No counterpart in the reference (its per-column calls are timed one by one).
  */

@@ -58,7 +58,26 @@ def run_batch(G, O, cols, dtypes, trees, steps=1):
         b.status()
         for i, x in enumerate(cols):
             assert G.to_host(outs[i]).tobytes() == x.tobytes(), (i, G.tree_names(trees[i]), x.dtype, x.size)
+    check_persistent(G, b, cols, trees, first, steps)
     return b, st, devs
+
+
+def check_persistent(G, b, cols, trees, framed_levels, steps=1):
+    """The same batch replayed as one persistent launch per step: the framed output is byte-identical
+    to the level schedule's, and the persistent decompress gives every column back bit-exact."""
+    b.set_schedule(True)
+    assert b.schedule() == "persistent" and b.launches(True) == 6 and b.launches(False) == 4
+    for _ in range(steps):
+        b.compress()
+        b.status()
+        p, nb, framed, _ = framed_blobs(G, b)
+        assert np.array_equal(framed, framed_levels), "persistent compress differs from the level schedule"
+        outs = [G.alloc(x.nbytes) for x in cols]
+        b.decompress(p, nb, outs)
+        b.status()
+        for i, x in enumerate(cols):
+            assert G.to_host(outs[i]).tobytes() == x.tobytes(), ("persistent", i, G.tree_names(trees[i]))
+    b.set_schedule(False)
 
 
 def test_batch_reference_tree_shapes(G, O, rng):
@@ -153,29 +172,31 @@ def test_batch_corrupt_frames_fail_cleanly(G, O, rng):
     b, st, devs = run_batch(G, O, cols, [OR.INT] * 2, trees)
     p, nb, framed, blobs = framed_blobs(G, b)
     outs = [G.alloc(x.nbytes) for x in cols]
-    for cut in [5, 20, nb // 2, nb - 1]:
-        bad = G.to_device(framed[:cut])
-        b.decompress(bad.ptr, bad.nbytes, outs)
+    for persistent in (False, True):
+        b.set_schedule(persistent)
+        for cut in [5, 20, nb // 2, nb - 1]:
+            bad = G.to_device(framed[:cut])
+            b.decompress(bad.ptr, bad.nbytes, outs)
+            with pytest.raises(G.GtscError):
+                b.status()
+        bad = framed.copy()
+        bad[8 + 8 * len(cols)] = 99  # unknown encoding type in the first node header
+        d = G.to_device(bad)
+        b.decompress(d.ptr, d.nbytes, outs)
         with pytest.raises(G.GtscError):
             b.status()
-    bad = framed.copy()
-    bad[8 + 8 * len(cols)] = 99  # unknown encoding type in the first node header
-    d = G.to_device(bad)
-    b.decompress(d.ptr, d.nbytes, outs)
-    with pytest.raises(G.GtscError):
+        bad = framed.copy()
+        bad[0] = 3  # wrong column count
+        d = G.to_device(bad)
+        b.decompress(d.ptr, d.nbytes, outs)
+        with pytest.raises(G.GtscError):
+            b.status()
+        # the engine still works after the errors
+        good = G.to_device(framed)
+        b.decompress(good.ptr, good.nbytes, outs)
         b.status()
-    bad = framed.copy()
-    bad[0] = 3  # wrong column count
-    d = G.to_device(bad)
-    b.decompress(d.ptr, d.nbytes, outs)
-    with pytest.raises(G.GtscError):
-        b.status()
-    # the engine still works after the errors
-    good = G.to_device(framed)
-    b.decompress(good.ptr, good.nbytes, outs)
-    b.status()
-    for i, x in enumerate(cols):
-        assert G.to_host(outs[i]).tobytes() == x.tobytes()
+        for i, x in enumerate(cols):
+            assert G.to_host(outs[i]).tobytes() == x.tobytes()
 
 
 VIEW_TREES = [
