@@ -224,7 +224,6 @@ constexpr uint32_t kBMergeSub = 4;      // kBTile tiles per block of the merge p
 constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
 constexpr uint32_t kBHistSmem = 2048;    // shared hash slots of a histogram block (8-byte values)
 constexpr uint32_t kBHistPacked = 4096;  // the same for values of up to 4 bytes (packed slots)
-constexpr int kBHistPackedLog2 = 12;
 
 // scratch layout of a histogram item
 struct BHistHdr {

@@ -4,8 +4,10 @@
 // Framed output: for every column, a uint64 blob length followed by the column's serialized tree
 // (the reference's per-column-chunk file framing, optimizer/compression_task.cpp:35-40, with
 // the blob of CompressionTree::Compress).
-// the persistent kernels here read, in later passes, what earlier passes of the same launch wrote
-#define GTSC_COHERENT_LOADS 1
+//
+// As in batch_kernels.cu, batch_persist_d.cu compiles the decode passes a second time (with
+// GTSC_PERSISTENT_TU and coherent loads) for the persistent decode kernel; the stage kernels and the
+// framing kernels are built only here.
 #include "batch_dev.cuh"
 
 #include <algorithm>
@@ -30,12 +32,31 @@ __device__ void block_copy(uint8_t *dst, const uint8_t *src, uint64_t n)
     const uint32_t sh = 8 * (uint32_t)((uintptr_t)sp & 3);
     const uint32_t *sw = (const uint32_t *)((uintptr_t)sp & ~(uintptr_t)3);
     uint32_t *dw = (uint32_t *)d;
+    // eight words a thread are loaded before any of them is stored, so the loads are in flight
+    // together whatever the compiler assumes about the two buffers overlapping
+    constexpr int U = 8;
+    uint64_t k = threadIdx.x;
     if (sh == 0) {
-#pragma unroll 4
-        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = ldg(sw + k);
+        for (; k + (U - 1) * kBThreads < words; k += U * kBThreads) {
+            uint32_t r[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) r[u] = ldg(sw + k + u * kBThreads);
+#pragma unroll
+            for (int u = 0; u < U; u++) dw[k + u * kBThreads] = r[u];
+        }
+        for (; k < words; k += kBThreads) dw[k] = ldg(sw + k);
     } else {
-#pragma unroll 4
-        for (uint64_t k = threadIdx.x; k < words; k += kBThreads) dw[k] = __funnelshift_r(ldg(sw + k), ldg(sw + k + 1), sh);
+        for (; k + (U - 1) * kBThreads < words; k += U * kBThreads) {
+            uint32_t r[U], q[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                r[u] = ldg(sw + k + u * kBThreads);
+                q[u] = ldg(sw + k + u * kBThreads + 1);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) dw[k + u * kBThreads] = __funnelshift_r(r[u], q[u], sh);
+        }
+        for (; k < words; k += kBThreads) dw[k] = __funnelshift_r(ldg(sw + k), ldg(sw + k + 1), sh);
     }
     const uint64_t tail = (n - h) - 4 * words;
     if (threadIdx.x < tail) d[4 * words + threadIdx.x] = sp[4 * words + threadIdx.x];
@@ -916,6 +937,7 @@ __device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDe
 #undef GTSC_ES_SWITCH
 }
 
+#ifdef GTSC_PERSISTENT_TU
 // ------------------------------------------------------------------------------- persistent step
 constexpr size_t kPersistSmemD = 8 * kBTile > kGfcRing * (kBThreads / 32) ? 8 * kBTile : kGfcRing * (kBThreads / 32);
 
@@ -954,10 +976,13 @@ __global__ void __launch_bounds__(kBThreads, 4) k_bpersist_d(PersistArgs a)
                 GTSC_RUN(B_GFC_SIZES)
                 GTSC_RUN(B_GFC_DEC)
 #undef GTSC_RUN
+            case B_GFC_SCAN: p_gfc_scan(it, tile, a.S, it.es == 8, it.mode != 0); break;
             default: set_status(a.status, GTSC_ERR_ARG); break;
             }
         });
 }
+
+#else
 
 // ------------------------------------------------------------------------------- framing
 // Framed buffer: uint64 column count C, uint64 blob bytes of every column (the directory), then the
@@ -1123,8 +1148,11 @@ __global__ void k_zero_ranges(const unsigned long long *ranges, int n)
     }
 }
 
+#endif  // GTSC_PERSISTENT_TU
+
 }  // namespace
 
+#ifndef GTSC_PERSISTENT_TU
 // as many blocks as fit at once for the streaming decode passes, else one block per tile
 template <class K>
 unsigned stage_grid_dec(K kernel, int op, uint64_t total_tiles)
@@ -1208,6 +1236,15 @@ void launch_parse_frames(const BColumnDev *cols, int ncols, const BNodeDev *node
     GTSC_CUDA(cudaGetLastError());
 }
 
+void launch_zero_ranges(const unsigned long long *ranges, int n, cudaStream_t s)
+{
+    if (!n) return;
+    k_zero_ranges<<<n < 1024 ? n : 1024, 256, 0, s>>>(ranges, n);
+    GTSC_CUDA(cudaGetLastError());
+}
+
+#else
+
 void launch_batch_persistent_d(const PersistArgs &a, cudaStream_t s)
 {
     if (a.total == 0) return;
@@ -1219,11 +1256,6 @@ void launch_batch_persistent_d(const PersistArgs &a, cudaStream_t s)
     GTSC_CUDA(cudaGetLastError());
 }
 
-void launch_zero_ranges(const unsigned long long *ranges, int n, cudaStream_t s)
-{
-    if (!n) return;
-    k_zero_ranges<<<n < 1024 ? n : 1024, 256, 0, s>>>(ranges, n);
-    GTSC_CUDA(cudaGetLastError());
-}
+#endif  // GTSC_PERSISTENT_TU
 
 }  // namespace gtsc

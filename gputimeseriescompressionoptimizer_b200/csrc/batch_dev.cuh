@@ -449,6 +449,56 @@ __device__ __forceinline__ const BItem &shared_item(const BItem *items, uint32_t
     return shared_item_ref();
 }
 
+// GFC: inclusive scan of the chunk sizes (compress: this node's; decode: p[1]); a pass of both the
+// compress and the decode step, so it lives here
+__device__ inline void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool dbl, bool decode)
+{
+    __shared__ unsigned long long ws[32];
+    __shared__ unsigned long long s_prefix;
+    uint64_t n;
+    int blocks = 0, wpb = 0;
+    if (decode) {
+        const StreamDesc m = S[it.in[0]];
+        if (m.len < 12) return;
+        blocks = (int32_t)ld_unaligned<4>(m.ptr);
+        wpb = (int32_t)ld_unaligned<4>(m.ptr + 4);
+        n = (uint64_t)(int32_t)ld_unaligned<4>(m.ptr + 8);
+        if (blocks <= 0 || wpb <= 0) return;
+    } else {
+        int nd = 0;
+        for (int k = 0; k < kMaxViewOps; k++) nd += it.vop[k] == V_DELTA;
+        const uint64_t n_src = S[it.in[0]].len / (dbl ? 8 : 4);
+        n = n_src > (uint64_t)nd ? n_src - nd : 0;
+    }
+    const DGfc g = d_gfc_geom(dbl, n, blocks, wpb);
+    // decode: p[3] = the chunks the scratch holds (a larger count is reported by the sizes pass)
+    if (decode && (uint64_t)g.warps > it.p[3]) return;
+    if (tile > 0 && (uint64_t)tile * kBTile >= (uint64_t)g.warps) return;  // past the chunks
+    const int32_t *sizes = (const int32_t *)(it.scratch + it.p[1]);
+    unsigned long long *incl = (unsigned long long *)(it.scratch + it.p[2]);
+    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    unsigned long long v[kBVPT], local = 0;
+#pragma unroll
+    for (int j = 0; j < (int)kBVPT; j++) {
+        v[j] = base + j < (uint64_t)g.warps ? (unsigned long long)(uint32_t)sizes[base + j] : 0ull;
+        local += v[j];
+    }
+    unsigned long long total;
+    const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
+    }
+    __syncthreads();
+    unsigned long long acc = s_prefix + excl;
+#pragma unroll
+    for (int j = 0; j < (int)kBVPT; j++) {
+        acc += v[j];
+        if (base + j < (uint64_t)g.warps) incl[base + j] = acc;
+    }
+}
+
 // ------------------------------------------------------------------------------- persistent step
 // Helpers of the persistent kernels (batch.hpp, PLaunch); all of them run on thread 0 of a block.
 

@@ -6,8 +6,11 @@
 // look-back of scan.cuh, per item.  Every pass reads its input length from the stream table and
 // writes its outputs' lengths there; tile 0 (or the tile that ends the input) writes metadata.
 // Byte layouts are the per-encoding ones of encodings.cu (and of the reference).
-// the persistent kernels here read, in later passes, what earlier passes of the same launch wrote
-#define GTSC_COHERENT_LOADS 1
+//
+// The stage kernels read their inputs through the read-only path (every input was written by an
+// earlier launch).  batch_persist_c.cu compiles this file a second time, with GTSC_PERSISTENT_TU and
+// coherent loads, for the persistent kernel, in which later passes read what earlier passes of the
+// same launch wrote.
 #include "batch_dev.cuh"
 
 #include <algorithm>
@@ -389,8 +392,7 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         for (uint64_t w = t0 / 16 + threadIdx.x; w < (e_end + 15) / 16; w += kBThreads) words[w] = 0u;
     }
     unsigned long long nan_min[4] = {EMPTY, EMPTY, EMPTY, EMPTY};
-    if constexpr (ES <= 4) {
-      if (t0 < n) {
+    if (ES <= 4 && t0 < n) {
         // values of up to 4 bytes: 32-bit keys and counts (twice the slots of the layout below); a
         // value already in the table costs a plain key read and one 32-bit atomicAdd.  0xffffffff
         // marks an empty slot, so that value itself is counted apart.
@@ -404,97 +406,84 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         if (threadIdx.x == 0) s_ones = 0;
         __syncthreads();
         const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
-        // rounds of 8 consecutive values per thread (16 for bytes, one 16-byte vector): all of a
-        // round's loads (16-byte vectors where the stream allows) are issued before the first
-        // insert, so each thread keeps a whole run in flight instead of one element
-        constexpr int V = ES == 1 ? 16 : 8;
-        for (uint64_t r0 = t0; r0 < end; r0 += (uint64_t)kBThreads * V) {
-            const uint64_t b = r0 + (uint64_t)threadIdx.x * V;
-            uint32_t cur[V];
-            {
-                uint64_t w[V];
-                load_view<ES, V>(it, vc, in.ptr, b, w);
-#pragma unroll
-                for (int j = 0; j < V; j++) cur[j] = (uint32_t)w[j];
-            }
-            // equal neighbours within the thread's run are counted once (constant and run-heavy
-            // columns would otherwise serialise on one shared counter): run lengths from the right
-            uint32_t runlen[V];
-#pragma unroll
-            for (int j = V - 1; j >= 0; j--) {
-                const bool more = j + 1 < V && b + j + 1 < end && cur[j + 1] == cur[j];
-                runlen[j] = more ? runlen[j + 1 < V ? j + 1 : j] + 1 : 1u;
-            }
-#pragma unroll
-            for (int j = 0; j < V; j++) {
-                if (b + j >= end || (j > 0 && cur[j] == cur[j - 1])) continue;  // past the end / inside a run
-                const uint32_t kk = cur[j], c = runlen[j];
-                if (is_nan_bits(kk, o)) {
-                    for (uint32_t r = 0; r < c; r++) {
-                        unsigned long long k = order_key(kk, ES, o);
-#pragma unroll
-                        for (int q = 0; q < 4; q++)
-                            if (k < nan_min[q]) { const unsigned long long x = nan_min[q]; nan_min[q] = k; k = x; }
+        // the next element's load is in flight while this one is inserted; every lane runs the
+        // same rounds, so that the warp can vote on its 32 elements
+        unsigned long long next = t0 + threadIdx.x < end ? view_elem<ES>(it, vc, in.ptr, t0 + threadIdx.x) : 0ull;
+        for (uint64_t r0 = t0; r0 < end; r0 += kBThreads) {
+            const uint64_t i = r0 + threadIdx.x;
+            const bool valid = i < end;
+            const unsigned long long key = next;
+            if (i + kBThreads < end) next = view_elem<ES>(it, vc, in.ptr, i + kBThreads);
+            // a warp whose 32 elements are one value (a constant or long-run column) counts them with
+            // one atomic instead of 32 on the same shared counter
+            const uint32_t k0 = __shfl_sync(0xffffffffu, (uint32_t)key, 0);
+            if (__all_sync(0xffffffffu, valid && (uint32_t)key == k0) && !is_nan_bits(k0, o)) {
+                if ((threadIdx.x & 31) == 0) {
+                    if (k0 == 0xffffffffu) {
+                        atomicAdd(&s_ones, 32u);
+                    } else {
+                        uint32_t h = (uint32_t)bhash(k0) & (kBHistPacked - 1);
+                        bool done = false;
+                        for (int p = 0; p < 8; p++) {
+                            uint32_t cur = ((volatile uint32_t *)k32)[h];
+                            if (cur == 0xffffffffu) cur = atomicCAS(&k32[h], 0xffffffffu, k0);
+                            if (cur == 0xffffffffu || cur == k0) {
+                                atomicAdd(&c32[h], 32u);
+                                done = true;
+                                break;
+                            }
+                            h = (h + 1) & (kBHistPacked - 1);
+                        }
+                        if (!done) g_insert(t, (unsigned long long)k0, 32u, status);
                     }
-                    continue;
                 }
-                if (kk == 0xffffffffu) {
-                    atomicAdd(&s_ones, c);
-                    continue;
-                }
-                // multiplicative (Fibonacci) hash: the product's top 12 bits pick the slot
-                uint32_t h = (kk * 0x9E3779B1u) >> (32 - kBHistPackedLog2);
-                bool done = false;
-                for (int p = 0; p < 8; p++) {
-                    uint32_t cs = ((volatile uint32_t *)k32)[h];
-                    if (cs == 0xffffffffu) cs = atomicCAS(&k32[h], 0xffffffffu, kk);
-                    if (cs == 0xffffffffu || cs == kk) {
-                        atomicAdd(&c32[h], c);
-                        done = true;
-                        break;
-                    }
-                    h = (h + 1) & (kBHistPacked - 1);
-                }
-                if (!done) g_insert(t, (unsigned long long)kk, c, status);
+                continue;
             }
+            if (!valid) continue;
+            if (is_nan_bits(key, o)) {
+                unsigned long long k = order_key(key, ES, o);
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
+                continue;
+            }
+            const uint32_t kk = (uint32_t)key;
+            if (kk == 0xffffffffu) {
+                atomicAdd(&s_ones, 1u);
+                continue;
+            }
+            uint32_t h = (uint32_t)bhash(key) & (kBHistPacked - 1);
+            bool done = false;
+            for (int p = 0; p < 8; p++) {
+                uint32_t cur = ((volatile uint32_t *)k32)[h];
+                if (cur == 0xffffffffu) cur = atomicCAS(&k32[h], 0xffffffffu, kk);
+                if (cur == 0xffffffffu || cur == kk) {
+                    atomicAdd(&c32[h], 1u);
+                    done = true;
+                    break;
+                }
+                h = (h + 1) & (kBHistPacked - 1);
+            }
+            if (!done) g_insert(t, key, 1u, status);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < (int)kBHistPacked; i += kBThreads)
             if (k32[i] != 0xffffffffu) g_insert(t, (unsigned long long)k32[i], c32[i], status);
         if (threadIdx.x == 0 && s_ones) g_insert(t, 0xffffffffull, s_ones, status);
-      }
-    } else {
-      if (t0 < n) {
+    } else if (t0 < n) {
         for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads) {
             skeys[i] = EMPTY;
             scounts[i] = 0;
         }
         __syncthreads();
         const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
-        // rounds of 8 consecutive values per thread, loaded before the first insert
-        constexpr int V = 8;
-        for (uint64_t r0 = t0; r0 < end; r0 += (uint64_t)kBThreads * V) {
-          const uint64_t b = r0 + (uint64_t)threadIdx.x * V;
-          uint64_t cur[V];
-          load_view<ES, V>(it, vc, in.ptr, b, cur);
-          uint32_t runlen[V];  // equal neighbours are counted once (as in the narrow path)
-#pragma unroll
-          for (int j = V - 1; j >= 0; j--) {
-            const bool more = j + 1 < V && b + j + 1 < end && cur[j + 1] == cur[j];
-            runlen[j] = more ? runlen[j + 1 < V ? j + 1 : j] + 1 : 1u;
-          }
-#pragma unroll
-          for (int j = 0; j < V; j++) {
-            if (b + j >= end || (j > 0 && cur[j] == cur[j - 1])) continue;
-            const unsigned long long key = cur[j];
-            const uint32_t c = runlen[j];
+        for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
+            const unsigned long long key = view_elem<ES>(it, vc, in.ptr, i);
             if (is_nan_bits(key, o)) {
-                for (uint32_t r = 0; r < c; r++) {
-                    unsigned long long k = order_key(key, ES, o);
+                unsigned long long k = order_key(key, ES, o);
 #pragma unroll
-                    for (int q = 0; q < 4; q++)
-                        if (k < nan_min[q]) { const unsigned long long x = nan_min[q]; nan_min[q] = k; k = x; }
-                }
+                for (int j = 0; j < 4; j++)
+                    if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
                 continue;
             }
             bool done = false;
@@ -503,20 +492,18 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
                 for (int p = 0; p < 8; p++) {
                     const unsigned long long prev = atomicCAS(&skeys[h], EMPTY, key);
                     if (prev == EMPTY || prev == key) {
-                        atomicAdd(&scounts[h], c);
+                        atomicAdd(&scounts[h], 1u);
                         done = true;
                         break;
                     }
                     h = (h + 1) & (kBHistSmem - 1);
                 }
             }
-            if (!done) g_insert(t, key, c, status);
-          }
+            if (!done) g_insert(t, key, 1u, status);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads)
             if (skeys[i] != EMPTY) g_insert(t, skeys[i], scounts[i], status);
-      }
     }
     // this tile's 4 smallest NaN sort keys
     for (int off = 16; off > 0; off >>= 1) {
@@ -1190,59 +1177,9 @@ __device__ void p_gfc_compress(const BItem &it, uint32_t tile, StreamDesc *S, ui
     }
 }
 
-// inclusive scan of the chunk sizes (compress: this node's; decode: p[1])
-__device__ void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S, bool dbl, bool decode)
-{
-    __shared__ unsigned long long ws[32];
-    __shared__ unsigned long long s_prefix;
-    uint64_t n;
-    int blocks = 0, wpb = 0;
-    if (decode) {
-        const StreamDesc m = S[it.in[0]];
-        if (m.len < 12) return;
-        blocks = (int32_t)ld_unaligned<4>(m.ptr);
-        wpb = (int32_t)ld_unaligned<4>(m.ptr + 4);
-        n = (uint64_t)(int32_t)ld_unaligned<4>(m.ptr + 8);
-        if (blocks <= 0 || wpb <= 0) return;
-    } else {
-        int nd = 0;
-        for (int k = 0; k < kMaxViewOps; k++) nd += it.vop[k] == V_DELTA;
-        const uint64_t n_src = S[it.in[0]].len / (dbl ? 8 : 4);
-        n = n_src > (uint64_t)nd ? n_src - nd : 0;
-    }
-    const DGfc g = d_gfc_geom(dbl, n, blocks, wpb);
-    // decode: p[3] = the chunks the scratch holds (a larger count is reported by the sizes pass)
-    if (decode && (uint64_t)g.warps > it.p[3]) return;
-    if (tile > 0 && (uint64_t)tile * kBTile >= (uint64_t)g.warps) return;  // past the chunks
-    const int32_t *sizes = (const int32_t *)(it.scratch + it.p[1]);
-    unsigned long long *incl = (unsigned long long *)(it.scratch + it.p[2]);
-    Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
-    unsigned long long v[kBVPT], local = 0;
-#pragma unroll
-    for (int j = 0; j < (int)kBVPT; j++) {
-        v[j] = base + j < (uint64_t)g.warps ? (unsigned long long)(uint32_t)sizes[base + j] : 0ull;
-        local += v[j];
-    }
-    unsigned long long total;
-    const unsigned long long excl = block_exclusive_scan<kBThreads>(local, ws, total);
-    if (threadIdx.x < 32) {
-        const unsigned long long e = lookback_exclusive(lb, tile, total);
-        if (threadIdx.x == 0) s_prefix = e;
-    }
-    __syncthreads();
-    unsigned long long acc = s_prefix + excl;
-#pragma unroll
-    for (int j = 0; j < (int)kBVPT; j++) {
-        acc += v[j];
-        if (base + j < (uint64_t)g.warps) incl[base + j] = acc;
-    }
-}
-
 // one warp copies n bytes between any addresses: head bytes up to a 4-byte aligned destination,
-// then whole words funnel-shifted out of aligned source words, then the tail.  The source is read
-// through the read-only path (it was written by an earlier launch), so the unrolled loads are all
-// in flight together.
+// then whole words funnel-shifted out of aligned source words, then the tail.  Eight words a lane
+// are loaded before any is stored, so the loads are in flight together.
 __device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint64_t n, int lane)
 {
     const uint64_t head = (4 - ((uintptr_t)dst & 3)) & 3;
@@ -1254,12 +1191,29 @@ __device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint
     const uint64_t words = (n - h) / 4;
     const uint32_t sh = 8 * (uint32_t)((uintptr_t)sp & 3);
     const uint32_t *sw = (const uint32_t *)((uintptr_t)sp & ~(uintptr_t)3);
+    constexpr int U = 8;
+    uint64_t k = lane;
     if (sh == 0) {
-#pragma unroll 4
-        for (uint64_t k = lane; k < words; k += 32) d[k] = ldg(sw + k);
+        for (; k + (U - 1) * 32 < words; k += U * 32) {
+            uint32_t r[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) r[u] = ldg(sw + k + u * 32);
+#pragma unroll
+            for (int u = 0; u < U; u++) d[k + u * 32] = r[u];
+        }
+        for (; k < words; k += 32) d[k] = ldg(sw + k);
     } else {
-#pragma unroll 4
-        for (uint64_t k = lane; k < words; k += 32) d[k] = __funnelshift_r(ldg(sw + k), ldg(sw + k + 1), sh);
+        for (; k + (U - 1) * 32 < words; k += U * 32) {
+            uint32_t r[U], q[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                r[u] = ldg(sw + k + u * 32);
+                q[u] = ldg(sw + k + u * 32 + 1);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) d[k + u * 32] = __funnelshift_r(r[u], q[u], sh);
+        }
+        for (; k < words; k += 32) d[k] = __funnelshift_r(ldg(sw + k), ldg(sw + k + 1), sh);
     }
     const uint64_t tail = (n - h) - 4 * words;
     if ((uint64_t)lane < tail) ((uint8_t *)d)[4 * words + lane] = sp[4 * words + lane];
@@ -1371,7 +1325,7 @@ constexpr bool stage_persistent(int op)
 // the others are persistent: an occupancy-sized grid strides over the tiles, skipping from a tile
 // past its item's real extent straight to its first tile of the next item.
 // resident blocks per SM the compiler keeps registers for (measured per pass on the mixed workload)
-constexpr int stage_min_blocks(int op) { return op == B_SPLIT || op == B_GFC_COMPRESS || op == B_TOPK || op == B_HIST ? 4 : 5; }
+constexpr int stage_min_blocks(int op) { return op == B_SPLIT || op == B_GFC_COMPRESS || op == B_TOPK ? 4 : 5; }
 
 template <int OP>
 __global__ void __launch_bounds__(kBThreads, stage_min_blocks(OP))
@@ -1446,6 +1400,7 @@ __device__ __forceinline__ void run_stage(const BItem &it, uint32_t tile, Stream
 #undef GTSC_ES_SWITCH
 }
 
+#ifdef GTSC_PERSISTENT_TU
 // ------------------------------------------------------------------------------- persistent step
 constexpr size_t persist_smem_c()
 {
@@ -1503,8 +1458,11 @@ __global__ void __launch_bounds__(kBThreads, 4) k_bpersist_c(PersistArgs a)
     });
 }
 
+#endif  // GTSC_PERSISTENT_TU
+
 }  // namespace
 
+#ifdef GTSC_PERSISTENT_TU
 void launch_batch_persistent_c(const PersistArgs &a, cudaStream_t s)
 {
     if (a.total == 0) return;
@@ -1515,6 +1473,7 @@ void launch_batch_persistent_c(const PersistArgs &a, cudaStream_t s)
     k_bpersist_c<<<(unsigned)grid, kBThreads, 0, s>>>(a);
     GTSC_CUDA(cudaGetLastError());
 }
+#else
 
 void launch_batch_decode_stage(int op, const BItem *d_items, const uint32_t *d_item_of, int n_items,
                                uint64_t total_tiles, StreamDesc *d_streams, uint32_t *d_counter, uint32_t *d_status,
@@ -1569,5 +1528,7 @@ void launch_batch_stage(int op, const BItem *d_items, const uint32_t *d_item_of,
     }
     GTSC_CUDA(cudaGetLastError());
 }
+
+#endif  // GTSC_PERSISTENT_TU
 
 }  // namespace gtsc
