@@ -891,8 +891,10 @@ void BatchEngine::plan_persistent(const std::vector<Launch> &launches, const std
         p.map_off = (uint32_t)L.map_off;
         p.qstart = (uint32_t)q;
         p.dyn = dyn_pass(L.op) ? 1 : 0;
+        p.per = p.dyn ? 1u : kPersistChunk;
+        p.pad = 0;
         pl.push_back(p);
-        q += L.tiles;
+        q += (L.tiles + p.per - 1) / p.per;
         for (int k = L.first; k < L.first + L.count; k++) {
             const int c = item_col[k];
             if (before[c] > 0xffffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles for the persistent schedule");
@@ -900,7 +902,7 @@ void BatchEngine::plan_persistent(const std::vector<Launch> &launches, const std
             tot[c] += items[k].tiles;
         }
     }
-    if (q >= 0xffffffffull - kPersistChunk) fail(GTSC_ERR_CAPACITY, "batch: too many tiles for the persistent schedule");
+    if (q >= 0xffffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles for the persistent schedule");
     total = (uint32_t)q;
 }
 

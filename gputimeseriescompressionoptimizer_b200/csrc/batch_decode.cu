@@ -1251,7 +1251,7 @@ void launch_batch_persistent_d(const PersistArgs &a, cudaStream_t s)
     int per_sm = 0;
     GTSC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bpersist_d, kBThreads, 0));
     const uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * (uint64_t)sm_count(),
-                                             (a.total + kPersistChunk - 1) / kPersistChunk);
+                                             (uint64_t)a.total);
     k_bpersist_d<<<(unsigned)grid, kBThreads, 0, s>>>(a);
     GTSC_CUDA(cudaGetLastError());
 }

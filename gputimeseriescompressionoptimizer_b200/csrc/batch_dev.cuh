@@ -540,53 +540,71 @@ __device__ __forceinline__ void persist_flush(const PersistArgs &a, int item, ui
     pend = 0;
 }
 
-// The persistent loop shared by the compress and the decode kernel.  EXTENT(op, item, S) gives an
-// item's tiles that do work (the level schedule's persistent passes skip the others), RUN(op,
-// item, tile) runs one tile.
+// The persistent loop shared by the compress and the decode kernel.  A block claims one queue unit
+// at a time: one tile of a look-back pass (its successors wait on it, so it is never held behind
+// other work of the same block), kPersistChunk tiles of any other pass.  Thread 0 walks the unit's
+// tiles; tiles past their item's real extent are counted without involving the block.
+// EXTENT(op, item, S) gives an item's tiles that do work (the level schedule's streaming passes skip
+// the others), RUN(op, item, tile) runs one tile with the whole block.
 template <class Extent, class Run>
 __device__ __forceinline__ void persist_loop(const PersistArgs &a, Extent extent, Run run)
 {
-    __shared__ uint32_t s_e0, s_tile, s_ext;
-    __shared__ int s_item, s_op, s_new;
-    int cur = -1;       // thread 0: the item whose entries it is counting
-    uint32_t pend = 0;  // thread 0: finished entries of cur not counted yet
+    __shared__ uint32_t s_u, s_tile;
+    __shared__ int s_item, s_op, s_new, s_run;
+    int cur = -1;       // thread 0: the item whose tiles it is counting
+    int loaded = -1;    // thread 0: the item in the block's shared descriptor
+    uint32_t pend = 0;  // thread 0: finished tiles of cur not counted yet
+    uint32_t cur_ext = 0;
     for (;;) {
-        if (threadIdx.x == 0) s_e0 = atomicAdd(a.qcounter, kPersistChunk);
+        if (threadIdx.x == 0) s_u = atomicAdd(a.qcounter, 1u);
         __syncthreads();
-        const uint32_t e0 = s_e0;
-        if (e0 >= a.total) break;
-        const uint32_t e1 = e0 + kPersistChunk < a.total ? e0 + kPersistChunk : a.total;
-        for (uint32_t e = e0; e < e1; e++) {
+        const uint32_t u = s_u;
+        if (u >= a.total) break;
+        const PLaunch *pl = nullptr;
+        uint32_t t = 0, t1 = 0;
+        if (threadIdx.x == 0) {
+            pl = &a.launches[persist_launch_of(a, u)];
+            t = (u - pl->qstart) * pl->per;
+            t1 = t + pl->per < pl->tiles ? t + pl->per : pl->tiles;
+        }
+        for (;;) {
             if (threadIdx.x == 0) {
-                const PLaunch &pl = a.launches[persist_launch_of(a, e)];
-                const uint32_t local = e - pl.qstart;
-                const uint32_t t = pl.dyn ? a.item_of[pl.map_off + pl.tiles + local] : local;
-                const int gi = pl.first + (int)a.item_of[pl.map_off + t];
-                s_new = gi != cur;
-                if (gi != cur) {
-                    persist_flush(a, cur, pend);
-                    persist_wait(a, a.pitems[gi]);
-                    cur = gi;
+                s_run = 0;
+                while (t < t1) {
+                    const uint32_t tt = pl->dyn ? a.item_of[pl->map_off + pl->tiles + t] : t;
+                    const int gi = pl->first + (int)a.item_of[pl->map_off + tt];
+                    const BItem &gitem = a.items[gi];
+                    if (gi != cur) {
+                        persist_flush(a, cur, pend);
+                        persist_wait(a, a.pitems[gi]);
+                        cur = gi;
+                        // the extent is cached per item (a stale read only recomputes the same value)
+                        uint32_t x = a.ext[gi];
+                        if (x == 0) {
+                            x = 1 + extent(pl->op, gitem, a.S);
+                            a.ext[gi] = x;
+                        }
+                        cur_ext = x - 1;
+                    }
+                    const uint32_t tile = tt - (uint32_t)gitem.tile_base;
+                    ++t;
+                    if (tile < cur_ext && tile < gitem.tiles) {
+                        s_run = 1;
+                        s_item = gi;
+                        s_op = pl->op;
+                        s_tile = tile;
+                        s_new = gi != loaded;
+                        loaded = gi;
+                        break;
+                    }
+                    ++pend;  // past the item's real length: nothing to do
                 }
-                s_item = gi;
-                s_op = pl.op;
-                s_tile = t - (uint32_t)a.items[gi].tile_base;
             }
             __syncthreads();
+            if (!s_run) break;
             if (s_new) shared_item(a.items, (uint32_t)s_item);
-            const BItem &it = shared_item_ref();
-            if (threadIdx.x == 0) {
-                // the extent is cached per item (a stale read only recomputes the same value)
-                uint32_t x = a.ext[s_item];
-                if (x == 0) {
-                    x = 1 + extent(s_op, it, a.S);
-                    a.ext[s_item] = x;
-                }
-                s_ext = x - 1;
-            }
-            __syncthreads();
-            if (s_tile < s_ext && s_tile < it.tiles) run(s_op, it, s_tile);
-            __syncthreads();  // the next entry reuses the shared memory and the descriptor
+            run(s_op, shared_item_ref(), s_tile);
+            __syncthreads();  // the next tile reuses the shared memory and the descriptor
             if (threadIdx.x == 0) ++pend;
         }
     }
