@@ -326,9 +326,9 @@ def config_column(k):
     return W.column(kind, dt, n, 0xB202 + (k if kind != "price" else 8))
 
 
-def per_config(g, torch, st, stream, peak, reps):
-    """Each benchmark configuration alone as a one-column batch (its tree's compress and decompress
-    steps, CUDA graphs, device-resident input): CUDA-event time per step (median of `reps`, the L2
+def per_config(g, torch, st, stream, peak, reps, tune):
+    """Each benchmark configuration alone as a one-column batch with the mixed workload's tuned
+    launch parameters (its tree's compress and decompress steps, CUDA graphs, device-resident input): CUDA-event time per step (median of `reps`, the L2
     flushed before each step when the column fits in it), GB/s of uncompressed input and the
     fraction of the HBM peak on algorithmic bytes (n*s + C each way).  Config 1 also times the AFL
     pack / unpack kernels alone at its bit width 11 (run_afl_compress_gpu / run_afl_decompress_gpu)."""
@@ -369,7 +369,9 @@ def per_config(g, torch, st, stream, peak, reps):
         dv = DevView(dev)
         small = x.nbytes < (128 << 20)
         nodes = g.tree_from_path(path, dt)
-        b = g.Batch([dv], [dt], [nodes], st)
+        b = g.Batch([dv], [dt], [nodes], st, tuning=g.tuning(
+            tune["minmax_tile"], tune["minmax_values_per_thread"], tune["hist_tile"],
+            tune["schedule_compress"] == "persistent", tune["schedule_decompress"] == "persistent"))
         o = torch.empty_like(dev)
         ov = [DevView(o)]
         b.compress()
@@ -460,6 +462,8 @@ def run_ours(args, world, rank, local):
     t0 = time.perf_counter()
     batch = g.Batch(dv, dts, trees, st)
     t_create = time.perf_counter() - t0
+    # the autotuner: schedule, min/max tile x values per thread, histogram tile, timed on this batch
+    tune = batch.autotune()
     outs = [torch.empty_like(d) for d in dev]
     ov = [DevView(o) for o in outs]
 
@@ -596,7 +600,7 @@ def run_ours(args, world, rank, local):
     cpu_gbs = cin / ct / 1e9
 
     tick = tick_table(g, torch, planner, st, stream, sp) if rank == 0 else None
-    configs = per_config(g, torch, st, stream, peak, max(3, args.steps)) if rank == 0 else None
+    configs = per_config(g, torch, st, stream, peak, max(3, args.steps), tune) if rank == 0 else None
     tree_names = {}
     for t in trees:
         k = "-".join(g.tree_names(t))
@@ -626,6 +630,7 @@ def run_ours(args, world, rank, local):
                    "speedup_vs_plain_step": round(t_plain / t_step, 2),
                    "speedup_vs_plain_with_planning": round((t_plan_exh + t_plain) / (t_plan_learned + t_step), 2),
                    "batch_create_ms": round(1e3 * t_create, 1), "generate_s": round(t_gen, 1),
+                   "autotune": tune,
                    "trees": dict(sorted(tree_names.items(), key=lambda kv: -kv[1]))},
         "roofline": {"bound": "hbm", "kernel": f"{top[0]}:{top[1]}", "achieved": round(top_ach, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(top_ach / peak, 4), "peak_kind": peak_kind, "traffic": None,

@@ -136,6 +136,10 @@ def lib():
         L.gtsc_batch_status.argtypes = [vp, vp]
         L.gtsc_batch_launches.argtypes = [vp, i32]
         L.gtsc_batch_set_schedule.argtypes = [vp, i32]
+        L.gtsc_batch_create_tuned.argtypes = [ctypes.POINTER(Column), ctypes.c_uint32, i16p, i32p,
+                                              ctypes.POINTER(Tuning), ctypes.POINTER(vp), vp]
+        L.gtsc_batch_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        L.gtsc_batch_autotune.argtypes = [vp, ctypes.POINTER(Tuning), vp]
         L.gtsc_batch_schedule.argtypes = [vp]
         L.gtsc_batch_destroy.argtypes = [vp]
         L.gtsc_batch_profile.argtypes = [vp, i32, i32p, ctypes.POINTER(ctypes.c_float), u64p, u64p, i32, i32p, vp]
@@ -398,13 +402,41 @@ PASS_NAMES.update({-1: "set_streams", -2: "zero", -3: "frame_sizes", -4: "frame_
                    -6: "parse_frames", -7: "persistent"})
 
 
+class Tuning(ctypes.Structure):
+    """gtsc_batch_tuning: a batch's launch parameters (and the autotuner's report)."""
+    _fields_ = [("minmax_tile", ctypes.c_uint32), ("minmax_values_per_thread", ctypes.c_uint32),
+                ("hist_tile", ctypes.c_uint32), ("schedule_compress", ctypes.c_int32),
+                ("schedule_decompress", ctypes.c_int32), ("ms_default_compress", ctypes.c_float),
+                ("ms_default_decompress", ctypes.c_float), ("ms_tuned_compress", ctypes.c_float),
+                ("ms_tuned_decompress", ctypes.c_float), ("candidates", ctypes.c_int32),
+                ("seconds", ctypes.c_float)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        for k in ("schedule_compress", "schedule_decompress"):
+            d[k] = "persistent" if d[k] == 1 else "levels"
+        for k in d:
+            if isinstance(d[k], float):
+                d[k] = round(d[k], 4)
+        return d
+
+
+def tuning(minmax_tile=8192, minmax_values_per_thread=16, hist_tile=16384, persistent_compress=False,
+           persistent_decompress=False):
+    t = Tuning()
+    t.minmax_tile, t.minmax_values_per_thread, t.hist_tile = minmax_tile, minmax_values_per_thread, hist_tile
+    t.schedule_compress = 1 if persistent_compress else 0
+    t.schedule_decompress = 1 if persistent_decompress else 0
+    return t
+
+
 class Batch:
     """Many columns with their trees, compressed / decompressed by the batched engine.
 
     columns: DeviceBuffers (or objects with .ptr and .nbytes); dtypes: data type codes;
-    trees: node lists (int16 pairs) per column."""
+    trees: node lists (int16 pairs) per column; tuning: launch parameters (None = the defaults)."""
 
-    def __init__(self, columns, dtypes, trees, stream):
+    def __init__(self, columns, dtypes, trees, stream, tuning=None):
         self.stream = stream
         self.n = len(columns)
         cols = (Column * self.n)()
@@ -413,9 +445,10 @@ class Batch:
         counts = np.array([len(t) // 2 for t in trees], np.int32)
         nodes = np.ascontiguousarray(np.concatenate([np.asarray(t, np.int16) for t in trees]))
         h = ctypes.c_void_p()
-        check(lib().gtsc_batch_create(cols, self.n, nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
-                                      counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(h),
-                                      stream.handle), "batch_create")
+        check(lib().gtsc_batch_create_tuned(cols, self.n, nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
+                                            counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                            ctypes.byref(tuning) if tuning is not None else None, ctypes.byref(h),
+                                            stream.handle), "batch_create")
         self.handle = h.value
         self.sizes = [c.nbytes for c in columns]
 
@@ -457,6 +490,18 @@ class Batch:
 
     def schedule(self):
         return "persistent" if lib().gtsc_batch_schedule(self.handle) == 1 else "levels"
+
+    def tuning(self):
+        t = Tuning()
+        check(lib().gtsc_batch_get_tuning(self.handle, ctypes.byref(t)), "batch_get_tuning")
+        return t
+
+    def autotune(self):
+        """Chooses the schedule, min/max tile and values per thread and histogram tile by timing them
+        on this batch; returns the report (a dict).  The framed output buffer may move."""
+        t = Tuning()
+        check(lib().gtsc_batch_autotune(self.handle, ctypes.byref(t), self.stream.handle), "batch_autotune")
+        return t.as_dict()
 
     def profile(self, compress=True):
         """One step launch by launch: [(pass name, ms, bytes moved at least, blocks)]."""

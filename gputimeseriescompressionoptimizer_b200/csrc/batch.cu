@@ -13,6 +13,7 @@
 #include "scan.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <functional>
 #include <map>
 #include <tuple>
@@ -99,6 +100,8 @@ bool dyn_pass(int op)
     return op == B_SPLIT || op == B_RLE_HEADS || op == B_GFC_SCAN || op == B_DELTA_DEC || op == B_RLE_SCAN;
 }
 
+constexpr uint32_t kMinMaxTileMin = 1024;  // the smallest min/max tile (tiles are reserved for it)
+
 uint64_t gfc_warps_for(bool dbl, uint64_t n)
 {
     const uint64_t wpb = dbl ? 16 : 32;
@@ -129,7 +132,9 @@ public:
     PItem *d_pitem_c = nullptr, *d_pitem_d = nullptr;
     uint32_t *d_done_c = nullptr, *d_done_d = nullptr, *d_ext_c = nullptr, *d_ext_d = nullptr;
     uint32_t *d_queue = nullptr;  // [0] compress claim counter, [1] decode claim counter
-    bool persistent = false;      // the schedule the step graphs replay
+    BatchTuning tune;             // launch parameters (schedule, tile sizes)
+    std::vector<BatchColumn> src_cols;  // the columns (current inputs) and trees, for re-tuning
+    std::vector<Tree> src_trees;
     std::vector<uint32_t> item_of;           // tile -> item tables of every launch, back to back
     uint64_t copy_map_off = 0;
     uint32_t *d_item_of = nullptr;
@@ -281,7 +286,7 @@ void BatchEngine::plan_passes()
             break;
         case GTSC_DICT: case GTSC_CONST: {
             nd.split_tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
-            nd.hist_tiles = std::max<uint64_t>(1, cdiv(n, kBHistTile));
+            nd.hist_tiles = std::max<uint64_t>(1, cdiv(n, tune.hist_tile));
             uint64_t cap = 1024;
             while (cap < 2 * n + 64) cap <<= 1;
             nd.tab_cap = cap;
@@ -353,6 +358,15 @@ void BatchEngine::plan_passes()
         for (int j = 0; j < kMaxViewOps; j++) it.vop[j] = nd.vop[j];
         return it;
     };
+    // a min/max pass with the tuned tile (p[0]) and values per thread (p[1]); its tiles are
+    // reserved for the smallest tile the tuner tries, so that both can change without a rebuild
+    // (the pass skips tiles past its real extent)
+    auto minmax_item = [&](const HNode &nd, uint64_t n) {
+        BItem it = base_item(nd, B_MINMAX, cdiv(n, kMinMaxTileMin));
+        it.p[0] = tune.minmax_tile;
+        it.p[1] = tune.minmax_vpt;
+        return it;
+    };
 
     // ---------------- compress passes (parents before children)
     for (size_t id = 0; id < nodes.size(); id++) {
@@ -377,7 +391,7 @@ void BatchEngine::plan_passes()
             BItem vm = base_item(nd, B_VMETA, 1);
             vm.mode = (int16_t)nd.enc;
             if (nd.enc == GTSC_SCALE) {
-                add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+                add(minmax_item(nd, n));
                 add(vm);
             } else {
                 add(vm);
@@ -392,18 +406,18 @@ void BatchEngine::plan_passes()
         case GTSC_NONE: break;
         case GTSC_DELTA: add(base_item(nd, B_DELTA_ENC, t2k)); break;
         case GTSC_SCALE:
-            add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+            add(minmax_item(nd, n));
             add(base_item(nd, B_SCALE_SUB, t2k));
             break;
         case GTSC_AFL: {
             BItem pk = base_item(nd, B_AFL_PACK, t2k);
             if (scale_view) pk.vflags |= 1;  // width from the scale's min / max: no min/max pass
-            else if (!folded_minmax((int)id)) add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+            else if (!folded_minmax((int)id)) add(minmax_item(nd, n));
             add(pk);
             break;
         }
         case GTSC_PATCH: case GTSC_PATCH_OUTSIDE: {
-            BItem mm = base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile));
+            BItem mm = minmax_item(nd, n);
             mm.order = (int16_t)native_order(nd.dt);
             add(mm);
             BItem sp = base_item(nd, B_SPLIT, nd.split_tiles);
@@ -423,6 +437,7 @@ void BatchEngine::plan_passes()
             h.p[0] = nd.tab_cap;
             h.p[1] = nd.hist_tiles;
             h.p[2] = nd.tab_off;
+            h.p[3] = tune.hist_tile;
             add(h);
             BItem tk = h;
             tk.op = B_TOPK;
@@ -478,7 +493,7 @@ void BatchEngine::plan_passes()
             } else {
                 BItem pk = base_item(nd, B_AFL_PACK, t2k);
                 if (scale_view) pk.vflags |= 1;
-                else if (!folded_minmax((int)id)) add(base_item(nd, B_MINMAX, cdiv(n, kBMinMaxTile)));
+                else if (!folded_minmax((int)id)) add(minmax_item(nd, n));
                 add(pk);
             }
             break;
@@ -1004,14 +1019,26 @@ void BatchEngine::capture(cudaStream_t s)
 
 // ---------------------------------------------------------------------------------- public
 
-BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vector<Tree> &trees, cudaStream_t s)
+BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vector<Tree> &trees, cudaStream_t s,
+                          const BatchTuning &tuning)
 {
     if (cols.empty() || cols.size() != trees.size()) fail(GTSC_ERR_ARG, "batch: columns and trees differ in number");
     if (!s) fail(GTSC_ERR_ARG, "batch: needs a non-default stream (steps are captured as CUDA graphs)");
     if (cols.size() >= (1u << 24)) fail(GTSC_ERR_ARG, "batch: at most 2^24 - 1 columns");
     for (const auto &c : cols)
         if (!aligned16(c.data)) fail(GTSC_ERR_ARG, "batch: column pointers must be 16-byte aligned");
+    if (tuning.minmax_vpt != 1 && tuning.minmax_vpt != 2 && tuning.minmax_vpt != 4 && tuning.minmax_vpt != 8 &&
+        tuning.minmax_vpt != 16)
+        fail(GTSC_ERR_ARG, "batch: min/max values per thread must be 1, 2, 4, 8 or 16");
+    if (tuning.minmax_tile < kMinMaxTileMin || tuning.minmax_tile % (256 * tuning.minmax_vpt) ||
+        tuning.minmax_tile > (1u << 20))
+        fail(GTSC_ERR_ARG, "batch: the min/max tile must be a multiple of 256 x its values per thread, 1K .. 1M");
+    if (tuning.hist_tile < 256 || tuning.hist_tile % 256 || tuning.hist_tile > (1u << 20))
+        fail(GTSC_ERR_ARG, "batch: the histogram tile must be a multiple of 256");
     std::unique_ptr<BatchEngine> e(new BatchEngine());
+    e->tune = tuning;
+    e->src_cols = cols;
+    e->src_trees = trees;
     for (size_t c = 0; c < cols.size(); c++) {
         const Tree &t = trees[c];
         if (t.size() == 0 || t.dt[0] != cols[c].dtype) fail(GTSC_ERR_ARG, "batch: tree root type differs from the column");
@@ -1059,10 +1086,11 @@ void batch_destroy(BatchEngine *e)
     delete e;
 }
 
-void batch_compress(BatchEngine *e, cudaStream_t s) { GTSC_CUDA(cudaGraphLaunch(e->graph_c[e->persistent], s)); }
+void batch_compress(BatchEngine *e, cudaStream_t s) { GTSC_CUDA(cudaGraphLaunch(e->graph_c[e->tune.persistent_c], s)); }
 
-void batch_set_schedule(BatchEngine *e, bool persistent) { e->persistent = persistent; }
-bool batch_schedule(const BatchEngine *e) { return e->persistent; }
+void batch_set_schedule(BatchEngine *e, bool persistent) { e->tune.persistent_c = e->tune.persistent_d = persistent; }
+bool batch_schedule(const BatchEngine *e) { return e->tune.persistent_c && e->tune.persistent_d; }
+BatchTuning batch_tuning(const BatchEngine *e) { return e->tune; }
 
 void batch_set_inputs(BatchEngine *e, const std::vector<const void *> &inputs, cudaStream_t s)
 {
@@ -1076,6 +1104,7 @@ void batch_set_inputs(BatchEngine *e, const std::vector<const void *> &inputs, c
         vals.push_back(e->col_bytes[c]);
     }
     GTSC_CUDA(cudaMemcpyAsync(e->d_set_vals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, s));
+    for (size_t c = 0; c < nc; c++) e->src_cols[c].data = inputs[c];
 }
 
 uint64_t batch_output_bytes(BatchEngine *e, cudaStream_t s)
@@ -1110,7 +1139,7 @@ void batch_decompress(BatchEngine *e, const uint8_t *framed, uint64_t framed_byt
     GTSC_CUDA(cudaMemcpyAsync(e->d_set_vals + 2 * nc, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, s));
     unsigned long long fr[2] = {(unsigned long long)(uintptr_t)framed, framed_bytes};
     GTSC_CUDA(cudaMemcpyAsync(e->d_frame_ptr, fr, 16, cudaMemcpyHostToDevice, s));
-    GTSC_CUDA(cudaGraphLaunch(e->graph_d[e->persistent], s));
+    GTSC_CUDA(cudaGraphLaunch(e->graph_d[e->tune.persistent_d], s));
 }
 
 // Bytes a pass must move at least: its inputs read and its outputs written (from the stream table
@@ -1162,8 +1191,8 @@ std::vector<BatchLaunchProfile> batch_profile(BatchEngine *e, bool compress, cud
             marks.push_back(m);
             GTSC_CUDA(cudaEventRecord(new_event(), s));
         };
-        if (compress) e->record_compress(s, mark, e->persistent);
-        else e->record_decompress(s, mark, e->persistent);
+        if (compress) e->record_compress(s, mark, e->tune.persistent_c);
+        else e->record_decompress(s, mark, e->tune.persistent_d);
         GTSC_CUDA(cudaStreamSynchronize(s));
         std::vector<StreamDesc> S(e->streams.size());
         d2h(S.data(), e->d_streams, S.size() * sizeof(StreamDesc), s);
@@ -1197,6 +1226,169 @@ std::vector<BatchLaunchProfile> batch_profile(BatchEngine *e, bool compress, cud
     return out;
 }
 
+// ---------------------------------------------------------------------------------- autotuner
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+// median milliseconds of `reps` steps (after one untimed step), CUDA events on s
+float time_step(BatchEngine *e, bool compress, const uint8_t *framed, uint64_t framed_bytes,
+                const std::vector<void *> &outs, cudaStream_t s, int reps)
+{
+    auto one = [&]() {
+        if (compress) batch_compress(e, s);
+        else batch_decompress(e, framed, framed_bytes, outs, s);
+    };
+    one();
+    std::vector<float> t;
+    cudaEvent_t a, b;
+    GTSC_CUDA(cudaEventCreate(&a));
+    GTSC_CUDA(cudaEventCreate(&b));
+    for (int r = 0; r < reps; r++) {
+        GTSC_CUDA(cudaEventRecord(a, s));
+        one();
+        GTSC_CUDA(cudaEventRecord(b, s));
+        GTSC_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        GTSC_CUDA(cudaEventElapsedTime(&ms, a, b));
+        t.push_back(ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    std::sort(t.begin(), t.end());
+    return t[t.size() / 2];
+}
+
+// the summed time of the compress launches of the given pass kinds (min over `reps` profiles)
+float time_passes(BatchEngine *e, std::initializer_list<int> ops, cudaStream_t s, int reps)
+{
+    float best = 1e30f;
+    for (int r = 0; r < reps; r++) {
+        float sum = 0;
+        for (const auto &p : batch_profile(e, true, s))
+            for (int op : ops)
+                if (p.op == op) sum += p.ms;
+        best = std::min(best, sum);
+    }
+    return best;
+}
+
+}  // namespace
+
+// the min/max tile and values per thread of every min/max item (no rebuild: tiles are reserved for
+// the smallest tile)
+static void set_minmax_params(BatchEngine *e, uint32_t tile, uint32_t vpt, cudaStream_t s)
+{
+    for (auto &it : e->items_c)
+        if (it.op == B_MINMAX) {
+            it.p[0] = tile;
+            it.p[1] = vpt;
+        }
+    GTSC_CUDA(cudaMemcpyAsync(e->d_items_c, e->items_c.data(), e->items_c.size() * sizeof(BItem),
+                              cudaMemcpyHostToDevice, s));
+    GTSC_CUDA(cudaStreamSynchronize(s));
+    e->tune.minmax_tile = tile;
+    e->tune.minmax_vpt = vpt;
+}
+
+BatchEngine *batch_autotune(BatchEngine *e, cudaStream_t s, TuneReport *report)
+{
+    const auto t_start = Clock::now();
+    TuneReport rep;
+    int cands = 0;
+    // decode outputs for the timing (one allocation, 256-byte aligned pieces)
+    uint64_t out_bytes = 0;
+    for (uint64_t b : e->col_bytes) out_bytes += align_up(std::max<uint64_t>(b, 16), 256);
+    DevBuf outbuf = dev_alloc(out_bytes, s);
+    std::vector<void *> outs;
+    uint64_t off = 0;
+    for (uint64_t b : e->col_bytes) {
+        outs.push_back(outbuf.get() + off);
+        off += align_up(std::max<uint64_t>(b, 16), 256);
+    }
+    auto measure = [&](BatchEngine *x, float ms[2]) {
+        batch_compress(x, s);
+        const uint64_t fb = batch_output_bytes(x, s);
+        ms[0] = time_step(x, true, nullptr, 0, outs, s, 5);
+        ms[1] = time_step(x, false, batch_output(x), fb, outs, s, 5);
+        if (batch_status(x, s) != GTSC_OK) fail(GTSC_ERR_FORMAT, "autotune: a candidate step failed");
+    };
+    // 1. the schedule of each step (both recorded in every batch: no rebuild)
+    BatchTuning best = e->tune;
+    best.persistent_c = best.persistent_d = false;
+    e->tune.persistent_c = e->tune.persistent_d = false;
+    measure(e, rep.ms_default);
+    e->tune.persistent_c = e->tune.persistent_d = true;
+    float pers[2];
+    measure(e, pers);
+    cands += 2;
+    best.persistent_c = pers[0] < rep.ms_default[0];
+    best.persistent_d = pers[1] < rep.ms_default[1];
+    e->tune.persistent_c = best.persistent_c;
+    e->tune.persistent_d = best.persistent_d;
+    // 2. the min/max tile x values per thread, on the min/max launches of the level schedule
+    const bool keep_c = e->tune.persistent_c;
+    e->tune.persistent_c = false;
+    batch_compress(e, s);
+    float best_mm = time_passes(e, {B_MINMAX}, s, 3);
+    for (uint32_t tile : {1024u, 2048u, 4096u, 8192u, 16384u})
+        for (uint32_t vpt : {1u, 2u, 4u, 8u, 16u}) {
+            if (tile % (256 * vpt) || (tile == best.minmax_tile && vpt == best.minmax_vpt)) continue;
+            set_minmax_params(e, tile, vpt, s);
+            const float t = time_passes(e, {B_MINMAX}, s, 3);
+            ++cands;
+            if (t < best_mm * 0.98f) {
+                best_mm = t;
+                best.minmax_tile = tile;
+                best.minmax_vpt = vpt;
+            }
+        }
+    set_minmax_params(e, best.minmax_tile, best.minmax_vpt, s);
+    e->tune.persistent_c = keep_c;
+    // 3. the histogram tile (it sizes the top-k pass's tiles: a rebuild per candidate)
+    const bool has_hist = std::any_of(e->items_c.begin(), e->items_c.end(), [](const BItem &it) { return it.op == B_HIST; });
+    if (has_hist) {
+        e->tune.persistent_c = false;
+        float best_h = time_passes(e, {B_HIST, B_TOPK}, s, 3);
+        e->tune.persistent_c = keep_c;
+        for (uint32_t tile : {4096u, 8192u, 16384u}) {
+            if (tile == best.hist_tile) continue;
+            BatchTuning cand = best;
+            cand.hist_tile = tile;
+            cand.persistent_c = false;
+            BatchEngine *x = batch_create(e->src_cols, e->src_trees, s, cand);
+            float t = 1e30f;
+            try {
+                batch_compress(x, s);
+                t = time_passes(x, {B_HIST, B_TOPK}, s, 3);
+            } catch (...) {
+                batch_destroy(x);
+                throw;
+            }
+            batch_destroy(x);
+            ++cands;
+            if (t < best_h * 0.98f) {
+                best_h = t;
+                best.hist_tile = tile;
+            }
+        }
+    }
+    // the tuned batch
+    BatchEngine *out = e;
+    if (best.hist_tile != e->tune.hist_tile) {
+        out = batch_create(e->src_cols, e->src_trees, s, best);
+        batch_destroy(e);
+    }
+    out->tune = best;
+    measure(out, rep.ms_tuned);
+    rep.best = best;
+    rep.candidates = cands;
+    rep.seconds = std::chrono::duration<float>(Clock::now() - t_start).count();
+    if (report) *report = rep;
+    return out;
+}
+
 gtsc_status batch_status(BatchEngine *e, cudaStream_t s)
 {
     uint32_t w = 0;
@@ -1208,7 +1400,7 @@ int batch_launches(BatchEngine *e, bool compress)
 {
     // compress: set streams, zero, stages, frame sizes / layout / copy; decompress: set streams,
     // zero, parse directory + frames, stages
-    if (e->persistent) return compress ? 6 : 4;
+    if (compress ? e->tune.persistent_c : e->tune.persistent_d) return compress ? 6 : 4;
     return compress ? (int)e->launch_c.size() + 5 : (int)e->launch_d.size() + 4;
 }
 

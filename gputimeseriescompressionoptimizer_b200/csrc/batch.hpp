@@ -121,8 +121,34 @@ struct BatchColumn {
 
 class BatchEngine;
 
+// Launch parameters chosen per batch by the autotuner (batch_autotune); the defaults are the
+// hand-picked values.  Tiles are values per block tile.
+struct BatchTuning {
+    uint32_t minmax_tile = 8192;   // min/max pass: a multiple of 256 x minmax_vpt, 1K .. 16K
+    uint32_t minmax_vpt = 16;      // min/max pass: consecutive values a thread loads per round (1 .. 16)
+    uint32_t hist_tile = 16384;    // histogram pass (dict / const), 1K .. 16K
+    bool persistent_c = false;     // compress step: one persistent launch instead of the levels
+    bool persistent_d = false;     // decompress step: the same
+};
+
 // Compile a batch: columns + their (Fix()ed) trees.  Owns the arena and the graphs.
-BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vector<Tree> &trees, cudaStream_t s);
+BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vector<Tree> &trees, cudaStream_t s,
+                          const BatchTuning &tuning = BatchTuning());
+// the batch's launch parameters
+BatchTuning batch_tuning(const BatchEngine *e);
+// Times candidate launch parameters on the batch's own columns and trees (CUDA events, each
+// candidate compiled as a batch of its own): the schedule of each step, then the min/max tile x
+// values per thread, then the histogram tile, each kept when it lowers the time of the passes it
+// affects.  Returns a batch built with the best parameters (the old one is destroyed), and the
+// step times before and after.
+struct TuneReport {
+    BatchTuning best;
+    float ms_default[2] = {0, 0};  // compress, decompress with the default parameters
+    float ms_tuned[2] = {0, 0};
+    int candidates = 0;
+    float seconds = 0;
+};
+BatchEngine *batch_autotune(BatchEngine *e, cudaStream_t s, TuneReport *report);
 void batch_destroy(BatchEngine *e);
 // compress all columns into the framed output: uint64 column count, uint64 blob bytes per column,
 // then the blobs (CompressionTree::Compress of each column) back to back
@@ -222,8 +248,6 @@ void launch_batch_stage(int op, const BItem *d_items, const uint32_t *d_item_of,
 // tile sizes (elements) of the batched passes
 constexpr uint32_t kBVPT = 16;         // values per thread of the element-wise and look-back passes
 constexpr uint32_t kBTile = 256 * kBVPT; // elements per tile of those passes (256 threads per block)
-constexpr uint32_t kBMinMaxTile = 8192;
-constexpr uint32_t kBHistTile = 16384;
 constexpr uint32_t kBMergeSub = 4;      // kBTile tiles per block of the merge pass
 constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
 constexpr uint32_t kBHistSmem = 2048;    // shared hash slots of a histogram block (8-byte values)

@@ -21,16 +21,34 @@ namespace gtsc {
 namespace {
 
 // ------------------------------------------------------------------------------- min / max
-template <int ES>
-__device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
+// VPT values of a view starting at base (zeros past the view): one vector run when a run is whole
+// 16-byte chunks, else element loads
+template <int ES, int VPT>
+__device__ __forceinline__ void load_view_any(const BItem &it, const ViewCtx &vc, const uint8_t *src, uint64_t base,
+                                              uint64_t (&v)[VPT])
+{
+    if constexpr ((VPT * ES) % 16 == 0) {
+        load_view<ES, VPT>(it, vc, src, base, v);
+    } else {
+#pragma unroll
+        for (int j = 0; j < VPT; j++) v[j] = base + j < vc.n ? view_elem<ES>(it, vc, src, base + j) : 0;
+    }
+}
+
+// A tile of it.p[0] values (the tuned min/max tile; a multiple of kBThreads * VPT): rounds of VPT
+// consecutive values a thread, two rounds loaded before either is reduced.
+template <int ES, int VPT>
+__device__ void p_minmax_v(const BItem &it, uint32_t tile, StreamDesc *S)
 {
     const StreamDesc in = S[it.in[0]];
     const ViewCtx vc = view_ctx<ES>(it, in);
     const uint64_t n = vc.n;
-    const uint64_t t0 = (uint64_t)tile * kBMinMaxTile;
+    const uint64_t T = it.p[0];
+    const uint64_t t0 = (uint64_t)tile * T;
     if (t0 >= n) return;
-    const uint64_t end = n < t0 + kBMinMaxTile ? n : t0 + kBMinMaxTile;
+    const uint64_t end = n < t0 + T ? n : t0 + T;
     const Order o = (Order)it.order;
+    constexpr uint64_t R = (uint64_t)kBThreads * VPT;  // values of one round of the block
     uint64_t kmin = ~0ull, kmax = 0;
     if constexpr (ES <= 4) {
         // 32-bit keys of the same order (sign bit flipped for integers, order_key's map for floats),
@@ -43,30 +61,30 @@ __device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
             if (f32) return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
             return (uint32_t)((int32_t)(u << SH) >> SH) ^ 0x80000000u;
         };
-        // the tile's two runs of 16 values a thread are both loaded before either is reduced
-        static_assert(kBMinMaxTile == 2 * kBThreads * kBVPT, "a min/max tile is two runs a thread");
-        const uint64_t b0 = t0 + (uint64_t)threadIdx.x * kBVPT, b1 = b0 + (uint64_t)kBThreads * kBVPT;
-        uint32_t u[2][kBVPT];
-        {
-            uint64_t v[kBVPT];
-            load_view<ES, kBVPT>(it, vc, in.ptr, b0, v);
+        for (uint64_t b0 = t0 + (uint64_t)threadIdx.x * VPT; b0 < end; b0 += 2 * R) {
+            const uint64_t b1 = b0 + R;
+            uint32_t u[2][VPT];
+            {
+                uint64_t v[VPT];
+                load_view_any<ES, VPT>(it, vc, in.ptr, b0, v);
 #pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) u[0][j] = (uint32_t)v[j];
-            if (b1 < end) load_view<ES, kBVPT>(it, vc, in.ptr, b1, v);
+                for (int j = 0; j < VPT; j++) u[0][j] = (uint32_t)v[j];
+                if (b1 < end) load_view_any<ES, VPT>(it, vc, in.ptr, b1, v);
 #pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) u[1][j] = (uint32_t)v[j];
-        }
+                for (int j = 0; j < VPT; j++) u[1][j] = (uint32_t)v[j];
+            }
 #pragma unroll
-        for (int r = 0; r < 2; r++) {
-            const uint64_t base = r ? b1 : b0;
-            const uint32_t cnt = base >= end ? 0u : end - base < kBVPT ? (uint32_t)(end - base) : kBVPT;
+            for (int r = 0; r < 2; r++) {
+                const uint64_t base = r ? b1 : b0;
+                const uint32_t cnt = base >= end ? 0u : end - base < (uint64_t)VPT ? (uint32_t)(end - base) : VPT;
 #pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) {
-                const bool ok = (uint32_t)j < cnt && !(f32 && (u[r][j] & 0x7fffffffu) > 0x7f800000u);
-                const uint32_t k = key32(u[r][j]);
-                k32min = ok && k < k32min ? k : k32min;
-                k32max = ok && k > k32max ? k : k32max;
-                seen |= ok;
+                for (int j = 0; j < VPT; j++) {
+                    const bool ok = (uint32_t)j < cnt && !(f32 && (u[r][j] & 0x7fffffffu) > 0x7f800000u);
+                    const uint32_t k = key32(u[r][j]);
+                    k32min = ok && k < k32min ? k : k32min;
+                    k32max = ok && k > k32max ? k : k32max;
+                    seen |= ok;
+                }
             }
         }
         if (seen) {
@@ -78,11 +96,11 @@ __device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
             kmax = order_key(umax, 4, o);
         }
     } else {
-        for (uint64_t base = t0 + (uint64_t)threadIdx.x * kBVPT; base < end; base += (uint64_t)kBThreads * kBVPT) {
-            uint64_t v[kBVPT];
-            load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+        for (uint64_t base = t0 + (uint64_t)threadIdx.x * VPT; base < end; base += R) {
+            uint64_t v[VPT];
+            load_view_any<ES, VPT>(it, vc, in.ptr, base, v);
 #pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) {
+            for (int j = 0; j < VPT; j++) {
                 if (base + j >= end || is_nan_bits(v[j], o)) continue;
                 const uint64_t k = order_key(v[j], ES, o);
                 kmin = k < kmin ? k : kmin;
@@ -95,6 +113,19 @@ __device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
         MinMaxAcc *acc = (MinMaxAcc *)it.scratch;
         if (kmin != ~0ull) atomicMax(&acc->nkmin, (unsigned long long)~kmin);
         if (kmax != 0) atomicMax(&acc->kmax, (unsigned long long)kmax);
+    }
+}
+
+// the min/max pass with the tuned values per thread (it.p[1]: 1, 2, 4, 8 or 16)
+template <int ES>
+__device__ void p_minmax(const BItem &it, uint32_t tile, StreamDesc *S)
+{
+    switch (it.p[1]) {
+    case 1: p_minmax_v<ES, 1>(it, tile, S); break;
+    case 2: p_minmax_v<ES, 2>(it, tile, S); break;
+    case 4: p_minmax_v<ES, 4>(it, tile, S); break;
+    case 8: p_minmax_v<ES, 8>(it, tile, S); break;
+    default: p_minmax_v<ES, 16>(it, tile, S); break;
     }
 }
 
@@ -382,13 +413,14 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
     const StreamDesc in = S[it.in[0]];
     const ViewCtx vc = view_ctx<ES>(it, in);
     const uint64_t n = vc.n;
-    const uint64_t t0 = (uint64_t)tile * kBHistTile;
+    const uint64_t HT = it.p[3];  // the tuned histogram tile
+    const uint64_t t0 = (uint64_t)tile * HT;
     const HTab t = htab(it);
     const Order o = (Order)it.order;
     if (it.mode == 4 && t0 < n) {
         // dict: clear this tile's share of the 2-bit code words (out1 after its 16 + 4*es header)
         uint32_t *words = (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES);
-        const uint64_t e_end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
+        const uint64_t e_end = n < t0 + HT ? n : t0 + HT;
         for (uint64_t w = t0 / 16 + threadIdx.x; w < (e_end + 15) / 16; w += kBThreads) words[w] = 0u;
     }
     unsigned long long nan_min[4] = {EMPTY, EMPTY, EMPTY, EMPTY};
@@ -405,7 +437,7 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         }
         if (threadIdx.x == 0) s_ones = 0;
         __syncthreads();
-        const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
+        const uint64_t end = n < t0 + HT ? n : t0 + HT;
         // the next element's load is in flight while this one is inserted; every lane runs the
         // same rounds, so that the warp can vote on its 32 elements
         unsigned long long next = t0 + threadIdx.x < end ? view_elem<ES>(it, vc, in.ptr, t0 + threadIdx.x) : 0ull;
@@ -476,7 +508,7 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
             scounts[i] = 0;
         }
         __syncthreads();
-        const uint64_t end = n < t0 + kBHistTile ? n : t0 + kBHistTile;
+        const uint64_t end = n < t0 + HT ? n : t0 + HT;
         for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
             const unsigned long long key = view_elem<ES>(it, vc, in.ptr, i);
             if (is_nan_bits(key, o)) {
@@ -1292,7 +1324,7 @@ __device__ __forceinline__ uint32_t stage_extent(const BItem &it, const StreamDe
         return n_src > (uint64_t)nd ? n_src - nd : 0;
     };
     uint64_t e = it.tiles;
-    if constexpr (OP == B_MINMAX) e = cdiv(view_n(), kBMinMaxTile);
+    if constexpr (OP == B_MINMAX) e = cdiv(view_n(), it.p[0]);  // the tuned min/max tile
     else if constexpr (OP == B_DELTA_ENC) {
         const uint64_t n = view_n();
         e = cdiv(n ? n - 1 : 0, kBTile);

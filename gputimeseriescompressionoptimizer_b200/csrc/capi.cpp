@@ -230,8 +230,29 @@ struct gtsc_batch {
     uint32_t n_cols;
 };
 
-gtsc_status gtsc_batch_create(const gtsc_column *cols, uint32_t n_cols, const int16_t *nodes,
-                              const int32_t *node_counts, gtsc_batch **out, void *stream)
+static BatchTuning to_tuning(const gtsc_batch_tuning &t)
+{
+    BatchTuning b;
+    b.minmax_tile = t.minmax_tile;
+    b.minmax_vpt = t.minmax_values_per_thread;
+    b.hist_tile = t.hist_tile;
+    b.persistent_c = t.schedule_compress == GTSC_SCHEDULE_PERSISTENT;
+    b.persistent_d = t.schedule_decompress == GTSC_SCHEDULE_PERSISTENT;
+    return b;
+}
+
+static void from_tuning(const BatchTuning &b, gtsc_batch_tuning *t)
+{
+    t->minmax_tile = b.minmax_tile;
+    t->minmax_values_per_thread = b.minmax_vpt;
+    t->hist_tile = b.hist_tile;
+    t->schedule_compress = b.persistent_c ? GTSC_SCHEDULE_PERSISTENT : GTSC_SCHEDULE_LEVELS;
+    t->schedule_decompress = b.persistent_d ? GTSC_SCHEDULE_PERSISTENT : GTSC_SCHEDULE_LEVELS;
+}
+
+gtsc_status gtsc_batch_create_tuned(const gtsc_column *cols, uint32_t n_cols, const int16_t *nodes,
+                                    const int32_t *node_counts, const gtsc_batch_tuning *tuning, gtsc_batch **out,
+                                    void *stream)
 {
     return guard([&] {
         if (!cols || !nodes || !node_counts || !out || !n_cols) fail(GTSC_ERR_ARG, "null argument");
@@ -243,8 +264,42 @@ gtsc_status gtsc_batch_create(const gtsc_column *cols, uint32_t n_cols, const in
             t.push_back(tree_from_nodes(p, node_counts[i]));
             p += 2 * node_counts[i];
         }
-        BatchEngine *e = batch_create(c, t, S(stream));
+        BatchEngine *e = batch_create(c, t, S(stream), tuning ? to_tuning(*tuning) : BatchTuning());
         *out = new gtsc_batch{e, n_cols};
+    });
+}
+
+gtsc_status gtsc_batch_create(const gtsc_column *cols, uint32_t n_cols, const int16_t *nodes,
+                              const int32_t *node_counts, gtsc_batch **out, void *stream)
+{
+    return gtsc_batch_create_tuned(cols, n_cols, nodes, node_counts, nullptr, out, stream);
+}
+
+gtsc_status gtsc_batch_get_tuning(gtsc_batch *b, gtsc_batch_tuning *tuning)
+{
+    return guard([&] {
+        if (!b || !tuning) fail(GTSC_ERR_ARG, "null argument");
+        *tuning = gtsc_batch_tuning{};
+        from_tuning(batch_tuning(b->e), tuning);
+    });
+}
+
+gtsc_status gtsc_batch_autotune(gtsc_batch *b, gtsc_batch_tuning *report, void *stream)
+{
+    return guard([&] {
+        if (!b) fail(GTSC_ERR_ARG, "null batch");
+        TuneReport rep;
+        b->e = batch_autotune(b->e, S(stream), &rep);
+        if (report) {
+            *report = gtsc_batch_tuning{};
+            from_tuning(rep.best, report);
+            report->ms_default_compress = rep.ms_default[0];
+            report->ms_default_decompress = rep.ms_default[1];
+            report->ms_tuned_compress = rep.ms_tuned[0];
+            report->ms_tuned_decompress = rep.ms_tuned[1];
+            report->candidates = rep.candidates;
+            report->seconds = rep.seconds;
+        }
     });
 }
 

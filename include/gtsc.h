@@ -205,6 +205,38 @@ enum { GTSC_SCHEDULE_LEVELS = 0, GTSC_SCHEDULE_PERSISTENT = 1 };
 gtsc_status gtsc_batch_set_schedule(gtsc_batch *b, int32_t schedule);
 int32_t gtsc_batch_schedule(gtsc_batch *b);
 /*
+ * Launch parameters of a batch, and the autotuner that chooses them (no counterpart in the
+ * reference, whose launch configuration is fixed, core/execution_policy.hpp:14-49).  Tiles are
+ * values per block tile.  Defaults: min/max tile 8192 with 16 values per thread, histogram tile
+ * 16384, level schedule for both steps.
+ */
+typedef struct {
+    uint32_t minmax_tile;               /* 1024 .. 16384, a multiple of 256 x the values per thread */
+    uint32_t minmax_values_per_thread;  /* consecutive values a thread loads per round: 1, 2, 4, 8, 16 */
+    uint32_t hist_tile;                 /* dict / const histogram: 4096, 8192 or 16384 */
+    int32_t schedule_compress;          /* GTSC_SCHEDULE_* */
+    int32_t schedule_decompress;
+    /* filled by gtsc_batch_autotune: step times (ms) with the default and with the chosen
+     * parameters, candidates timed, seconds spent */
+    float ms_default_compress, ms_default_decompress, ms_tuned_compress, ms_tuned_decompress;
+    int32_t candidates;
+    float seconds;
+} gtsc_batch_tuning;
+/* gtsc_batch_create with explicit launch parameters (NULL: the defaults) */
+gtsc_status gtsc_batch_create_tuned(const gtsc_column *cols, uint32_t n_cols, const int16_t *nodes,
+                                    const int32_t *node_counts, const gtsc_batch_tuning *tuning, gtsc_batch **out,
+                                    void *stream);
+gtsc_status gtsc_batch_get_tuning(gtsc_batch *b, gtsc_batch_tuning *tuning);
+/*
+ * Times candidate parameters on the batch's own columns and trees with CUDA events: the schedule of
+ * each step; then the min/max tile (1K .. 16K) x values per thread (1 .. 16) on the min/max
+ * launches; then the histogram tile (4K .. 16K) on the histogram and top-k launches (a rebuild
+ * each); a candidate is kept when it is at least 2 % faster.  The batch keeps the best parameters
+ * (its device buffers, the framed output included, may move: call gtsc_batch_output again).
+ * Synchronises; a few seconds for hundreds of columns.  *report may be NULL.
+ */
+gtsc_status gtsc_batch_autotune(gtsc_batch *b, gtsc_batch_tuning *report, void *stream);
+/*
  * One step run launch by launch with CUDA events between the launches (not the graph): per launch
  * its pass kind (ops[i] >= 0, or -1 stream setup, -2 scratch zeroing, -3/-4/-5 frame sizes / layout
  * / copy, -6 frame parse, -7 the persistent launch of every pass), its time in ms, the bytes it must read and write at least (its input and

@@ -32,10 +32,10 @@ def framed_blobs(G, b):
     return p, nb, framed, G.split_framed(framed)
 
 
-def run_batch(G, O, cols, dtypes, trees, steps=1):
+def run_batch(G, O, cols, dtypes, trees, steps=1, tuning=None):
     st = G.Stream()
     devs = [G.to_device(x) for x in cols]
-    b = G.Batch(devs, dtypes, trees, st)
+    b = G.Batch(devs, dtypes, trees, st, tuning=tuning)
     assert b.launches(True) > 0 and b.launches(False) > 0
     first = None
     for _ in range(steps):
@@ -256,3 +256,68 @@ def test_batch_view_chains_float(G, O, rng, dt):
             dts.append(dt)
             trees.append(G.tree_from_path(path, dt))
     run_batch(G, O, cols, dts, trees)
+
+
+# launch parameters the autotuner may choose (gtsc_batch_tuning)
+TUNINGS = [dict(minmax_tile=1024, minmax_values_per_thread=1),
+           dict(minmax_tile=2048, minmax_values_per_thread=2, hist_tile=4096),
+           dict(minmax_tile=4096, minmax_values_per_thread=4, hist_tile=8192),
+           dict(minmax_tile=16384, minmax_values_per_thread=8),
+           dict(minmax_tile=16384, minmax_values_per_thread=16, persistent_compress=True, persistent_decompress=True)]
+
+
+def tuning_columns(G, rng):
+    """columns whose trees run the min/max (AFL, scale, patch) and histogram (dict, const) passes,
+    over every element size and over views"""
+    cols, dts, trees = [], [], []
+    paths = [[OR.AFL, OR.NONE], [OR.SCALE, OR.AFL, OR.NONE], [OR.DELTA, OR.SCALE, OR.AFL, OR.NONE],
+             [OR.PATCH, OR.AFL, OR.NONE, OR.AFL, OR.NONE], [OR.DICT, OR.AFL, OR.NONE, OR.AFL, OR.NONE],
+             [OR.CONST, OR.AFL, OR.NONE], [OR.DELTA, OR.DICT, OR.NONE, OR.NONE]]
+    for dt in [OR.CHAR, OR.SHORT, OR.INT, OR.TIME]:
+        for path in paths:
+            for n in [1, 300, 5000, 70001]:
+                for kind in ["int", "b"]:
+                    cols.append(gen(rng, kind, dt, n))
+                    dts.append(dt)
+                    trees.append(G.tree_from_path(path, dt))
+    for dt in [OR.FLOAT, OR.DOUBLE]:
+        for path in [[OR.PATCH, OR.GFC, OR.NONE, OR.NONE, OR.GFC, OR.NONE, OR.NONE],
+                     [OR.DICT, OR.NONE, OR.GFC, OR.NONE, OR.NONE], [OR.CONST, OR.GFC, OR.NONE, OR.NONE]]:
+            for n in [7, 40000]:
+                cols.append(W.column("price", dt, n, int(rng.integers(1 << 30))))
+                dts.append(dt)
+                trees.append(G.tree_from_path(path, dt))
+    return cols, dts, trees
+
+
+@pytest.mark.parametrize("tk", range(len(TUNINGS)), ids=[str(i) for i in range(len(TUNINGS))])
+def test_batch_tuned_parameters(G, O, rng, tk):
+    """every min/max tile x values per thread, histogram tile and schedule the autotuner may choose
+    gives byte-identical blobs and bit-exact decodes"""
+    cols, dts, trees = tuning_columns(G, rng)
+    b, _, _ = run_batch(G, O, cols, dts, trees, tuning=G.tuning(**TUNINGS[tk]))
+    t = b.tuning()
+    assert t.minmax_tile == TUNINGS[tk]["minmax_tile"] and t.minmax_values_per_thread == TUNINGS[tk]["minmax_values_per_thread"]
+
+
+def test_batch_autotune(G, O, rng):
+    """the autotuner reports its choice and timings, and the tuned batch still writes the oracle's
+    blobs and decodes them bit-exact"""
+    cols, dts, trees = tuning_columns(G, rng)
+    st = G.Stream()
+    devs = [G.to_device(x) for x in cols]
+    b = G.Batch(devs, dts, trees, st)
+    rep = b.autotune()
+    assert rep["candidates"] >= 2 and rep["seconds"] > 0
+    assert rep["ms_default_compress"] > 0 and rep["ms_tuned_compress"] > 0
+    assert rep["minmax_tile"] % (256 * rep["minmax_values_per_thread"]) == 0
+    b.compress()
+    b.status()
+    p, nb, framed, blobs = framed_blobs(G, b)
+    for i, x in enumerate(cols):
+        assert np.array_equal(blobs[i], O.tree_compress(trees[i], x)), i
+    outs = [G.alloc(x.nbytes) for x in cols]
+    b.decompress(p, nb, outs)
+    b.status()
+    for i, x in enumerate(cols):
+        assert G.to_host(outs[i]).tobytes() == x.tobytes(), i
