@@ -376,7 +376,7 @@ __device__ __forceinline__ HTab htab(const BItem &it)
     return t;
 }
 
-__device__ __noinline__ void g_insert(const HTab &t, unsigned long long key, unsigned int c, uint32_t *status)
+__device__ void g_insert(const HTab &t, unsigned long long key, unsigned int c, uint32_t *status)
 {
     constexpr unsigned long long EMPTY = ~0ull;
     if (key == EMPTY) {
@@ -438,40 +438,11 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         if (threadIdx.x == 0) s_ones = 0;
         __syncthreads();
         const uint64_t end = n < t0 + HT ? n : t0 + HT;
-        // the next element's load is in flight while this one is inserted; every lane runs the
-        // same rounds, so that the warp can vote on its 32 elements
+        // the next element's load is in flight while this one is inserted
         unsigned long long next = t0 + threadIdx.x < end ? view_elem<ES>(it, vc, in.ptr, t0 + threadIdx.x) : 0ull;
-        for (uint64_t r0 = t0; r0 < end; r0 += kBThreads) {
-            const uint64_t i = r0 + threadIdx.x;
-            const bool valid = i < end;
+        for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
             const unsigned long long key = next;
             if (i + kBThreads < end) next = view_elem<ES>(it, vc, in.ptr, i + kBThreads);
-            // a warp whose 32 elements are one value (a constant or long-run column) counts them with
-            // one atomic instead of 32 on the same shared counter
-            const uint32_t k0 = __shfl_sync(0xffffffffu, (uint32_t)key, 0);
-            if (__all_sync(0xffffffffu, valid && (uint32_t)key == k0) && !is_nan_bits(k0, o)) {
-                if ((threadIdx.x & 31) == 0) {
-                    if (k0 == 0xffffffffu) {
-                        atomicAdd(&s_ones, 32u);
-                    } else {
-                        uint32_t h = (uint32_t)bhash(k0) & (kBHistPacked - 1);
-                        bool done = false;
-                        for (int p = 0; p < 8; p++) {
-                            uint32_t cur = ((volatile uint32_t *)k32)[h];
-                            if (cur == 0xffffffffu) cur = atomicCAS(&k32[h], 0xffffffffu, k0);
-                            if (cur == 0xffffffffu || cur == k0) {
-                                atomicAdd(&c32[h], 32u);
-                                done = true;
-                                break;
-                            }
-                            h = (h + 1) & (kBHistPacked - 1);
-                        }
-                        if (!done) g_insert(t, (unsigned long long)k0, 32u, status);
-                    }
-                }
-                continue;
-            }
-            if (!valid) continue;
             if (is_nan_bits(key, o)) {
                 unsigned long long k = order_key(key, ES, o);
 #pragma unroll

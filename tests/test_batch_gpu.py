@@ -275,6 +275,11 @@ def tuning_columns(G, rng):
              [OR.CONST, OR.AFL, OR.NONE], [OR.DELTA, OR.DICT, OR.NONE, OR.NONE]]
     for dt in [OR.CHAR, OR.SHORT, OR.INT, OR.TIME]:
         for path in paths:
+            if dt == OR.TIME and path[0] == OR.DICT:
+                # the dictionary's code stream is re-read as 8-byte values by its first child and is
+                # not always a whole number of them: the reference drops its last 4 bytes there
+                # (CastSharedCudaPtr), so that tree cannot round-trip; the rest goes to AFL instead
+                path = [OR.DICT, OR.NONE, OR.AFL, OR.NONE]
             for n in [1, 300, 5000, 70001]:
                 for kind in ["int", "b"]:
                     cols.append(gen(rng, kind, dt, n))
