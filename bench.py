@@ -166,6 +166,26 @@ def cpu_roundtrip(cols, trees, threads):
     return dt, sum(c.nbytes for c in cols), sum(b for b, _, _ in res)
 
 
+DRAM_PROFILE = os.path.join(ROOT, "profiles", "batch_step_mixed512_dram.json")
+
+
+def dram_traffic(prof, phase, index):
+    """DRAM bytes (read + written) of launch `index` of a step phase, from the committed ncu
+    capture of this workload's step (profiles/batch_step_mixed512_dram.json: per phase, the pass of
+    every launch and its dram__bytes_read.sum + dram__bytes_write.sum).  Used only when the capture's
+    launch sequence is the one this run profiled; otherwise (None, reason)."""
+    try:
+        with open(DRAM_PROFILE) as f:
+            cap = json.load(f)
+    except (OSError, ValueError):
+        return None, "no ncu capture of this step"
+    seq = [x[0] for x in prof[phase]]
+    got = cap.get(phase, [])
+    if [g[0] for g in got] != seq:
+        return None, "the ncu capture's launch sequence differs from this build's"
+    return int(got[index][1]), f"ncu dram__bytes_read.sum + dram__bytes_write.sum, {phase} launch {index} ({DRAM_PROFILE[len(ROOT) + 1:]})"
+
+
 def oracle_check(cols, trees, blobs, threads=None):
     """Parity at full size: every batched blob byte-compared with the oracle's
     CompressionTree::Compress of the same column (largest columns first, all host threads).
@@ -585,6 +605,8 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = peak_hbm()
     allp = [(phase, *x) for phase, lst in prof.items() for x in lst]
     top = max(allp, key=lambda r: r[2])
+    top_index = prof[top[0]].index(top[1:])
+    traffic, traffic_src = dram_traffic(prof, top[0], top_index)
     t_prof = {k: sum(x[1] for x in v) for k, v in prof.items()}
     top_ach = top[3] / (top[2] / 1e3) / 1e9 if top[2] > 0 else 0.0
     alg_step = 2 * (in_bytes + blob_bytes + 8 + 8 * len(cols))
@@ -633,7 +655,8 @@ def run_ours(args, world, rank, local):
                    "autotune": tune,
                    "trees": dict(sorted(tree_names.items(), key=lambda kv: -kv[1]))},
         "roofline": {"bound": "hbm", "kernel": f"{top[0]}:{top[1]}", "achieved": round(top_ach, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(top_ach / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "unit": "GB/s", "frac": round(top_ach / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
+                     "traffic_source": traffic_src,
                      "algorithmic_bytes_per_launch": top[3], "launch_ms": round(top[2], 4), "blocks": top[4],
                      "share_of_step": round(top[2] / (t_prof["compress"] + t_prof["decompress"]), 4),
                      "timing": "CUDA events around each launch of one step replayed launch by launch"},

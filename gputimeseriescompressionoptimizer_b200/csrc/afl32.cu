@@ -151,10 +151,55 @@ __global__ void __launch_bounds__(256) k_afl_values(const uint8_t *__restrict__ 
     st_elem<ES>(out, t, v);
 }
 
+// Every element of an aligned (omega 32) stream, 16 bytes of output a thread: its 16 / ES elements
+// are consecutive lanes of one row of one block, so their words are consecutive too -- one 16-byte
+// load of the row's words (and one of the next row's when the values cross into it), shifts, one
+// 16-byte store.  Rows whose words reach past the stream, and a ragged end, take the element path.
+template <int ES>
+__global__ void __launch_bounds__(256) k_afl32_values_all(const uint8_t *__restrict__ comp, uint64_t words, int b,
+                                                          uint64_t n, uint8_t *__restrict__ out)
+{
+    using T = typename WordOf<ES>::T;
+    constexpr int W = 8 * ES, V = 16 / ES;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t e0 = t * V;
+    if (e0 >= n) return;
+    const uint64_t per = 32ull * W;
+    const uint64_t blk = e0 / per, in_blk = e0 % per;
+    const uint32_t lane0 = (uint32_t)(in_blk % 32), row = (uint32_t)(in_blk / 32);
+    const uint32_t rb = row * (uint32_t)b;
+    const uint64_t word = blk * 32ull * b + lane0 + (uint64_t)(rb / W) * 32;
+    const int bit = (int)(rb % W);
+    const bool cross = bit > W - b;
+    if (e0 + V > n || word + V + (cross ? 32 : 0) > words) {
+        for (int j = 0; j < V && e0 + j < n; j++)
+            st_elem<ES>(out, e0 + j, afl_value<ES, 32, uint64_t>(comp, words, b, e0 + j));
+        return;
+    }
+    const uint4 lo = ld_chunk(comp + word * ES);
+    uint4 hi = make_uint4(0, 0, 0, 0);
+    if (cross) hi = ld_chunk(comp + (word + 32) * ES);
+    const T mask = low_mask<T>(b);
+    uint64_t v[V];
+#pragma unroll
+    for (int j = 0; j < V; j++) {
+        const T a = (T)chunk_elem<ES>(lo, j);
+        T x = a >> bit;
+        if (cross) x |= (T)chunk_elem<ES>(hi, j) << (W - bit);
+        v[j] = x & mask;
+    }
+    reinterpret_cast<uint4 *>(out + e0 * ES)[0] = make_chunk<ES>(v);
+}
+
 template <int ES>
 void values_es(const uint8_t *comp, uint64_t words, int b, int omega, const uint64_t *idx, uint64_t n, uint8_t *out,
                cudaStream_t s)
 {
+    if (omega == 32 && !idx && ((uintptr_t)comp & 15) == 0 && ((uintptr_t)out & 15) == 0) {
+        const uint64_t threads = (n + 16 / ES - 1) / (16 / ES);
+        k_afl32_values_all<ES><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(comp, words, b, n, out);
+        return;
+    }
     const unsigned g = (unsigned)((n + 255) / 256);
     if (omega == 32) k_afl_values<ES, 32><<<g, 256, 0, s>>>(comp, words, b, idx, n, out);
     else k_afl_values<ES, 1><<<g, 256, 0, s>>>(comp, words, b, idx, n, out);

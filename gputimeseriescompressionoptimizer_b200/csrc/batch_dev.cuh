@@ -502,13 +502,14 @@ __device__ inline void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S,
 // ------------------------------------------------------------------------------- persistent step
 // Helpers of the persistent kernels (batch.hpp, PLaunch); all of them run on thread 0 of a block.
 
-// the launch holding queue entry e: the last launch whose first entry is <= e
-__device__ __forceinline__ int persist_launch_of(const PersistArgs &a, uint32_t e)
+// the launch holding queue unit u: the last launch whose first unit is <= u (qs: the launches'
+// first units, in shared memory when they fit, else the launch table itself)
+__device__ __forceinline__ int persist_launch_of(const PersistArgs &a, const uint32_t *qs, uint32_t u)
 {
     int lo = 0, hi = a.n_launches - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (a.launches[mid].qstart <= e) lo = mid;
+        if ((qs ? qs[mid] : a.launches[mid].qstart) <= u) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -542,42 +543,54 @@ __device__ __forceinline__ void persist_flush(const PersistArgs &a, int item, ui
 
 // The persistent loop shared by the compress and the decode kernel.  A block claims one queue unit
 // at a time: one tile of a look-back pass (its successors wait on it, so it is never held behind
-// other work of the same block), kPersistChunk tiles of any other pass.  Thread 0 walks the unit's
-// tiles; tiles past their item's real extent are counted without involving the block.
-// EXTENT(op, item, S) gives an item's tiles that do work (the level schedule's streaming passes skip
-// the others), RUN(op, item, tile) runs one tile with the whole block.
+// other work of the same block), kPersistChunk tiles of any other pass.  Tiles are taken item by
+// item (a look-back pass's tiles of one item in order, so every predecessor was claimed first).
+// Thread 0 does the bookkeeping: it claims the next unit before the block runs the current tile
+// (the claim's latency hides behind the tile), finds the launch in a shared copy of the launches'
+// first units, keeps the current item's descriptor fields in registers, and walks past tiles
+// beyond an item's real extent without involving the block.  EXTENT(op, item, S) gives an item's
+// tiles that do work (the level schedule's streaming passes skip the others), RUN(op, item, tile)
+// runs one tile with the whole block.
+constexpr int kPersistShared = 256;  // launches whose first units fit in shared memory
 template <class Extent, class Run>
 __device__ __forceinline__ void persist_loop(const PersistArgs &a, Extent extent, Run run)
 {
-    __shared__ uint32_t s_u, s_tile;
+    __shared__ uint32_t s_qs[kPersistShared];
+    __shared__ uint32_t s_tile;
     __shared__ int s_item, s_op, s_new, s_run;
+    const uint32_t *qs = a.n_launches <= kPersistShared ? s_qs : nullptr;
+    if (qs)
+        for (int i = threadIdx.x; i < a.n_launches; i += blockDim.x) s_qs[i] = a.launches[i].qstart;
     int cur = -1;       // thread 0: the item whose tiles it is counting
     int loaded = -1;    // thread 0: the item in the block's shared descriptor
     uint32_t pend = 0;  // thread 0: finished tiles of cur not counted yet
-    uint32_t cur_ext = 0;
+    uint32_t cur_ext = 0, cur_base = 0, cur_tiles = 0;
+    uint32_t next = threadIdx.x == 0 ? atomicAdd(a.qcounter, 1u) : 0u;  // thread 0: the claimed unit
+    __syncthreads();
     for (;;) {
-        if (threadIdx.x == 0) s_u = atomicAdd(a.qcounter, 1u);
-        __syncthreads();
-        const uint32_t u = s_u;
-        if (u >= a.total) break;
+        // thread 0: take the claimed unit (all threads learn through s_run whether there was one)
         const PLaunch *pl = nullptr;
         uint32_t t = 0, t1 = 0;
-        if (threadIdx.x == 0) {
-            pl = &a.launches[persist_launch_of(a, u)];
-            t = (u - pl->qstart) * pl->per;
+        bool have = false;
+        if (threadIdx.x == 0 && next < a.total) {
+            pl = &a.launches[persist_launch_of(a, qs, next)];
+            t = (next - pl->qstart) * pl->per;
             t1 = t + pl->per < pl->tiles ? t + pl->per : pl->tiles;
+            have = true;
+            next = atomicAdd(a.qcounter, 1u);  // the following unit, claimed ahead
         }
         for (;;) {
             if (threadIdx.x == 0) {
-                s_run = 0;
-                while (t < t1) {
-                    const uint32_t tt = pl->dyn ? a.item_of[pl->map_off + pl->tiles + t] : t;
-                    const int gi = pl->first + (int)a.item_of[pl->map_off + tt];
-                    const BItem &gitem = a.items[gi];
+                s_run = have ? 0 : -1;
+                while (have && t < t1) {
+                    const int gi = pl->first + (int)a.item_of[pl->map_off + t];
                     if (gi != cur) {
                         persist_flush(a, cur, pend);
                         persist_wait(a, a.pitems[gi]);
                         cur = gi;
+                        const BItem &gitem = a.items[gi];
+                        cur_base = (uint32_t)gitem.tile_base;
+                        cur_tiles = gitem.tiles;
                         // the extent is cached per item (a stale read only recomputes the same value)
                         uint32_t x = a.ext[gi];
                         if (x == 0) {
@@ -586,9 +599,9 @@ __device__ __forceinline__ void persist_loop(const PersistArgs &a, Extent extent
                         }
                         cur_ext = x - 1;
                     }
-                    const uint32_t tile = tt - (uint32_t)gitem.tile_base;
+                    const uint32_t tile = t - cur_base;
                     ++t;
-                    if (tile < cur_ext && tile < gitem.tiles) {
+                    if (tile < cur_ext && tile < cur_tiles) {
                         s_run = 1;
                         s_item = gi;
                         s_op = pl->op;
@@ -601,12 +614,14 @@ __device__ __forceinline__ void persist_loop(const PersistArgs &a, Extent extent
                 }
             }
             __syncthreads();
-            if (!s_run) break;
+            if (s_run <= 0) break;
             if (s_new) shared_item(a.items, (uint32_t)s_item);
             run(s_op, shared_item_ref(), s_tile);
             __syncthreads();  // the next tile reuses the shared memory and the descriptor
             if (threadIdx.x == 0) ++pend;
         }
+        if (s_run < 0) break;  // the queue is exhausted
+        __syncthreads();       // every thread has read s_run before thread 0 writes it again
     }
     if (threadIdx.x == 0) persist_flush(a, cur, pend);
 }

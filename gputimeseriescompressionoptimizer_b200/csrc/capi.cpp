@@ -680,7 +680,9 @@ gtsc_status gtsc_afl32_compress_gpu(int32_t dtype, uint32_t bit_length, const vo
         if (((uintptr_t)d_data | (uintptr_t)d_out) % es) fail(GTSC_ERR_ARG, "afl32: pointers must be element aligned");
         const uint64_t words = afl32_words(n, (int)bit_length, es);
         if (out_bytes < words * es) fail(GTSC_ERR_CAPACITY, "afl32: output smaller than gtsc_afl32_bytes");
-        GTSC_CUDA(cudaMemsetAsync(d_out, 0, words * es, S(stream)));  // the layout has holes in a last block
+        // the layout has holes only in a last, partial block of 32 x W elements: clear just that block
+        const uint64_t full = n / (32ull * 8 * es) * 32ull * bit_length;
+        if (words > full) GTSC_CUDA(cudaMemsetAsync((uint8_t *)d_out + full * es, 0, (words - full) * es, S(stream)));
         launch_afl32_pack((const uint8_t *)d_data, n, es, (int)bit_length, (uint8_t *)d_out, words, S(stream));
     });
 }
