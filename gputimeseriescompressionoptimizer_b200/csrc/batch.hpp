@@ -198,7 +198,7 @@ const void *pipeline_column_output(Pipeline *p, int c);
 //
 // The queue is the level schedule laid end to end, in units: unit u belongs to launch L when
 // qstart[L] <= u < qstart[L] + ceil(tiles[L] / per[L]), and names per[L] consecutive tiles of that
-// launch, item after item (each item's tiles in order).  A block claims one unit at a time and
+// launch (for look-back passes, in the stage launch's claim order).  A block claims one unit at a time and
 // runs its tiles in order; a look-back pass has one tile per unit, so no tile waits behind other
 // work of the block that holds its predecessor.  An item
 // waits, before its first tile, until its column has finished every tile of the earlier levels
@@ -215,7 +215,7 @@ struct PLaunch {
     uint32_t map_off;   // its tile -> item table in item_of; look-back passes: claim order after it
     uint32_t qstart;    // its first queue unit
     uint32_t per;       // tiles per unit: 1 for a look-back pass, kPersistChunk for the others
-    int32_t dyn;        // a look-back pass
+    int32_t dyn;        // a look-back pass (tiles in claim order)
     int32_t pad;
 };
 struct PItem {

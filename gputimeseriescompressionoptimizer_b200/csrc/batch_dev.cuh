@@ -542,13 +542,13 @@ __device__ __forceinline__ void persist_flush(const PersistArgs &a, int item, ui
 }
 
 // The persistent loop shared by the compress and the decode kernel.  A block claims one queue unit
-// at a time: one tile of a look-back pass (its successors wait on it, so it is never held behind
-// other work of the same block), kPersistChunk tiles of any other pass.  Tiles are taken item by
-// item (a look-back pass's tiles of one item in order, so every predecessor was claimed first).
-// Thread 0 does the bookkeeping: it claims the next unit before the block runs the current tile
-// (the claim's latency hides behind the tile), finds the launch in a shared copy of the launches'
-// first units, keeps the current item's descriptor fields in registers, and walks past tiles
-// beyond an item's real extent without involving the block.  EXTENT(op, item, S) gives an item's
+// at a time, when it needs one: one tile of a look-back pass (its successors wait on it, so it is
+// never held behind other work of the same block -- claiming the next unit ahead measured 3x
+// slower for that reason), kPersistChunk tiles of any other pass.  A look-back pass's tiles are
+// taken in the stage launch's claim order (tile j of every item before tile j + 1 of any, each
+// item's tiles in order).  Thread 0 does the bookkeeping: it finds the launch in a shared copy of
+// the launches' first units, keeps the current item's descriptor fields in registers, and walks
+// past tiles beyond an item's real extent without involving the block.  EXTENT(op, item, S) gives an item's
 // tiles that do work (the level schedule's streaming passes skip the others), RUN(op, item, tile)
 // runs one tile with the whole block.
 constexpr int kPersistShared = 256;  // launches whose first units fit in shared memory
@@ -565,25 +565,27 @@ __device__ __forceinline__ void persist_loop(const PersistArgs &a, Extent extent
     int loaded = -1;    // thread 0: the item in the block's shared descriptor
     uint32_t pend = 0;  // thread 0: finished tiles of cur not counted yet
     uint32_t cur_ext = 0, cur_base = 0, cur_tiles = 0;
-    uint32_t next = threadIdx.x == 0 ? atomicAdd(a.qcounter, 1u) : 0u;  // thread 0: the claimed unit
     __syncthreads();
     for (;;) {
-        // thread 0: take the claimed unit (all threads learn through s_run whether there was one)
+        // thread 0: claim a unit (all threads learn through s_run whether there was one)
         const PLaunch *pl = nullptr;
         uint32_t t = 0, t1 = 0;
         bool have = false;
-        if (threadIdx.x == 0 && next < a.total) {
-            pl = &a.launches[persist_launch_of(a, qs, next)];
-            t = (next - pl->qstart) * pl->per;
-            t1 = t + pl->per < pl->tiles ? t + pl->per : pl->tiles;
-            have = true;
-            next = atomicAdd(a.qcounter, 1u);  // the following unit, claimed ahead
+        if (threadIdx.x == 0) {
+            const uint32_t u = atomicAdd(a.qcounter, 1u);
+            if (u < a.total) {
+                pl = &a.launches[persist_launch_of(a, qs, u)];
+                t = (u - pl->qstart) * pl->per;
+                t1 = t + pl->per < pl->tiles ? t + pl->per : pl->tiles;
+                have = true;
+            }
         }
         for (;;) {
             if (threadIdx.x == 0) {
                 s_run = have ? 0 : -1;
                 while (have && t < t1) {
-                    const int gi = pl->first + (int)a.item_of[pl->map_off + t];
+                    const uint32_t tt = pl->dyn ? a.item_of[pl->map_off + pl->tiles + t] : t;
+                    const int gi = pl->first + (int)a.item_of[pl->map_off + tt];
                     if (gi != cur) {
                         persist_flush(a, cur, pend);
                         persist_wait(a, a.pitems[gi]);
@@ -599,7 +601,7 @@ __device__ __forceinline__ void persist_loop(const PersistArgs &a, Extent extent
                         }
                         cur_ext = x - 1;
                     }
-                    const uint32_t tile = t - cur_base;
+                    const uint32_t tile = tt - cur_base;
                     ++t;
                     if (tile < cur_ext && tile < cur_tiles) {
                         s_run = 1;
