@@ -502,6 +502,10 @@ std::vector<uint8_t> validity(const std::vector<std::vector<int16_t>> &classes)
                 Tree t = tree_from_path(classes[c].data(), (int)classes[c].size(), dt);
                 bool ok = t.size() == (int)classes[c].size();
                 for (int k = 0; k < t.size(); k++) ok = ok && node_supported(t.enc[k], t.dt[k]);
+                // a dictionary's code stream, re-read as 8-byte values by its first child, is not
+                // always a whole number of them: only none may sit there (as the planners offer)
+                for (int k = 0; k + 1 < t.size(); k++)
+                    if (t.enc[k] == GTSC_DICT && dtype_size(t.dt[k]) == 8 && t.enc[k + 1] != GTSC_NONE) ok = false;
                 v[c * 6 + dt] = ok;
             } catch (const Error &) {
                 v[c * 6 + dt] = 0;

@@ -17,13 +17,17 @@ namespace {
 
 constexpr int MAX_LEVEL = 3;  // optimizer/path_generator.cpp:15
 
-// PathGenerator::GetContinuations (optimizer/path_generator.cpp:93-146)
-std::vector<int> continuations(int et, int dt, const Stats &st, int level)
+// PathGenerator::GetContinuations (optimizer/path_generator.cpp:93-146).  `whole` = the input is a
+// whole number of elements of its type; when it is not (a dictionary's code stream re-read as
+// 8-byte values), every encoding but none would drop its last bytes (the reference's
+// CastSharedCudaPtr), so only none is offered: a deliberate departure that keeps every planned
+// tree lossless (the oracle does the same).
+std::vector<int> continuations(int et, int dt, const Stats &st, int level, bool whole)
 {
     std::vector<int> r;
     if (level != 0 && (et == GTSC_NONE || st.size == 0)) return r;
     r.push_back(GTSC_NONE);
-    if (et == GTSC_AFL || et == GTSC_GFC) return r;
+    if (et == GTSC_AFL || et == GTSC_GFC || !whole) return r;
     if (level < MAX_LEVEL) {
         if (et != GTSC_DELTA) r.push_back(GTSC_DELTA);
         if (et != GTSC_SCALE && st.min != 0) r.push_back(GTSC_SCALE);
@@ -56,7 +60,7 @@ bool fsu(View data, int et, int dt, int level, Cand &best, PlanCounters &ctr, cu
 {
     const Stats st = column_stats(dt, data, s);
     ctr.stats_calls++;
-    const std::vector<int> cont = continuations(et, dt, st, level);
+    const std::vector<int> cont = continuations(et, dt, st, level, data.bytes % dtype_size(dt) == 0);
     if (cont.empty()) return false;
     best.size = UINT64_MAX;
     for (int c : cont) {
@@ -92,7 +96,7 @@ bool fsu(View data, int et, int dt, int level, Cand &best, PlanCounters &ctr, cu
 void fsu_all(View data, int et, int dt, int level, std::vector<Candidate> &out, cudaStream_t s)
 {
     const Stats st = column_stats(dt, data, s);
-    for (int c : continuations(et, dt, st, level)) {
+    for (int c : continuations(et, dt, st, level, data.bytes % dtype_size(dt) == 0)) {
         Parts p = encode(c, dt, data, s);
         uint64_t psize = 8;
         for (auto &b : p) psize += b.bytes;

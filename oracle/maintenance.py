@@ -11,6 +11,7 @@ Restates:
   CompressionOptimizer::FullStatisticsUpdate / CrossTrees  optimizer/compression_optimizer.cpp:38-140
   CompressionOptimizer::CompressData                       optimizer/compression_optimizer.cpp:142-193
   PathGenerator::GetContinuations                          optimizer/path_generator.cpp:93-146
+    (an input that is not a whole number of elements is offered only none)
 
 Fixed choices where the reference is unordered or undefined (the same ones the library makes):
 statistics entries are scanned in (parent, child) order; a node regrown below the last edge number
@@ -199,12 +200,14 @@ class OptimalTree:
         return False
 
 
-def continuations(et, dt, st, level, max_level=3):
+def continuations(et, dt, st, level, max_level=3, whole=True):
+    """`whole`: the input is a whole number of elements of its type; when it is not (a dictionary's
+    code stream re-read as 8-byte values) only none is offered, as the library's planner does."""
     r = []
     if level != 0 and (et == OR.NONE or st.size == 0):
         return r
     r.append(OR.NONE)
-    if et in (OR.AFL, OR.GFC):
+    if et in (OR.AFL, OR.GFC) or not whole:
         return r
     if level < max_level:
         if et != OR.DELTA:
@@ -231,7 +234,7 @@ def candidates(data, dt, et=OR.NONE, level=0):
     data = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
     st = OR.stats(dt, data)
     out = []
-    for c in continuations(et, dt, st, level):
+    for c in continuations(et, dt, st, level, whole=data.size % OR.NP_TYPES[dt]().itemsize == 0):
         parts = OR.encode(c, dt, data)
         psize = 8 + sum(p.size for p in parts)
         r = N_RESULTS[c]

@@ -282,13 +282,16 @@ int or_tree_predict_size(const int16_t *nodes, int n_nodes, const uint8_t *in, u
 
 #define MAX_LEVEL 3   /* optimizer/path_generator.cpp:15 */
 
-/* PathGenerator::GetContinuations (optimizer/path_generator.cpp:93-146) */
-static int continuations(int et, int dt, const or_stats_t *s, int level, int *out)
+/* PathGenerator::GetContinuations (optimizer/path_generator.cpp:93-146).  `whole` = the input is a
+ * whole number of elements of its type; when it is not (a dictionary's code stream re-read as 8-byte
+ * values), every encoding but none would drop its last bytes (CastSharedCudaPtr), so only none is
+ * offered: a deliberate departure that keeps every planned tree lossless. */
+static int continuations(int et, int dt, const or_stats_t *s, int level, int whole, int *out)
 {
     int k = 0;
     if (level != 0 && (et == OR_NONE || s->size == 0)) return 0;
     out[k++] = OR_NONE;
-    if (et == OR_AFL || et == OR_GFC) return k;
+    if (et == OR_AFL || et == OR_GFC || !whole) return k;
     if (level < MAX_LEVEL) {
         if (et != OR_DELTA) out[k++] = OR_DELTA;
         if (et != OR_SCALE && s->min != 0) out[k++] = OR_SCALE;
@@ -334,7 +337,7 @@ static int fsu(const uint8_t *data, uint64_t bytes, int et, int dt, int level, c
     or_stats_t st;
     or_stats(dt, data, bytes, &st);
     int cont[16];
-    int nc = continuations(et, dt, &st, level, cont);
+    int nc = continuations(et, dt, &st, level, bytes % es_of(dt) == 0, cont);
     if (nc == 0) return 0;
     best->size = UINT64_MAX;
     uint64_t ec = enc_cap(bytes);
