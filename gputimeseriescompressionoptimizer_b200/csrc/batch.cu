@@ -124,11 +124,11 @@ public:
     std::vector<BItem> items_c, items_d, items_copy;
     std::vector<int> item_col_c, item_col_d;  // each item's column
     std::vector<Launch> launch_c, launch_d;
-    // the persistent schedule (batch.hpp, PLaunch) of each phase
-    std::vector<PLaunch> plaunch_c, plaunch_d;
+    // the persistent schedule (batch.hpp, PUnit) of each phase
+    std::vector<PUnit> punit_c, punit_d;
     std::vector<PItem> pitem_c, pitem_d;
     uint32_t q_total_c = 0, q_total_d = 0;
-    PLaunch *d_plaunch_c = nullptr, *d_plaunch_d = nullptr;
+    PUnit *d_punit_c = nullptr, *d_punit_d = nullptr;
     PItem *d_pitem_c = nullptr, *d_pitem_d = nullptr;
     uint32_t *d_done_c = nullptr, *d_done_d = nullptr, *d_ext_c = nullptr, *d_ext_d = nullptr;
     uint32_t *d_queue = nullptr;  // [0] compress claim counter, [1] decode claim counter
@@ -172,7 +172,7 @@ public:
     void record_compress(cudaStream_t s, const std::function<void(int)> &mark, bool pers);
     void record_decompress(cudaStream_t s, const std::function<void(int)> &mark, bool pers);
     void plan_persistent(const std::vector<Launch> &launches, const std::vector<BItem> &items,
-                         const std::vector<int> &item_col, std::vector<PLaunch> &pl, std::vector<PItem> &pi,
+                         const std::vector<int> &item_col, std::vector<PUnit> &units, std::vector<PItem> &pi,
                          uint32_t &total);
     PersistArgs persist_args(bool compress) const;
 };
@@ -721,8 +721,8 @@ void BatchEngine::layout(cudaStream_t s)
     };
     build(pass_c, items_c, launch_c, item_col_c);
     build(pass_d, items_d, launch_d, item_col_d);
-    plan_persistent(launch_c, items_c, item_col_c, plaunch_c, pitem_c, q_total_c);
-    plan_persistent(launch_d, items_d, item_col_d, plaunch_d, pitem_d, q_total_d);
+    plan_persistent(launch_c, items_c, item_col_c, punit_c, pitem_c, q_total_c);
+    plan_persistent(launch_d, items_d, item_col_d, punit_d, pitem_d, q_total_d);
 
     // zero ranges per step
     auto zr = [](std::vector<unsigned long long> &z, uint8_t *p, uint64_t bytes) {
@@ -811,8 +811,8 @@ void BatchEngine::layout(cudaStream_t s)
     const uint64_t o_counters = t_off; t_off += sz(n_counters, 4);
     const uint64_t o_item_of = t_off; t_off += sz(item_of.size(), 4);
     const uint64_t ncol = col_root.size();
-    const uint64_t o_plc = t_off; t_off += sz(plaunch_c.size(), sizeof(PLaunch));
-    const uint64_t o_pld = t_off; t_off += sz(plaunch_d.size(), sizeof(PLaunch));
+    const uint64_t o_plc = t_off; t_off += sz(punit_c.size(), sizeof(PUnit));
+    const uint64_t o_pld = t_off; t_off += sz(punit_d.size(), sizeof(PUnit));
     const uint64_t o_pic = t_off; t_off += sz(pitem_c.size(), sizeof(PItem));
     const uint64_t o_pid = t_off; t_off += sz(pitem_d.size(), sizeof(PItem));
     const uint64_t o_done_c = t_off; t_off += sz(ncol, 4);
@@ -842,8 +842,8 @@ void BatchEngine::layout(cudaStream_t s)
     d_status = (uint32_t *)(T + o_status);
     d_counters = (uint32_t *)(T + o_counters);
     d_item_of = (uint32_t *)(T + o_item_of);
-    d_plaunch_c = (PLaunch *)(T + o_plc);
-    d_plaunch_d = (PLaunch *)(T + o_pld);
+    d_punit_c = (PUnit *)(T + o_plc);
+    d_punit_d = (PUnit *)(T + o_pld);
     d_pitem_c = (PItem *)(T + o_pic);
     d_pitem_d = (PItem *)(T + o_pid);
     d_done_c = (uint32_t *)(T + o_done_c);
@@ -876,60 +876,60 @@ void BatchEngine::layout(cudaStream_t s)
     h2d(d_zero_c, zero_c.data(), zero_c.size() * 8);
     h2d(d_zero_d, zero_d.data(), zero_d.size() * 8);
     h2d(d_item_of, item_of.data(), item_of.size() * 4);
-    h2d(d_plaunch_c, plaunch_c.data(), plaunch_c.size() * sizeof(PLaunch));
-    h2d(d_plaunch_d, plaunch_d.data(), plaunch_d.size() * sizeof(PLaunch));
+    h2d(d_punit_c, punit_c.data(), punit_c.size() * sizeof(PUnit));
+    h2d(d_punit_d, punit_d.data(), punit_d.size() * sizeof(PUnit));
     h2d(d_pitem_c, pitem_c.data(), pitem_c.size() * sizeof(PItem));
     h2d(d_pitem_d, pitem_d.data(), pitem_d.size() * sizeof(PItem));
     GTSC_CUDA(cudaStreamSynchronize(s));
 }
 
-// The persistent schedule of one phase (batch.hpp, PLaunch): the level launches end to end as one
-// queue, and per item its column and the number of that column's entries in earlier levels.
+// The persistent schedule of one phase (batch.hpp, PUnit): the level launches end to end as one
+// queue of units, and per item its column and the number of that column's tiles in earlier levels.
 void BatchEngine::plan_persistent(const std::vector<Launch> &launches, const std::vector<BItem> &items,
-                                  const std::vector<int> &item_col, std::vector<PLaunch> &pl,
+                                  const std::vector<int> &item_col, std::vector<PUnit> &units,
                                   std::vector<PItem> &pi, uint32_t &total)
 {
+    static_assert(kPersistChunk <= 15, "a unit's tile count has four bits");
     const size_t nc = col_root.size();
-    std::vector<uint64_t> tot(nc, 0), before(nc, 0);  // entries so far / in the earlier levels
+    std::vector<uint64_t> tot(nc, 0), before(nc, 0);  // tiles so far / in the earlier levels
     pi.assign(items.size(), PItem{0, 0});
-    uint64_t q = 0;
+    units.clear();
     int level = INT32_MIN;
     for (const Launch &L : launches) {
         if (L.level != level) {  // launches are sorted by level
             before = tot;
             level = L.level;
         }
-        PLaunch p;
-        p.op = L.op;
-        p.first = L.first;
-        p.tiles = (uint32_t)L.tiles;
-        p.map_off = (uint32_t)L.map_off;
-        p.qstart = (uint32_t)q;
-        p.dyn = dyn_pass(L.op) ? 1 : 0;
-        p.per = p.dyn ? 1u : kPersistChunk;
-        p.pad = 0;
-        pl.push_back(p);
-        q += (L.tiles + p.per - 1) / p.per;
         for (int k = L.first; k < L.first + L.count; k++) {
             const int c = item_col[k];
             if (before[c] > 0xffffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles for the persistent schedule");
             pi[k] = PItem{(uint32_t)c, (uint32_t)before[c]};
             tot[c] += items[k].tiles;
         }
+        const bool dyn = dyn_pass(L.op);
+        const uint32_t per = dyn ? 1u : kPersistChunk;
+        for (uint64_t t = 0; t < L.tiles; t += per) {
+            // the unit's first tile: look-back passes in the launch's claim order (item_of after its
+            // tile table), the others in tile order
+            const uint64_t tt = dyn ? item_of[L.map_off + L.tiles + t] : t;
+            const int gi = L.first + (int)item_of[L.map_off + tt];
+            const uint64_t tile = tt - items[gi].tile_base;
+            const uint32_t cnt = (uint32_t)std::min<uint64_t>(per, L.tiles - t);
+            if (tile >= (1u << 28)) fail(GTSC_ERR_CAPACITY, "batch: an item has too many tiles for the persistent schedule");
+            units.push_back(PUnit{(uint32_t)gi, (uint32_t)tile | (cnt << 28)});
+        }
     }
-    if (q >= 0xffffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles for the persistent schedule");
-    total = (uint32_t)q;
+    if (units.size() >= 0xffffffffull) fail(GTSC_ERR_CAPACITY, "batch: too many tiles for the persistent schedule");
+    total = (uint32_t)units.size();
 }
 
 PersistArgs BatchEngine::persist_args(bool compress) const
 {
     PersistArgs a;
-    a.launches = compress ? d_plaunch_c : d_plaunch_d;
-    a.n_launches = (int)(compress ? plaunch_c.size() : plaunch_d.size());
+    a.units = compress ? d_punit_c : d_punit_d;
     a.total = compress ? q_total_c : q_total_d;
     a.items = compress ? d_items_c : d_items_d;
     a.pitems = compress ? d_pitem_c : d_pitem_d;
-    a.item_of = d_item_of;
     a.done = compress ? d_done_c : d_done_d;
     a.ext = compress ? d_ext_c : d_ext_d;
     a.qcounter = d_queue + (compress ? 0 : 1);

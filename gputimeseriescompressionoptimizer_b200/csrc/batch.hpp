@@ -196,46 +196,39 @@ const void *pipeline_column_output(Pipeline *p, int c);
 
 // ---- the persistent schedule: one launch per step whose blocks pull work from a device queue
 //
-// The queue is the level schedule laid end to end, in units: unit u belongs to launch L when
-// qstart[L] <= u < qstart[L] + ceil(tiles[L] / per[L]), and names per[L] consecutive tiles of that
-// launch (for look-back passes, in the stage launch's claim order).  A block claims one unit at a time and
-// runs its tiles in order; a look-back pass has one tile per unit, so no tile waits behind other
-// work of the block that holds its predecessor.  An item
-// waits, before its first tile, until its column has finished every tile of the earlier levels
-// (done[col] >= wait): passes of
-// different columns never depend on one another, and a level only follows levels of its own
-// column, so small columns run ahead instead of waiting at every level for the largest ones.
-// Every tile depends only on tiles of lower units (look-back predecessors come earlier in claim
-// order, earlier levels earlier in the queue), so the lowest unfinished unit can always run and the
-// resident blocks always make progress; each wait is still bounded (GTSC_ERR_TIMEOUT).
-struct PLaunch {
-    int32_t op;
-    int32_t first;      // first item of the launch in the phase's item table
-    uint32_t tiles;     // the launch's tiles
-    uint32_t map_off;   // its tile -> item table in item_of; look-back passes: claim order after it
-    uint32_t qstart;    // its first queue unit
-    uint32_t per;       // tiles per unit: 1 for a look-back pass, kPersistChunk for the others
-    int32_t dyn;        // a look-back pass (tiles in claim order)
-    int32_t pad;
+// The queue is the level schedule laid end to end, in units: the launches in order, each cut into
+// units of one tile (look-back passes, taken in the stage launch's claim order: tile j of every
+// item before tile j + 1 of any) or of up to kPersistChunk consecutive tiles (the other passes).  A
+// unit names its first tile (item, tile) and its tile count; a block claims one unit at a time and
+// runs its tiles in order (a chunk walks on into the next item of the same launch), so a look-back
+// tile never waits behind other work of the block that holds its predecessor.  An item waits,
+// before its first tile, until its column has finished every tile of the earlier levels
+// (done[col] >= wait): passes of different columns never depend on one another, and a level only
+// follows levels of its own column, so small columns run ahead instead of waiting at every level
+// for the largest ones.  Every tile depends only on tiles of lower units (look-back predecessors
+// come earlier in claim order, earlier levels earlier in the queue), so the lowest unfinished unit
+// can always run and the resident blocks always make progress; each wait is still bounded
+// (GTSC_ERR_TIMEOUT).
+struct PUnit {
+    uint32_t item;        // the item of the unit's first tile (phase item table)
+    uint32_t tile_count;  // that tile (low 28 bits) and the unit's tiles (high 4 bits)
 };
 struct PItem {
     uint32_t col;       // the item's column
     uint32_t wait;      // tiles of that column in earlier levels
 };
 struct PersistArgs {
-    const PLaunch *launches;
-    int n_launches;
+    const PUnit *units;
     uint32_t total;     // queue units
     const BItem *items;
     const PItem *pitems;
-    const uint32_t *item_of;
     uint32_t *done;     // per column: tiles finished (zeroed each step)
     uint32_t *ext;      // per item: 1 + its extent in tiles once a block computed it (zeroed)
     uint32_t *qcounter; // the claim counter (zeroed)
     StreamDesc *S;
     uint32_t *status;
 };
-constexpr uint32_t kPersistChunk = 8;  // tiles per queue unit of a pass without look-back
+constexpr uint32_t kPersistChunk = 8;  // tiles per queue unit of a pass without look-back (<= 15)
 // one persistent launch of a whole compress (batch_kernels.cu) or decode (batch_decode.cu) step
 void launch_batch_persistent_c(const PersistArgs &a, cudaStream_t s);
 void launch_batch_persistent_d(const PersistArgs &a, cudaStream_t s);

@@ -953,7 +953,7 @@ __device__ __forceinline__ uint32_t persist_extent_d(int op, const BItem &it, co
     }
 }
 
-// The whole decode step in one launch (batch.hpp, PLaunch); the merges' counting pass is the
+// The whole decode step in one launch (batch.hpp, PUnit); the merges' counting pass is the
 // queue's first launch.
 __global__ void __launch_bounds__(kBThreads, 4) k_bpersist_d(PersistArgs a)
 {

@@ -500,20 +500,7 @@ __device__ inline void p_gfc_scan(const BItem &it, uint32_t tile, StreamDesc *S,
 }
 
 // ------------------------------------------------------------------------------- persistent step
-// Helpers of the persistent kernels (batch.hpp, PLaunch); all of them run on thread 0 of a block.
-
-// the launch holding queue unit u: the last launch whose first unit is <= u (qs: the launches'
-// first units, in shared memory when they fit, else the launch table itself)
-__device__ __forceinline__ int persist_launch_of(const PersistArgs &a, const uint32_t *qs, uint32_t u)
-{
-    int lo = 0, hi = a.n_launches - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if ((qs ? qs[mid] : a.launches[mid].qstart) <= u) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
+// Helpers of the persistent kernels (batch.hpp, PUnit); all of them run on thread 0 of a block.
 
 // waits until the item's column has finished the entries of its earlier levels; bounded: gives up
 // with GTSC_ERR_TIMEOUT after kSpinLimit polls, or at once when another block recorded an error
@@ -544,70 +531,69 @@ __device__ __forceinline__ void persist_flush(const PersistArgs &a, int item, ui
 // The persistent loop shared by the compress and the decode kernel.  A block claims one queue unit
 // at a time, when it needs one: one tile of a look-back pass (its successors wait on it, so it is
 // never held behind other work of the same block -- claiming the next unit ahead measured 3x
-// slower for that reason), kPersistChunk tiles of any other pass.  A look-back pass's tiles are
-// taken in the stage launch's claim order (tile j of every item before tile j + 1 of any, each
-// item's tiles in order).  Thread 0 does the bookkeeping: it finds the launch in a shared copy of
-// the launches' first units, keeps the current item's descriptor fields in registers, and walks
-// past tiles beyond an item's real extent without involving the block.  EXTENT(op, item, S) gives an item's
-// tiles that do work (the level schedule's streaming passes skip the others), RUN(op, item, tile)
-// runs one tile with the whole block.
-constexpr int kPersistShared = 256;  // launches whose first units fit in shared memory
+// slower for that reason), up to kPersistChunk consecutive tiles of any other pass.  The unit table
+// gives the unit's first (item, tile) and its tile count, so a claim costs one 8-byte load; the
+// look-back passes' units are already in the stage launch's claim order (tile j of every item
+// before tile j + 1 of any, each item's tiles in order).  Thread 0 does the bookkeeping: it keeps
+// the current item's fields in registers and walks past tiles beyond an item's real extent without
+// involving the block.  EXTENT(op, item, S) gives an item's tiles that do work (the level
+// schedule's streaming passes skip the others), RUN(op, item, tile) runs one tile with the whole
+// block.
 template <class Extent, class Run>
 __device__ __forceinline__ void persist_loop(const PersistArgs &a, Extent extent, Run run)
 {
-    __shared__ uint32_t s_qs[kPersistShared];
     __shared__ uint32_t s_tile;
     __shared__ int s_item, s_op, s_new, s_run;
-    const uint32_t *qs = a.n_launches <= kPersistShared ? s_qs : nullptr;
-    if (qs)
-        for (int i = threadIdx.x; i < a.n_launches; i += blockDim.x) s_qs[i] = a.launches[i].qstart;
     int cur = -1;       // thread 0: the item whose tiles it is counting
     int loaded = -1;    // thread 0: the item in the block's shared descriptor
     uint32_t pend = 0;  // thread 0: finished tiles of cur not counted yet
-    uint32_t cur_ext = 0, cur_base = 0, cur_tiles = 0;
-    __syncthreads();
+    uint32_t cur_ext = 0, cur_tiles = 0;
+    int cur_op = 0;
     for (;;) {
         // thread 0: claim a unit (all threads learn through s_run whether there was one)
-        const PLaunch *pl = nullptr;
-        uint32_t t = 0, t1 = 0;
-        bool have = false;
+        int gi = 0;
+        uint32_t tile = 0, cnt = 0;
         if (threadIdx.x == 0) {
             const uint32_t u = atomicAdd(a.qcounter, 1u);
             if (u < a.total) {
-                pl = &a.launches[persist_launch_of(a, qs, u)];
-                t = (u - pl->qstart) * pl->per;
-                t1 = t + pl->per < pl->tiles ? t + pl->per : pl->tiles;
-                have = true;
+                const PUnit pu = a.units[u];
+                gi = (int)pu.item;
+                tile = pu.tile_count & 0x0fffffffu;
+                cnt = pu.tile_count >> 28;
             }
         }
+        const bool have = cnt > 0;
         for (;;) {
             if (threadIdx.x == 0) {
                 s_run = have ? 0 : -1;
-                while (have && t < t1) {
-                    const uint32_t tt = pl->dyn ? a.item_of[pl->map_off + pl->tiles + t] : t;
-                    const int gi = pl->first + (int)a.item_of[pl->map_off + tt];
+                while (cnt > 0) {
                     if (gi != cur) {
                         persist_flush(a, cur, pend);
                         persist_wait(a, a.pitems[gi]);
                         cur = gi;
                         const BItem &gitem = a.items[gi];
-                        cur_base = (uint32_t)gitem.tile_base;
                         cur_tiles = gitem.tiles;
+                        cur_op = gitem.op;
                         // the extent is cached per item (a stale read only recomputes the same value)
                         uint32_t x = a.ext[gi];
                         if (x == 0) {
-                            x = 1 + extent(pl->op, gitem, a.S);
+                            x = 1 + extent(cur_op, gitem, a.S);
                             a.ext[gi] = x;
                         }
                         cur_ext = x - 1;
                     }
-                    const uint32_t tile = tt - cur_base;
-                    ++t;
-                    if (tile < cur_ext && tile < cur_tiles) {
+                    if (tile >= cur_tiles) {  // the unit goes on with the launch's next item
+                        ++gi;
+                        tile = 0;
+                        continue;
+                    }
+                    const uint32_t my = tile++;
+                    --cnt;
+                    if (my < cur_ext) {
                         s_run = 1;
                         s_item = gi;
-                        s_op = pl->op;
-                        s_tile = tile;
+                        s_op = cur_op;
+                        s_tile = my;
                         s_new = gi != loaded;
                         loaded = gi;
                         break;

@@ -1430,7 +1430,7 @@ __device__ __forceinline__ uint32_t persist_extent_c(int op, const BItem &it, co
 }
 
 // The whole compress step in one launch: every pass kind behind one switch, tiles pulled from the
-// queue of batch.hpp (PLaunch).
+// queue of batch.hpp (PUnit).
 __global__ void __launch_bounds__(kBThreads, 4) k_bpersist_c(PersistArgs a)
 {
     __shared__ __align__(16) unsigned char smem[persist_smem_c()];

@@ -1,4 +1,4 @@
-// batch_persist_c.cu -- the persistent compress kernel (batch.hpp, PLaunch): the compress passes of
+// batch_persist_c.cu -- the persistent compress kernel (batch.hpp, PUnit): the compress passes of
 // batch_kernels.cu compiled a second time with coherent loads.  In one persistent launch a pass
 // reads what earlier passes of the same launch wrote, which the read-only (non-coherent) path the
 // stage kernels use does not allow.
