@@ -54,6 +54,18 @@ def build_ref():
     return True
 
 
+# the reference's own encoders and compression tree, built from its sources (oracle/Makefile,
+# target refenc; oracle/ref_enc_shim.cu); they run on the GPU
+REF_ENC_PATH = os.path.join(HERE, "_ref", "libref_enc.so")
+
+
+def build_ref_enc():
+    """Compile the reference encoders; returns whether the library exists afterwards."""
+    if os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "refenc", f"REF={REF_SRC}"], check=True)
+    return os.path.exists(REF_ENC_PATH)
+
+
 _lib = None
 _ref = None
 
@@ -121,6 +133,92 @@ def ref():
     if _ref is None and os.path.exists(REF_PATH):
         _ref = ctypes.CDLL(REF_PATH)
     return _ref
+
+
+_ref_enc = None
+
+
+def ref_enc():
+    """The reference's encoders and tree (a CUDA library), or None when it was not built."""
+    global _ref_enc
+    if _ref_enc is None and os.path.exists(REF_ENC_PATH):
+        L = ctypes.CDLL(REF_ENC_PATH)
+        vp, u64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)
+        L.ref_enc_error.restype = ctypes.c_char_p
+        L.ref_enc_free.argtypes = [vp]
+        L.ref_enc_encode.argtypes = [ctypes.c_int, ctypes.c_int, vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(vp), u64p]
+        L.ref_enc_decode.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), u64p,
+                                     ctypes.POINTER(vp), u64p]
+        L.ref_tree_compress.argtypes = [vp, ctypes.c_int, vp, ctypes.c_uint64, ctypes.POINTER(vp), u64p]
+        L.ref_tree_decompress.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(vp), u64p]
+        _ref_enc = L
+    return _ref_enc
+
+
+def _ref_take(L, p, n):
+    """Copy a host buffer the reference shim allocated into numpy and free it."""
+    out = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_uint8)), (max(n, 1),))[:n].copy() \
+        if n else np.zeros(0, np.uint8)
+    L.ref_enc_free(p)
+    return out
+
+
+def _ref_check(L, rc, what):
+    if rc != 0:
+        raise OracleError(f"reference {what}: {L.ref_enc_error().decode()}")
+
+
+def ref_encode(enc, dtype, data):
+    """The reference's Encoding::Encode (through its factory's Get(data)) -> [metadata, out1, ...]."""
+    L = ref_enc()
+    src = as_bytes(data)
+    nres = ctypes.c_int(0)
+    outs = (ctypes.c_void_p * 4)()
+    sizes = (ctypes.c_uint64 * 4)()
+    rc = L.ref_enc_encode(enc, dtype, _ptr(src), src.size, ctypes.byref(nres), outs, sizes)
+    res = [_ref_take(L, outs[i], sizes[i]) for i in range(nres.value)]
+    _ref_check(L, rc, f"encode {ENC_NAMES[enc]}")
+    return res
+
+
+def ref_decode(enc, dtype, parts):
+    """The reference's Encoding::Decode (through its factory's Get()) -> byte array."""
+    L = ref_enc()
+    parts = [as_bytes(p) for p in parts]
+    ptrs = (ctypes.c_void_p * len(parts))(*[_ptr(p) for p in parts])
+    sizes = (ctypes.c_uint64 * len(parts))(*[p.size for p in parts])
+    out = ctypes.c_void_p()
+    ob = ctypes.c_uint64(0)
+    rc = L.ref_enc_decode(enc, dtype, len(parts), ptrs, sizes, ctypes.byref(out), ctypes.byref(ob))
+    res = _ref_take(L, out, ob.value) if out.value else np.zeros(0, np.uint8)
+    _ref_check(L, rc, f"decode {ENC_NAMES[enc]}")
+    return res
+
+
+def ref_tree_compress(nodes, data):
+    """The reference's CompressionTree::Compress of a pre-order (encoding, type) node list."""
+    L = ref_enc()
+    nodes = np.asarray(nodes, np.int16)
+    src = as_bytes(data)
+    out = ctypes.c_void_p()
+    ob = ctypes.c_uint64(0)
+    rc = L.ref_tree_compress(_ptr(nodes), nodes.size // 2, _ptr(src), src.size, ctypes.byref(out), ctypes.byref(ob))
+    res = _ref_take(L, out, ob.value) if out.value else np.zeros(0, np.uint8)
+    _ref_check(L, rc, "tree compress")
+    return res
+
+
+def ref_tree_decompress(blob):
+    """The reference's CompressionTree::Decompress."""
+    L = ref_enc()
+    blob = as_bytes(blob)
+    out = ctypes.c_void_p()
+    ob = ctypes.c_uint64(0)
+    rc = L.ref_tree_decompress(_ptr(blob), blob.size, ctypes.byref(out), ctypes.byref(ob))
+    res = _ref_take(L, out, ob.value) if out.value else np.zeros(0, np.uint8)
+    _ref_check(L, rc, "tree decompress")
+    return res
 
 
 def _ptr(a):
