@@ -421,7 +421,7 @@ class Tuning(ctypes.Structure):
         return d
 
 
-def tuning(minmax_tile=8192, minmax_values_per_thread=16, hist_tile=16384, persistent_compress=False,
+def tuning(minmax_tile=8192, minmax_values_per_thread=16, hist_tile=32768, persistent_compress=False,
            persistent_decompress=False):
     t = Tuning()
     t.minmax_tile, t.minmax_values_per_thread, t.hist_tile = minmax_tile, minmax_values_per_thread, hist_tile

@@ -1352,7 +1352,7 @@ BatchEngine *batch_autotune(BatchEngine *e, cudaStream_t s, TuneReport *report)
         e->tune.persistent_c = false;
         float best_h = time_passes(e, {B_HIST, B_TOPK}, s, 3);
         e->tune.persistent_c = keep_c;
-        for (uint32_t tile : {4096u, 8192u, 16384u}) {
+        for (uint32_t tile : {8192u, 16384u, 32768u, 65536u}) {
             if (tile == best.hist_tile) continue;
             BatchTuning cand = best;
             cand.hist_tile = tile;

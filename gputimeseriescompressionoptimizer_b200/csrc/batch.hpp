@@ -126,7 +126,7 @@ class BatchEngine;
 struct BatchTuning {
     uint32_t minmax_tile = 8192;   // min/max pass: a multiple of 256 x minmax_vpt, 1K .. 16K
     uint32_t minmax_vpt = 16;      // min/max pass: consecutive values a thread loads per round (1 .. 16)
-    uint32_t hist_tile = 16384;    // histogram pass (dict / const), 1K .. 16K
+    uint32_t hist_tile = 32768;    // histogram pass (dict / const), 8K .. 64K
     bool persistent_c = false;     // compress step: one persistent launch instead of the levels
     bool persistent_d = false;     // decompress step: the same
 };

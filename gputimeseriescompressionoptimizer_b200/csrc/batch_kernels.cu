@@ -427,7 +427,9 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
     if (ES <= 4 && t0 < n) {
         // values of up to 4 bytes: 32-bit keys and counts (twice the slots of the layout below); a
         // value already in the table costs a plain key read and one 32-bit atomicAdd.  0xffffffff
-        // marks an empty slot, so that value itself is counted apart.
+        // marks an empty slot, so that value itself is counted apart.  Each thread reads 16
+        // consecutive bytes a round (one vector load), two rounds in flight before either is
+        // inserted; slots are chosen by a 32-bit multiplicative hash.
         uint32_t *k32 = (uint32_t *)smem;
         uint32_t *c32 = k32 + kBHistPacked;
         __shared__ uint32_t s_ones;
@@ -438,72 +440,136 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         if (threadIdx.x == 0) s_ones = 0;
         __syncthreads();
         const uint64_t end = n < t0 + HT ? n : t0 + HT;
-        // the next element's load is in flight while this one is inserted
-        unsigned long long next = t0 + threadIdx.x < end ? view_elem<ES>(it, vc, in.ptr, t0 + threadIdx.x) : 0ull;
-        for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
-            const unsigned long long key = next;
-            if (i + kBThreads < end) next = view_elem<ES>(it, vc, in.ptr, i + kBThreads);
-            if (is_nan_bits(key, o)) {
-                unsigned long long k = order_key(key, ES, o);
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                    if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
-                continue;
-            }
-            const uint32_t kk = (uint32_t)key;
-            if (kk == 0xffffffffu) {
-                atomicAdd(&s_ones, 1u);
-                continue;
-            }
-            uint32_t h = (uint32_t)bhash(key) & (kBHistPacked - 1);
-            bool done = false;
+        constexpr int VPT = 16 / ES;
+        constexpr uint64_t R = (uint64_t)kBThreads * VPT;  // values of one round of the block
+        constexpr uint32_t HSH = 32 - 12;                   // log2(kBHistPacked) = 12
+        static_assert(kBHistPacked == 4096, "the slot hash takes the top 12 bits");
+        // a thread counts a run of equal values in registers and inserts the run once when the
+        // value changes (a constant or run-heavy column then costs a compare per value)
+        uint32_t run_key = 0, run_cnt = 0;
+        auto add = [&](uint32_t kk, uint32_t c) {
+            uint32_t h = (kk * 0x9E3779B1u) >> HSH;
             for (int p = 0; p < 8; p++) {
                 uint32_t cur = ((volatile uint32_t *)k32)[h];
                 if (cur == 0xffffffffu) cur = atomicCAS(&k32[h], 0xffffffffu, kk);
                 if (cur == 0xffffffffu || cur == kk) {
-                    atomicAdd(&c32[h], 1u);
-                    done = true;
-                    break;
+                    atomicAdd(&c32[h], c);
+                    return;
                 }
                 h = (h + 1) & (kBHistPacked - 1);
             }
-            if (!done) g_insert(t, key, 1u, status);
+            g_insert(t, (unsigned long long)kk, c, status);
+        };
+        auto insert = [&](uint32_t kk, bool valid) {
+            if (!valid) return;
+            if (run_cnt && kk == run_key) {  // run_key is never a NaN or 0xffffffff
+                ++run_cnt;
+                return;
+            }
+            if (ES == 4 && is_nan_bits(kk, o)) {
+                unsigned long long k = order_key(kk, ES, o);
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
+                return;
+            }
+            if (kk == 0xffffffffu) {
+                atomicAdd(&s_ones, 1u);
+                return;
+            }
+            if (run_cnt) add(run_key, run_cnt);
+            run_key = kk;
+            run_cnt = 1;
+        };
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint64_t wfirst = t0 + (uint64_t)(threadIdx.x - lane) * VPT;
+        for (uint64_t w0 = wfirst; w0 < end; w0 += 2 * R) {
+            const uint64_t b0 = w0 + (uint64_t)lane * VPT, b1 = b0 + R;
+            uint32_t u[2][VPT];
+            {
+                uint64_t v[VPT];
+                if (b0 < end) load_view_any<ES, VPT>(it, vc, in.ptr, b0, v);
+#pragma unroll
+                for (int j = 0; j < VPT; j++) u[0][j] = (uint32_t)v[j];
+                if (b1 < end) load_view_any<ES, VPT>(it, vc, in.ptr, b1, v);
+#pragma unroll
+                for (int j = 0; j < VPT; j++) u[1][j] = (uint32_t)v[j];
+            }
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const uint64_t base = r ? b1 : b0;
+                const uint32_t cnt = base >= end ? 0u : end - base < (uint64_t)VPT ? (uint32_t)(end - base) : VPT;
+#pragma unroll
+                for (int j = 0; j < VPT; j++) insert(u[r][j], (uint32_t)j < cnt);
+            }
         }
+        if (run_cnt) add(run_key, run_cnt);
         __syncthreads();
         for (int i = threadIdx.x; i < (int)kBHistPacked; i += kBThreads)
             if (k32[i] != 0xffffffffu) g_insert(t, (unsigned long long)k32[i], c32[i], status);
         if (threadIdx.x == 0 && s_ones) g_insert(t, 0xffffffffull, s_ones, status);
     } else if (t0 < n) {
+        // 8-byte values: 64-bit keys, two values a round (one 16-byte load), two rounds in flight
         for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads) {
             skeys[i] = EMPTY;
             scounts[i] = 0;
         }
         __syncthreads();
         const uint64_t end = n < t0 + HT ? n : t0 + HT;
-        for (uint64_t i = t0 + threadIdx.x; i < end; i += kBThreads) {
-            const unsigned long long key = view_elem<ES>(it, vc, in.ptr, i);
+        constexpr int VPT = 2;
+        constexpr uint64_t R = (uint64_t)kBThreads * VPT;
+        constexpr uint32_t HSH = 32 - 11;  // log2(kBHistSmem) = 11
+        static_assert(kBHistSmem == 2048, "the slot hash takes the top 11 bits");
+        const uint32_t lane = threadIdx.x & 31u;
+        unsigned long long run_key = 0;
+        uint32_t run_cnt = 0;
+        auto add = [&](unsigned long long key, uint32_t c) {
+            if (key != EMPTY) {
+                uint32_t h = ((uint32_t)(key ^ (key >> 32)) * 0x9E3779B1u) >> HSH;
+                for (int p = 0; p < 8; p++) {
+                    unsigned long long cur = ((volatile unsigned long long *)skeys)[h];
+                    if (cur == EMPTY) cur = atomicCAS(&skeys[h], EMPTY, key);
+                    if (cur == EMPTY || cur == key) {
+                        atomicAdd(&scounts[h], c);
+                        return;
+                    }
+                    h = (h + 1) & (kBHistSmem - 1);
+                }
+            }
+            g_insert(t, key, c, status);
+        };
+        auto insert = [&](unsigned long long key, bool valid) {
+            if (!valid) return;
+            if (run_cnt && key == run_key) {  // run_key is never a NaN
+                ++run_cnt;
+                return;
+            }
             if (is_nan_bits(key, o)) {
                 unsigned long long k = order_key(key, ES, o);
 #pragma unroll
                 for (int j = 0; j < 4; j++)
                     if (k < nan_min[j]) { const unsigned long long x = nan_min[j]; nan_min[j] = k; k = x; }
-                continue;
+                return;
             }
-            bool done = false;
-            if (key != EMPTY) {
-                uint32_t h = (uint32_t)bhash(key) & (kBHistSmem - 1);
-                for (int p = 0; p < 8; p++) {
-                    const unsigned long long prev = atomicCAS(&skeys[h], EMPTY, key);
-                    if (prev == EMPTY || prev == key) {
-                        atomicAdd(&scounts[h], 1u);
-                        done = true;
-                        break;
-                    }
-                    h = (h + 1) & (kBHistSmem - 1);
-                }
+            if (run_cnt) add(run_key, run_cnt);
+            run_key = key;
+            run_cnt = 1;
+        };
+        const uint64_t wfirst = t0 + (uint64_t)(threadIdx.x - lane) * VPT;
+        for (uint64_t w0 = wfirst; w0 < end; w0 += 2 * R) {
+            const uint64_t b0 = w0 + (uint64_t)lane * VPT, b1 = b0 + R;
+            uint64_t u[2][VPT];
+            if (b0 < end) load_view_any<ES, VPT>(it, vc, in.ptr, b0, u[0]);
+            if (b1 < end) load_view_any<ES, VPT>(it, vc, in.ptr, b1, u[1]);
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const uint64_t base = r ? b1 : b0;
+                const uint32_t cnt = base >= end ? 0u : end - base < (uint64_t)VPT ? (uint32_t)(end - base) : VPT;
+#pragma unroll
+                for (int j = 0; j < VPT; j++) insert(u[r][j], (uint32_t)j < cnt);
             }
-            if (!done) g_insert(t, key, 1u, status);
         }
+        if (run_cnt) add(run_key, run_cnt);
         __syncthreads();
         for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads)
             if (skeys[i] != EMPTY) g_insert(t, skeys[i], scounts[i], status);
