@@ -215,11 +215,37 @@ def cpu_trees(cols, specs):
     return trees
 
 
+def reference_gpu():
+    """The reference's own CompressionTree::Compress (its sources compiled for sm_100a into
+    oracle/_ref/libref_enc.so) over the same workload on this GPU, compress only, the columns whose
+    trees hold no GFC node (its GFC kernels rely on implicit warp synchrony), timed by
+    oracle/time_ref_tree.py in a child process: the reference exits its process on a CUDA error."""
+    import oracle
+    if not os.path.exists(oracle.REF_ENC_PATH):
+        return {"unavailable": "oracle/_ref/libref_enc.so not built (make -C oracle refenc where the reference is)"}
+    script = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "time_ref_tree.py")
+    try:
+        p = subprocess.run([sys.executable, script, "--reference-only"], capture_output=True, text=True,
+                           timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "the reference's tree compress did not finish in 900 s"}
+    lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+    if p.returncode != 0 or not lines:
+        tail = " ".join((p.stderr or "").strip().splitlines()[-2:])[-200:]
+        return {"unavailable": f"the reference's run failed (status {p.returncode}): {tail}"}
+    r = json.loads(lines[-1])
+    r["what"] = ("the reference's own CompressionTree::Compress (compiled from its sources for sm_100a), "
+                 f"compress only, {r['columns']} of {r['of_columns']} columns (those without GFC), the exhaustive "
+                 "planner's trees, column after column, host clock around the synchronous calls")
+    return r
+
+
 def run_reference(args, world, rank):
-    """The reference's CPU implementation of the path on the same workload: no part of the
-    reference's own tree code compiles here (boost, log4cplus, a missing submodule), so this is the
-    oracle restatement built -O3 -march=native on this host, with every host thread, over the full
-    512-column workload per step, with the trees the exhaustive planner picks."""
+    """A CPU implementation of the path on the same workload.  The reference has none (its
+    encoders are CUDA kernels and Thrust calls), so this is the oracle restatement built -O3
+    -march=native on this host, with every host thread, over the full 512-column workload per step,
+    with the trees the exhaustive planner picks.  The reference's own GPU tree compress on the same
+    workload is reported beside it (reference_gpu)."""
     if rank != 0:
         return
     import oracle
@@ -250,6 +276,7 @@ def run_reference(args, world, rank):
         "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample,
                          "cpu_model": model},
         "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu(),
     }
     print(json.dumps(line), flush=True)
 

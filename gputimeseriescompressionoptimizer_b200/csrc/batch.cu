@@ -281,11 +281,11 @@ void BatchEngine::plan_passes()
         uint64_t c = 64;
         switch (nd.enc) {
         case GTSC_PATCH: case GTSC_PATCH_OUTSIDE:
-            nd.split_tiles = std::max<uint64_t>(1, cdiv(n, (uint64_t)kBTile * kBSplitSub));
+            nd.split_tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
             c = 64 + align_up(lookback_bytes(nd.split_tiles), 256);
             break;
         case GTSC_DICT: case GTSC_CONST: {
-            nd.split_tiles = std::max<uint64_t>(1, cdiv(n, (uint64_t)kBTile * kBSplitSub));
+            nd.split_tiles = std::max<uint64_t>(1, cdiv(n, kBTile));
             nd.hist_tiles = std::max<uint64_t>(1, cdiv(n, tune.hist_tile));
             uint64_t cap = 1024;
             while (cap < 2 * n + 64) cap <<= 1;

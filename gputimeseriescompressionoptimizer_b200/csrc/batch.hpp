@@ -242,7 +242,6 @@ void launch_batch_stage(int op, const BItem *d_items, const uint32_t *d_item_of,
 constexpr uint32_t kBVPT = 16;         // values per thread of the element-wise and look-back passes
 constexpr uint32_t kBTile = 256 * kBVPT; // elements per tile of those passes (256 threads per block)
 constexpr uint32_t kBMergeSub = 4;      // kBTile tiles per block of the merge pass
-constexpr uint32_t kBSplitSub = 4;      // kBTile sub-tiles per tile (and look-back) of the split pass
 constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
 constexpr uint32_t kBHistSmem = 2048;    // shared hash slots of a histogram block (8-byte values)
 constexpr uint32_t kBHistPacked = 4096;  // the same for values of up to 4 bytes (packed slots)

@@ -737,87 +737,60 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
             if (mode != SPLIT_NOT_CONST) S[it.out[2]].len = 0;
         }
     }
-    // A tile is `subs` sub-tiles of kBTile values (up to kBSplitSub: as many as the item's tiles
-    // need to cover its values).  Phase 1 classifies them (stencil bytes, the min / max folds, the
-    // tile's match count) and takes the tile's place in the match stream by one look-back; phase 2
-    // reads them again (from L2) and scatters both runs.  One look-back per several sub-tiles
-    // keeps the chain of predecessors short.
-    uint32_t subs = (uint32_t)((((n + it.tiles - 1) / it.tiles) + kBTile - 1) / kBTile);
-    subs = subs < 1 ? 1 : (subs > kBSplitSub ? kBSplitSub : subs);
-    const uint64_t T = (uint64_t)kBTile * subs;
     // a tile past the input has no successor waiting on its look-back descriptor (every later
     // tile is past the input too), so it leaves at once; grids are sized for the worst case
-    if (tile > 0 && (uint64_t)tile * T >= n) return;
-    // classification of the kBVPT values of a thread at `base`: bit j set for a match, and for a
-    // dictionary the 2-bit code of each match
-    auto classify = [&](const uint64_t (&v)[kBVPT], uint32_t &bits, uint32_t &codes) {
-        bits = 0;
-        codes = 0;
-        if (mode == SPLIT_LOWER && outside) {
-            // OutsideOperator (stencil_operators.hpp:14-25): false when x > high or x < low
+    if (tile > 0 && (uint64_t)tile * kBTile >= n) return;
+    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    uint64_t v[kBVPT];
+    load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+    uint32_t bits = 0, codes = 0;
+    if (mode == SPLIT_LOWER && outside) {
+        // OutsideOperator (stencil_operators.hpp:14-25): false when x > high or x < low
 #pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++)
-                bits |= (uint32_t)!(lt_native(thr, v[j], ES, o) || lt_native(v[j], lo, ES, o)) << j;
-        } else if (mode == SPLIT_LOWER) {
+        for (int j = 0; j < (int)kBVPT; j++)
+            bits |= (uint32_t)!(lt_native(thr, v[j], ES, o) || lt_native(v[j], lo, ES, o)) << j;
+    } else if (mode == SPLIT_LOWER) {
 #pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) bits |= (uint32_t)lt_native(v[j], thr, ES, o) << j;
-        } else {
-            // equal bits and not NaN (bsame): NaN-ness once per value, not once per candidate
-            const bool fp = o != ORD_INT;
+        for (int j = 0; j < (int)kBVPT; j++) bits |= (uint32_t)lt_native(v[j], thr, ES, o) << j;
+    } else {
+        // equal bits and not NaN (bsame): NaN-ness once per value, not once per candidate
+        const bool fp = o != ORD_INT;
 #pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) {
-                const bool nan = fp && is_nan_bits(v[j], o);
-                if (mode == SPLIT_NOT_CONST) {
-                    bits |= (uint32_t)(nan || v[j] != top[0]) << j;
-                } else {
-                    const uint32_t e0 = v[j] == top[0], e1 = v[j] == top[1], e2 = v[j] == top[2], e3 = v[j] == top[3];
-                    bits |= (uint32_t)(!nan && (e0 | e1 | e2 | e3)) << j;
-                    codes |= (nan ? 0u : (e1 | (e2 << 1) | (e3 * 3u))) << (2 * j);
-                }
-            }
-        }
-    };
-    auto valid_of = [&](uint64_t base) -> uint32_t {
-        return base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
-    };
-    // ---- phase 1
-    const bool fold_y = it.p[2] != 0, fold_n = it.p[3] != 0, folds = fold_y || fold_n;
-    uint64_t ymin = ~0ull, ymax = 0, nmin = ~0ull, nmax = 0;
-    uint32_t count = 0;
-    for (uint32_t sub = 0; sub < subs; sub++) {
-        const uint64_t sb = (uint64_t)tile * T + (uint64_t)sub * kBTile;
-        if (sb >= n) break;  // the same for every thread of the block
-        const uint64_t base = sb + (uint64_t)threadIdx.x * kBVPT;
-        uint64_t v[kBVPT];
-        load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
-        uint32_t bits, codes;
-        classify(v, bits, codes);
-        if (base < n) {
-            const uint64_t valid = n - base;
-            if (valid < kBVPT) {  // Stencil::pack's index clamp: the last element fills the last byte
-                const uint32_t last = (bits >> (valid - 1)) & 1u;
-                for (int j = (int)valid; j < (int)kBVPT; j++) bits = (bits & ~(1u << j)) | (last << j);
-            }
-#pragma unroll
-            for (int q = 0; q < (int)kBVPT / 8; q++)
-                if (base + 8 * q < n) stencil[base / 8 + q] = (uint8_t)(bits >> (8 * q));
-        }
-        const uint32_t valid_mask = valid_of(base);
-        const uint32_t yes_bits = bits & valid_mask;
-        count += __popc(yes_bits);
-        if (folds) {
-            // min / max of the matches and of the rest, for the AFL children that read them
-            // (integer order, as their own min/max pass would compute it)
-#pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++) {
-                const uint64_t k = order_key(v[j], ES, ORD_INT);
-                const bool in = (valid_mask >> j) & 1u, y = (yes_bits >> j) & 1u;
-                if (fold_y && in && y) { ymin = k < ymin ? k : ymin; ymax = k > ymax ? k : ymax; }
-                if (fold_n && in && !y) { nmin = k < nmin ? k : nmin; nmax = k > nmax ? k : nmax; }
+        for (int j = 0; j < (int)kBVPT; j++) {
+            const bool nan = fp && is_nan_bits(v[j], o);
+            if (mode == SPLIT_NOT_CONST) {
+                bits |= (uint32_t)(nan || v[j] != top[0]) << j;
+            } else {
+                const uint32_t e0 = v[j] == top[0], e1 = v[j] == top[1], e2 = v[j] == top[2], e3 = v[j] == top[3];
+                bits |= (uint32_t)(!nan && (e0 | e1 | e2 | e3)) << j;
+                codes |= (nan ? 0u : (e1 | (e2 << 1) | (e3 * 3u))) << (2 * j);
             }
         }
     }
-    if (folds) {
+    if (base < n) {
+        const uint64_t valid = n - base;
+        if (valid < kBVPT) {  // Stencil::pack's index clamp: the last element fills the last byte
+            const uint32_t last = (bits >> (valid - 1)) & 1u;
+            for (int j = (int)valid; j < (int)kBVPT; j++) bits = (bits & ~(1u << j)) | (last << j);
+        }
+#pragma unroll
+        for (int q = 0; q < (int)kBVPT / 8; q++)
+            if (base + 8 * q < n) stencil[base / 8 + q] = (uint8_t)(bits >> (8 * q));
+    }
+    const uint32_t valid_mask = base >= n ? 0u : (n - base >= kBVPT ? (1u << kBVPT) - 1 : ((1u << (n - base)) - 1));
+    const uint32_t yes_bits = bits & valid_mask;
+    if (it.p[2] | it.p[3]) {
+        // min / max of the matches and of the rest, for the AFL children that read them (integer
+        // order, as their own min/max pass would compute it); only the classes with such a child
+        const bool fold_y = it.p[2] != 0, fold_n = it.p[3] != 0;
+        uint64_t ymin = ~0ull, ymax = 0, nmin = ~0ull, nmax = 0;
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++) {
+            const uint64_t k = order_key(v[j], ES, ORD_INT);
+            const bool in = (valid_mask >> j) & 1u, y = (yes_bits >> j) & 1u;
+            if (fold_y && in && y) { ymin = k < ymin ? k : ymin; ymax = k > ymax ? k : ymax; }
+            if (fold_n && in && !y) { nmin = k < nmin ? k : nmin; nmax = k > nmax ? k : nmax; }
+        }
         block_minmax(ymin, ymax);
         block_minmax(nmin, nmax);
         if (threadIdx.x == 0) {
@@ -828,106 +801,88 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
             if (an && nmax != 0) atomicMax(&an->kmax, (unsigned long long)nmax);
         }
     }
-    {
-        unsigned long long total;
-        block_exclusive_scan<kBThreads>((unsigned long long)count, ws, total);
-        if (threadIdx.x < 32) {
-            const unsigned long long e = lookback_exclusive(lb, tile, total);
-            if (threadIdx.x == 0) s_prefix = e;
-        }
-        __syncthreads();
+    unsigned long long total;
+    const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(yes_bits), ws, total);
+    if (threadIdx.x < 32) {
+        const unsigned long long e = lookback_exclusive(lb, tile, total);
+        if (threadIdx.x == 0) s_prefix = e;
     }
-    // ---- phase 2
-    uint64_t ycur = s_prefix;  // matches before this sub-tile
-    for (uint32_t sub = 0; sub < subs; sub++) {
-        const uint64_t tile_base = (uint64_t)tile * T + (uint64_t)sub * kBTile;
-        if (tile_base >= n) break;  // the same for every thread of the block
-        const uint64_t base = tile_base + (uint64_t)threadIdx.x * kBVPT;
-        uint64_t v[kBVPT];
-        load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
-        uint32_t bits, codes;
-        classify(v, bits, codes);
-        const uint32_t valid_mask = valid_of(base);
-        const uint32_t yes_bits = bits & valid_mask;
-        unsigned long long total;
-        const unsigned long long excl = block_exclusive_scan<kBThreads>((unsigned long long)__popc(yes_bits), ws, total);
-        // the sub-tile's values go to shared memory in output order (matches first, then the
-        // rest), then the block writes both runs with coalesced stores
-        const uint64_t tile_n = n - tile_base < kBTile ? n - tile_base : kBTile;
-        const uint64_t ny = total, nn = tile_n - ny;
-        const uint64_t yes0 = ycur, no0 = tile_base - yes0;
-        // staged at spad(position): one spare slot per 16, so the runs of consecutive threads (16
-        // apart when most values match) fall into different banks.  Only the runs that are written
-        // are staged: a dictionary writes codes for its matches, a const node only its mismatches.
-        uint32_t ly = (uint32_t)excl, ln = threadIdx.x * kBVPT - (uint32_t)excl;
-        const uint32_t ny32 = (uint32_t)ny;
-        const bool stage_y = mode != SPLIT_DICT, stage_n = mode != SPLIT_NOT_CONST;
+    __syncthreads();
+    // the tile's values go to shared memory in output order (matches first, then the rest), then
+    // the block writes both runs with coalesced stores
+    const uint64_t tile_base = (uint64_t)tile * kBTile;
+    const uint64_t tile_n = tile_base < n ? (n - tile_base < kBTile ? n - tile_base : kBTile) : 0;
+    const uint64_t ny = total, nn = tile_n - ny;
+    const uint64_t yes0 = s_prefix, no0 = tile_base - (tile_base < n ? yes0 : 0);
+    // staged at spad(position): one spare slot per 16, so the runs of consecutive threads (16 apart
+    // when most values match) fall into different banks.  Only the runs that are written are
+    // staged: a dictionary writes codes for its matches, a const node only its mismatches.
+    uint32_t ly = (uint32_t)excl, ln = threadIdx.x * kBVPT - (uint32_t)excl;
+    const uint32_t ny32 = (uint32_t)ny;
+    const bool stage_y = mode != SPLIT_DICT, stage_n = mode != SPLIT_NOT_CONST;
 #pragma unroll
-        for (int j = 0; j < (int)kBVPT; j++) {
-            if (!((valid_mask >> j) & 1u)) break;
+    for (int j = 0; j < (int)kBVPT; j++) {
+        if (!((valid_mask >> j) & 1u)) break;
+        if ((yes_bits >> j) & 1u) {
+            if (stage_y) st_elem<ES>(sm, spad(ly), v[j]);
+            ++ly;
+        } else {
+            if (stage_n) st_elem<ES>(sm, spad(ny32 + ln), v[j]);
+            ++ln;
+        }
+    }
+    if (mode == SPLIT_DICT) {
+        // 2-bit codes of this thread's matches: at most two code words; a word wholly inside the
+        // thread's range is stored, a shared one is merged with atomicOr (the words start zeroed)
+        uint32_t *words = (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES);
+        const uint64_t y0 = yes0 + excl, y1 = y0 + __popc(yes_bits);
+        uint32_t acc0 = 0u, acc1 = 0u;  // the first and the second code word of the range
+        uint32_t r = (uint32_t)(y0 & 15);  // position inside the first word (at most 15 + 16 < 32)
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++)
             if ((yes_bits >> j) & 1u) {
-                if (stage_y) st_elem<ES>(sm, spad(ly), v[j]);
-                ++ly;
-            } else {
-                if (stage_n) st_elem<ES>(sm, spad(ny32 + ln), v[j]);
-                ++ln;
+                const uint32_t bits2 = ((codes >> (2 * j)) & 3u) << (2 * (r & 15));
+                if (r < 16) acc0 |= bits2;
+                else acc1 |= bits2;
+                ++r;
+            }
+        if (y1 > y0) {
+            for (uint64_t w = y0 >> 4; w <= (y1 - 1) >> 4; w++) {
+                const uint32_t a = w == (y0 >> 4) ? acc0 : acc1;
+                if (16 * w >= y0 && 16 * w + 16 <= y1) words[w] = a;
+                else if (a) atomicOr(words + w, a);
             }
         }
-        if (mode == SPLIT_DICT) {
-            // 2-bit codes of this thread's matches: at most two code words; a word wholly inside
-            // the thread's range is stored, a shared one is merged with atomicOr (the words start
-            // zeroed)
-            uint32_t *words = (uint32_t *)(S[it.out[1]].ptr + 16 + 4 * ES);
-            const uint64_t y0 = yes0 + excl, y1 = y0 + __popc(yes_bits);
-            uint32_t acc0 = 0u, acc1 = 0u;     // the first and the second code word of the range
-            uint32_t r = (uint32_t)(y0 & 15);  // position inside the first word (at most 15 + 16 < 32)
-#pragma unroll
-            for (int j = 0; j < (int)kBVPT; j++)
-                if ((yes_bits >> j) & 1u) {
-                    const uint32_t bits2 = ((codes >> (2 * j)) & 3u) << (2 * (r & 15));
-                    if (r < 16) acc0 |= bits2;
-                    else acc1 |= bits2;
-                    ++r;
-                }
-            if (y1 > y0) {
-                for (uint64_t w = y0 >> 4; w <= (y1 - 1) >> 4; w++) {
-                    const uint32_t a = w == (y0 >> 4) ? acc0 : acc1;
-                    if (16 * w >= y0 && 16 * w + 16 <= y1) words[w] = a;
-                    else if (a) atomicOr(words + w, a);
-                }
-            }
+    }
+    __syncthreads();
+    if (mode != SPLIT_DICT) {
+        uint8_t *yes = S[it.out[1]].ptr + yes0 * ES;
+        for (uint32_t i = threadIdx.x; i < ny32; i += kBThreads) st_elem<ES>(yes, i, ld_elem_sm<ES>(sm, spad(i)));
+    }
+    if (mode != SPLIT_NOT_CONST) {
+        uint8_t *no = S[it.out[2]].ptr + no0 * ES;
+        const uint32_t nn32 = (uint32_t)nn;
+        for (uint32_t i = threadIdx.x; i < nn32; i += kBThreads)
+            st_elem<ES>(no, i, ld_elem_sm<ES>(sm, spad(ny32 + i)));
+    }
+    const uint64_t yes_pos = yes0 + ny;
+    if (base < n && base + kBVPT >= n) {  // the thread holding the last element: lengths and headers
+        const uint64_t m = yes_pos;  // this is the last tile: its matches end the match stream
+        if (mode == SPLIT_LOWER) {
+            S[it.out[0]].len = 1 + (n + 7) / 8;
+            S[it.out[1]].len = m * ES;
+            S[it.out[2]].len = (n - m) * ES;
+        } else if (mode == SPLIT_NOT_CONST) {
+            S[it.out[0]].len = ES + 1 + (n + 7) / 8;
+            S[it.out[1]].len = m * ES;
+        } else {
+            uint64_t *sz = (uint64_t *)S[it.out[1]].ptr;
+            sz[0] = 4;
+            sz[1] = m;
+            S[it.out[0]].len = 1 + (n + 7) / 8;
+            S[it.out[1]].len = m ? 16 + 4 * ES + 4 * ((m + 15) / 16) : 0;
+            S[it.out[2]].len = (n - m) * ES;
         }
-        __syncthreads();
-        if (mode != SPLIT_DICT) {
-            uint8_t *yes = S[it.out[1]].ptr + yes0 * ES;
-            for (uint32_t i = threadIdx.x; i < ny32; i += kBThreads) st_elem<ES>(yes, i, ld_elem_sm<ES>(sm, spad(i)));
-        }
-        if (mode != SPLIT_NOT_CONST) {
-            uint8_t *no = S[it.out[2]].ptr + no0 * ES;
-            const uint32_t nn32 = (uint32_t)nn;
-            for (uint32_t i = threadIdx.x; i < nn32; i += kBThreads)
-                st_elem<ES>(no, i, ld_elem_sm<ES>(sm, spad(ny32 + i)));
-        }
-        ycur += ny;
-        if (base < n && base + kBVPT >= n) {  // the thread holding the last element: lengths and headers
-            const uint64_t m = ycur;  // this is the last sub-tile: its matches end the match stream
-            if (mode == SPLIT_LOWER) {
-                S[it.out[0]].len = 1 + (n + 7) / 8;
-                S[it.out[1]].len = m * ES;
-                S[it.out[2]].len = (n - m) * ES;
-            } else if (mode == SPLIT_NOT_CONST) {
-                S[it.out[0]].len = ES + 1 + (n + 7) / 8;
-                S[it.out[1]].len = m * ES;
-            } else {
-                uint64_t *sz = (uint64_t *)S[it.out[1]].ptr;
-                sz[0] = 4;
-                sz[1] = m;
-                S[it.out[0]].len = 1 + (n + 7) / 8;
-                S[it.out[1]].len = m ? 16 + 4 * ES + 4 * ((m + 15) / 16) : 0;
-                S[it.out[2]].len = (n - m) * ES;
-            }
-        }
-        __syncthreads();  // the next sub-tile reuses the staging area
     }
     (void)status;
 }

@@ -17,8 +17,12 @@ reference's API is synchronous (it allocates, copies and synchronises inside), s
 timed by the host clock around whole calls, after warm-up, median of the repetitions; GB/s counts
 the uncompressed input bytes.
 
+--reference-only: the mixed workload through the reference alone (no library call), with the trees
+the oracle's exhaustive planner picks -- the extra line of `bench.py --impl reference`; prints one
+JSON line.
+
 TEST INFRASTRUCTURE: a measurement script, not part of the library.  Usage:
-    python oracle/time_ref_tree.py [--out FILE] [--reps 5] [--mixed-reps 1]
+    python oracle/time_ref_tree.py [--out FILE] [--reps 5] [--mixed-reps 1] [--reference-only]
 """
 import argparse
 import ctypes
@@ -79,13 +83,44 @@ def _ref_call(L, h, nodes):
     return ob.value
 
 
+def reference_only(L, reps):
+    """The bench workload's columns through the reference's own tree compress, one after another;
+    trees from the oracle's exhaustive planner; columns whose tree holds GFC left out."""
+    import bench
+    t0 = time.perf_counter()
+    specs = bench.workload_specs()
+    cols = bench.gen_columns(specs)
+    trees = bench.cpu_trees(cols, specs)
+    keep = [i for i, t in enumerate(trees) if OR.GFC not in [int(v) for v in np.asarray(t)[0::2]]]
+    handles = [L.ref_dev_upload(OR._ptr(OR.as_bytes(cols[i])), cols[i].nbytes) for i in keep]
+    if any(h is None for h in handles):
+        raise OR.OracleError(f"reference upload: {L.ref_enc_error().decode()}")
+    nodes = [np.asarray(trees[i], np.int16) for i in keep]
+    in_bytes = sum(cols[i].nbytes for i in keep)
+
+    def all_columns():
+        for h, nd in zip(handles, nodes):
+            _ref_call(L, h, nd)
+
+    t = _median_time(all_columns, reps, warm=1)
+    for h in handles:
+        L.ref_dev_free(h)
+    print(json.dumps({"value": round(in_bytes / 1e9 / t, 4), "unit": "GB/s", "ms": round(t * 1e3, 1),
+                      "columns": len(keep), "of_columns": len(cols), "input_bytes": int(in_bytes),
+                      "seconds": round(time.perf_counter() - t0, 1)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=None)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--mixed-reps", type=int, default=1)
+    ap.add_argument("--reference-only", action="store_true")
     args = ap.parse_args()
     L = _lib()
+    if args.reference_only:
+        reference_only(L, args.mixed_reps)
+        return
     st = G.Stream()
     rows = []
     for k, (name, kind, path) in enumerate(CONFIGS):
