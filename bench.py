@@ -38,7 +38,7 @@ N_COLUMNS = int(os.environ.get("GTSC_BENCH_COLUMNS", "512"))
 MAX_LEN = 1 << int(os.environ.get("GTSC_BENCH_MAX_LOG2", "24"))
 MIN_CONFIDENCE = 0.5         # learned planner: below this softmax probability the exhaustive search decides
 TICK_CHUNKS = 4              # streaming tick table: 40 columns x 2^20 rows per chunk
-E2E_GROUPS = 8               # end to end: column groups pipelined over their own streams
+E2E_GROUPS = 16              # end to end: column groups pipelined over their own streams
 METRIC = "batched mixed-workload compress+decompress throughput (uncompressed GB/s)"
 WORKLOAD = (f"mixed {N_COLUMNS} columns, lengths log-uniform [4096, {MAX_LEN}], int32:float32:float64 = 2:1:1, "
             "generators walk/runs/zipf/const/outliers/price, seed 0xB204")
@@ -598,7 +598,7 @@ def run_ours(args, world, rank, local):
     n_launch = batch.launches(True) + batch.launches(False)
     del batch, outs, ov
 
-    # end to end through the public API: the column-chunk pipeline (8 column groups, each with its
+    # end to end through the public API: the column-chunk pipeline (E2E_GROUPS column groups, each with its
     # batch engine and stream) from pinned host columns to pinned host framed output, each group's
     # device decode right after its read-back; the call is synchronous, timed by CUDA events
     # around it

@@ -403,6 +403,32 @@ __device__ void g_insert(const HTab &t, unsigned long long key, unsigned int c, 
     set_status(status, GTSC_ERR_CAPACITY);
 }
 
+// Adds P (key, count) pairs of a thread to the node's global table (a zero count adds nothing).
+// Each key's first slot is read with a plain load, all P loads in flight together: after a
+// column's first tiles most keys are already there, and their counts are then added with
+// reductions that nothing waits for.  A key not at its first slot takes the full insert.  (Keys
+// never move once set, so a slot read holding the key is the key's slot.)
+template <int P>
+__device__ __forceinline__ void g_insert_many(const HTab &t, const unsigned long long (&key)[P],
+                                              const uint32_t (&cnt)[P], uint32_t *status)
+{
+    constexpr unsigned long long EMPTY = ~0ull;
+    const uint64_t mask = t.cap - 1;
+    uint64_t h[P];
+    unsigned long long cur[P];
+#pragma unroll
+    for (int j = 0; j < P; j++) {
+        h[j] = bhash(key[j]) & mask;
+        cur[j] = cnt[j] && key[j] != EMPTY ? *(volatile const unsigned long long *)(t.keys + h[j]) : EMPTY;
+    }
+#pragma unroll
+    for (int j = 0; j < P; j++) {
+        if (!cnt[j]) continue;
+        if (key[j] != EMPTY && cur[j] == key[j]) atomicAdd(t.counts + h[j], cnt[j]);
+        else g_insert(t, key[j], cnt[j], status);
+    }
+}
+
 template <int ES>
 __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, unsigned char *smem)
 {
@@ -505,8 +531,18 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         }
         if (run_cnt) add(run_key, run_cnt);
         __syncthreads();
-        for (int i = threadIdx.x; i < (int)kBHistPacked; i += kBThreads)
-            if (k32[i] != 0xffffffffu) g_insert(t, (unsigned long long)k32[i], c32[i], status);
+        for (int i0 = threadIdx.x; i0 < (int)kBHistPacked; i0 += 4 * kBThreads) {
+            unsigned long long k[4];
+            uint32_t c[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int i = i0 + j * kBThreads;
+                const uint32_t kk = i < (int)kBHistPacked ? k32[i] : 0xffffffffu;
+                k[j] = kk;
+                c[j] = kk != 0xffffffffu ? c32[i] : 0u;
+            }
+            g_insert_many<4>(t, k, c, status);
+        }
         if (threadIdx.x == 0 && s_ones) g_insert(t, 0xffffffffull, s_ones, status);
     } else if (t0 < n) {
         // 8-byte values: 64-bit keys, two values a round (one 16-byte load), two rounds in flight
@@ -571,8 +607,17 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         }
         if (run_cnt) add(run_key, run_cnt);
         __syncthreads();
-        for (int i = threadIdx.x; i < (int)kBHistSmem; i += kBThreads)
-            if (skeys[i] != EMPTY) g_insert(t, skeys[i], scounts[i], status);
+        for (int i0 = threadIdx.x; i0 < (int)kBHistSmem; i0 += 4 * kBThreads) {
+            unsigned long long k[4];
+            uint32_t c[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int i = i0 + j * kBThreads;
+                k[j] = i < (int)kBHistSmem ? skeys[i] : EMPTY;
+                c[j] = k[j] != EMPTY ? scounts[i] : 0u;
+            }
+            g_insert_many<4>(t, k, c, status);
+        }
     }
     // this tile's 4 smallest NaN sort keys
     for (int off = 16; off > 0; off >>= 1) {

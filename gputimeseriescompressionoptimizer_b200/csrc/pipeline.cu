@@ -5,9 +5,13 @@
 // 39-63: per column chunk a CompressionTask that compresses and writes `size_t len` + blob,
 // optimizer/compression_task.cpp:35-77).  The columns are split into groups of about equal bytes;
 // each group has its own batch engine (its trees captured as CUDA graphs) and stream.  A chunk:
-//   1. every group: host -> device copies of its columns, then its compress graph (all enqueued);
+//   1. the host -> device copies of all groups, group after group, on one upload stream; each
+//      group's compress graph waits only for its own group's copies;
 //   2. every group in turn: wait for its compress, copy its framed output to the host (async),
-// so group g's device -> host copy runs while groups g+1.. still upload and compress.
+// so group 0 compresses while group 1 uploads, and group g's device -> host copy runs while groups
+// g+1.. still upload and compress.  (Copies queued on every group's stream at once share the copy
+// engines: every group's upload then ends near the end of all of them, and the compression and
+// read-back of the early groups no longer hide behind the later uploads.)
 #include "batch.hpp"
 
 #include <algorithm>
@@ -24,6 +28,8 @@ struct Pipeline {
     std::vector<DevBuf> d_in, d_out;            // per column
     std::vector<BatchEngine *> eng;             // per group
     std::vector<cudaStream_t> st;               // per group
+    cudaStream_t up = nullptr;                  // the host -> device copies of every group, in order
+    std::vector<cudaEvent_t> uploaded;          // per group: its copies are done
     std::vector<const uint8_t *> framed;        // per group: last compress output (device)
     std::vector<uint64_t> framed_bytes;
     ~Pipeline()
@@ -34,6 +40,9 @@ struct Pipeline {
         for (auto *e : eng) batch_destroy(e);
         for (auto s : st)
             if (s) cudaStreamDestroy(s);
+        for (auto e : uploaded)
+            if (e) cudaEventDestroy(e);
+        if (up) cudaStreamDestroy(up);
     }
 };
 
@@ -61,6 +70,9 @@ Pipeline *pipeline_create(const std::vector<uint64_t> &bytes, const std::vector<
     for (auto &m : p->members) std::sort(m.begin(), m.end());
     p->st.assign(groups, nullptr);
     for (int g = 0; g < groups; g++) GTSC_CUDA(cudaStreamCreateWithFlags(&p->st[g], cudaStreamNonBlocking));
+    GTSC_CUDA(cudaStreamCreateWithFlags(&p->up, cudaStreamNonBlocking));
+    p->uploaded.assign(groups, nullptr);
+    for (int g = 0; g < groups; g++) GTSC_CUDA(cudaEventCreateWithFlags(&p->uploaded[g], cudaEventDisableTiming));
     p->d_in.resize(n);
     p->d_out.resize(n);
     for (size_t c = 0; c < n; c++) {
@@ -96,11 +108,15 @@ void pipeline_compress_host(Pipeline *p, const void *const *host_cols, uint8_t *
                             uint64_t *sizes, bool decode)
 {
     const int G = p->groups;
+    // (the previous call ended with every group's stream synchronised, so no step still reads the
+    // input buffers that these copies overwrite)
     for (int g = 0; g < G; g++) {
         if (!p->eng[g]) continue;
         for (int c : p->members[g])
             if (p->bytes[c])
-                GTSC_CUDA(cudaMemcpyAsync(p->d_in[c].get(), host_cols[c], p->bytes[c], cudaMemcpyHostToDevice, p->st[g]));
+                GTSC_CUDA(cudaMemcpyAsync(p->d_in[c].get(), host_cols[c], p->bytes[c], cudaMemcpyHostToDevice, p->up));
+        GTSC_CUDA(cudaEventRecord(p->uploaded[g], p->up));
+        GTSC_CUDA(cudaStreamWaitEvent(p->st[g], p->uploaded[g], 0));
         batch_compress(p->eng[g], p->st[g]);
     }
     uint64_t off = 0;
@@ -111,6 +127,7 @@ void pipeline_compress_host(Pipeline *p, const void *const *host_cols, uint8_t *
         if (off + nb > cap) {
             // earlier groups' copies into host_framed (and their decodes) are in flight: let them
             // finish so that nothing writes the caller's buffer after the error returns
+            cudaStreamSynchronize(p->up);
             for (int h = 0; h < G; h++) cudaStreamSynchronize(p->st[h]);
             fail(GTSC_ERR_CAPACITY, "pipeline: host framed buffer too small");
         }
