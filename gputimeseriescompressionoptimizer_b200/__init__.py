@@ -98,6 +98,7 @@ def lib():
         L.gtsc_sample_bytes.argtypes = [i32, u64]
         L.gtsc_sample_bytes.restype = u64
         L.gtsc_delta_decode_noalloc.argtypes = [i32, vp, vp, u64, vp, vp]
+        L.gtsc_selftest_lookback_timeout.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double), vp]
         i16, f64 = ctypes.c_int16, ctypes.c_double
         L.gtsc_optimizer_create.argtypes = [i32, ctypes.POINTER(vp)]
         L.gtsc_optimizer_compress.argtypes = [vp, vp, u64, vp, vp, vp, vp]
@@ -375,6 +376,16 @@ def tree_names(nodes):
 
 
 # ------------------------------------------------------------------------ streams and batches
+def selftest_lookback_timeout(stream=None):
+    """Runs one decoupled look-back whose predecessor never publishes (gtsc_selftest_lookback_timeout):
+    returns (the status the waiting tile recorded, seconds the bounded wait took)."""
+    err = ctypes.c_int32(0)
+    sec = ctypes.c_double(0.0)
+    check(lib().gtsc_selftest_lookback_timeout(ctypes.byref(err), ctypes.byref(sec), stream),
+          "selftest_lookback_timeout")
+    return err.value, sec.value
+
+
 class Stream:
     """A non-blocking CUDA stream owned by the library (batched steps are captured on it)."""
 

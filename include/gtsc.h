@@ -448,6 +448,17 @@ gtsc_status gtsc_optimal_tree_destroy(gtsc_optimal_tree *t);
 gtsc_status gtsc_delta_decode_noalloc(int32_t dtype, const void *d_first, const void *d_deltas,
                                       uint64_t n_deltas, void *d_out, void *stream);
 
+/*
+ * Self-test of the bounded waits (no counterpart in the reference).  Every scan in the library
+ * chains its tiles by a decoupled look-back whose waits are bounded: a tile whose predecessor never
+ * publishes gives up after a fixed number of polls (about a second), records GTSC_ERR_TIMEOUT in
+ * the scan's error word and returns, so a broken predecessor cannot hang the GPU.  This call runs
+ * one look-back whose predecessor is never published and returns, in *error_word, what the waiting
+ * tile recorded (GTSC_ERR_TIMEOUT when the bound works) and, in *seconds, how long the wait took.
+ * The device stays usable afterwards.  Synchronises the stream before returning.
+ */
+gtsc_status gtsc_selftest_lookback_timeout(int32_t *error_word, double *seconds, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
