@@ -110,3 +110,67 @@ def test_batch_matches_reference(G, case):
     blobs = G.split_framed(G.to_host(G.DeviceBuffer(p, nb, owned=False)))
     assert len(blobs) == 1
     assert blobs[0].size == ref.size and np.array_equal(blobs[0], ref)
+
+
+# the planner's fixed paths (a first stage, then a second stage ending in leaves), as
+# optimizer/compression_optimizer.cpp:16-36 enumerates them; floatToInt only on float columns
+FIRST = [[], [OR.FLOAT2INT], [OR.DELTA], [OR.SCALE], [OR.DELTA, OR.FLOAT2INT], [OR.SCALE, OR.FLOAT2INT]]
+SECOND = [[OR.DICT, OR.AFL, OR.NONE, OR.AFL, OR.NONE], [OR.CONST, OR.AFL, OR.NONE],
+          [OR.RLE, OR.AFL, OR.NONE, OR.AFL, OR.NONE], [OR.AFL, OR.NONE],
+          [OR.PATCH, OR.AFL, OR.NONE, OR.AFL, OR.NONE]]
+PATH_TYPES = [OR.SHORT, OR.INT, OR.TIME, OR.FLOAT, OR.DOUBLE]
+
+
+def _path_cases():
+    out = []
+    for dt in PATH_TYPES:
+        for a in FIRST:
+            if OR.FLOAT2INT in a and dt not in (OR.FLOAT, OR.DOUBLE):
+                continue
+            for b in SECOND:
+                out.append((dt, a + b))
+    return out
+
+
+PATH_CASES = _path_cases()
+
+
+@pytest.mark.parametrize("case", range(len(PATH_CASES)),
+                         ids=[f"dt{dt}-" + "-".join(OR.ENC_NAMES[e] for e in p if e != OR.NONE) for dt, p in PATH_CASES])
+def test_planner_path_matches_reference(G, case):
+    """Every fixed planner path on every type: the library's blob equals the reference tree's."""
+    dt, path = PATH_CASES[case]
+    nodes = OR.tree_from_path(path, dt)
+    pairs = [(int(nodes[2 * k]), int(nodes[2 * k + 1])) for k in range(len(nodes) // 2)]
+    if (OR.AFL, OR.DOUBLE) in pairs:
+        # AflEncoding::EncodeDouble returns no streams, and CompressionNode::Compress then reads
+        # past its result vector (tree/compression_node.cpp:114): the reference's process dies
+        pytest.skip("the reference cannot run AFL on a double node")
+    for j, kind in enumerate(RC.kinds_of(dt)[:3]):
+        x = W.column(kind, dt, (1 << 16) + 5, SEED + 3000 + 97 * case + j)
+        try:
+            ref = OR.ref_tree_compress(nodes, x)
+        except OR.OracleError as e:
+            pytest.skip(f"the reference refuses this tree: {e}")
+        blob = G.tree_compress(nodes, G.to_device(x))
+        ours = G.to_host(blob)
+        if ours.size == ref.size and np.array_equal(ours, ref):
+            continue
+        # The documented deviations, all on float columns, where the reference compares or converts
+        # floating-point values (its intermediate streams hold NaN and -0.0 bit patterns too, e.g.
+        # the deltas of a float column):
+        # - its own blob does not decode to the column: -0.0 merged with +0.0 or a NaN lost in a
+        #   dictionary, const, RLE or unique node, or a lossy floatToInt (deviations 1, 2, 8);
+        # - both decode, but its choice of most frequent values or its min / max (a patch node's
+        #   threshold) depends on where its sorts and reductions put a NaN (deviations 4, 5).
+        assert x.dtype.kind == "f", (G.tree_names(nodes), kind, ours.size, ref.size)
+        try:
+            back, _ = OR.tree_decompress(ref, x.nbytes)
+            lossy = back.tobytes() != x.tobytes()
+        except OR.OracleError:
+            lossy = True
+        compares = any(e in path for e in (OR.DICT, OR.CONST, OR.RLE, OR.PATCH, OR.UNIQUE))
+        assert lossy or compares, (G.tree_names(nodes), kind, ours.size, ref.size)
+        out, _ = G.tree_decompress(blob)
+        assert G.to_host(out).tobytes() == x.tobytes(), (G.tree_names(nodes), kind)
+
