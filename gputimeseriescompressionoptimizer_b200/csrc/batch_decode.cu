@@ -576,12 +576,20 @@ __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint
         if (s_end[mid] > b) hi = mid;
         else lo = mid + 1;
     }
+    // a run's value is read (through the values' view, which may unpack it) once per run, not per
+    // element: the thread's 16 elements usually lie in one or two runs
     uint64_t v[kBVPT];
+    uint64_t last_r = ~0ull, last_v = 0;
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++) {
         while (lo < m && s_end[lo] <= b + j) ++lo;
         const uint64_t r = r_lo + lo;
-        v[j] = (base + j < n && lo < m && r < values.n) ? dview_elem<ES>(values, r) : 0;
+        const bool in = base + j < n && lo < m && r < values.n;
+        if (in && r != last_r) {
+            last_v = dview_elem<ES>(values, r);
+            last_r = r;
+        }
+        v[j] = in ? last_v : 0;
     }
     store_run<ES, kBVPT>(out.ptr, base, n, v);
     (void)status;
