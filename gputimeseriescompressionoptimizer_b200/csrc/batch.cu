@@ -1033,7 +1033,7 @@ BatchEngine *batch_create(const std::vector<BatchColumn> &cols, const std::vecto
     if (tuning.minmax_tile < kMinMaxTileMin || tuning.minmax_tile % (256 * tuning.minmax_vpt) ||
         tuning.minmax_tile > (1u << 20))
         fail(GTSC_ERR_ARG, "batch: the min/max tile must be a multiple of 256 x its values per thread, 1K .. 1M");
-    if (tuning.hist_tile < 256 || tuning.hist_tile % 256 || tuning.hist_tile > (1u << 20))
+    if (tuning.hist_tile < 256 || tuning.hist_tile % 256 || tuning.hist_tile > kBHistTileMax)
         fail(GTSC_ERR_ARG, "batch: the histogram tile must be a multiple of 256");
     std::unique_ptr<BatchEngine> e(new BatchEngine());
     e->tune = tuning;
@@ -1352,7 +1352,7 @@ BatchEngine *batch_autotune(BatchEngine *e, cudaStream_t s, TuneReport *report)
         e->tune.persistent_c = false;
         float best_h = time_passes(e, {B_HIST, B_TOPK}, s, 3);
         e->tune.persistent_c = keep_c;
-        for (uint32_t tile : {8192u, 16384u, 32768u, 65536u}) {
+        for (uint32_t tile : {8192u, 16384u, 32768u}) {
             if (tile == best.hist_tile) continue;
             BatchTuning cand = best;
             cand.hist_tile = tile;

@@ -126,7 +126,7 @@ class BatchEngine;
 struct BatchTuning {
     uint32_t minmax_tile = 8192;   // min/max pass: a multiple of 256 x minmax_vpt, 1K .. 16K
     uint32_t minmax_vpt = 16;      // min/max pass: consecutive values a thread loads per round (1 .. 16)
-    uint32_t hist_tile = 32768;    // histogram pass (dict / const), 8K .. 64K
+    uint32_t hist_tile = 32768;    // histogram pass (dict / const), 8K .. 32K
     bool persistent_c = false;     // compress step: one persistent launch instead of the levels
     bool persistent_d = false;     // decompress step: the same
 };
@@ -244,7 +244,9 @@ constexpr uint32_t kBTile = 256 * kBVPT; // elements per tile of those passes (2
 constexpr uint32_t kBMergeSub = 4;      // kBTile tiles per block of the merge pass
 constexpr uint32_t kBGfcChunks = 8;     // GFC chunks (warps) per tile
 constexpr uint32_t kBHistSmem = 2048;    // shared hash slots of a histogram block (8-byte values)
-constexpr uint32_t kBHistPacked = 4096;  // the same for values of up to 4 bytes (packed slots)
+constexpr uint32_t kBHistPacked = 4096;  // 8 x this = the bytes of a histogram block's shared table
+constexpr uint32_t kBHistSlots16 = 5456; // its slots for values of up to 4 bytes (16-bit counts)
+constexpr uint32_t kBHistTileMax = 32768; // largest histogram tile (a 16-bit count holds its values)
 
 // scratch layout of a histogram item
 struct BHistHdr {

@@ -451,38 +451,40 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
     }
     unsigned long long nan_min[4] = {EMPTY, EMPTY, EMPTY, EMPTY};
     if (ES <= 4 && t0 < n) {
-        // values of up to 4 bytes: 32-bit keys and counts (twice the slots of the layout below); a
-        // value already in the table costs a plain key read and one 32-bit atomicAdd.  0xffffffff
-        // marks an empty slot, so that value itself is counted apart.  Each thread reads 16
-        // consecutive bytes a round (one vector load), two rounds in flight before either is
-        // inserted; slots are chosen by a 32-bit multiplicative hash.
+        // values of up to 4 bytes: 32-bit keys and 16-bit counts (a tile holds at most
+        // kBHistTileMax = 32768 values, so a count never wraps), two counts a word, as many slots as
+        // the block's shared buffer holds (5456: a 32K tile of Zipf ids, 3,500-4,000 distinct
+        // values, leaves the table under 3/4 full, so few inserts run out of probes).  A value
+        // already in the table costs a plain key read and one 32-bit atomicAdd.  0xffffffff marks an
+        // empty slot, so that value itself is counted apart.  Each thread reads 16 consecutive bytes
+        // a round (one vector load), two rounds in flight before either is inserted; slots are
+        // chosen by a multiplicative hash scaled to the table.
+        constexpr uint32_t SL = kBHistSlots16;
+        static_assert(6 * SL <= 8 * kBHistPacked, "the table fits the shared buffer");
+        static_assert(kBHistTileMax <= 65535, "a 16-bit count holds a tile's values");
         uint32_t *k32 = (uint32_t *)smem;
-        uint32_t *c32 = k32 + kBHistPacked;
+        uint32_t *c16w = k32 + SL;
         __shared__ uint32_t s_ones;
-        for (int i = threadIdx.x; i < (int)kBHistPacked; i += kBThreads) {
-            k32[i] = 0xffffffffu;
-            c32[i] = 0u;
-        }
+        for (int i = threadIdx.x; i < (int)SL; i += kBThreads) k32[i] = 0xffffffffu;
+        for (int i = threadIdx.x; i < (int)SL / 2; i += kBThreads) c16w[i] = 0u;
         if (threadIdx.x == 0) s_ones = 0;
         __syncthreads();
         const uint64_t end = n < t0 + HT ? n : t0 + HT;
         constexpr int VPT = 16 / ES;
         constexpr uint64_t R = (uint64_t)kBThreads * VPT;  // values of one round of the block
-        constexpr uint32_t HSH = 32 - 12;                   // log2(kBHistPacked) = 12
-        static_assert(kBHistPacked == 4096, "the slot hash takes the top 12 bits");
         // a thread counts a run of equal values in registers and inserts the run once when the
         // value changes (a constant or run-heavy column then costs a compare per value)
         uint32_t run_key = 0, run_cnt = 0;
         auto add = [&](uint32_t kk, uint32_t c) {
-            uint32_t h = (kk * 0x9E3779B1u) >> HSH;
+            uint32_t h = (uint32_t)(((uint64_t)(kk * 0x9E3779B1u) * SL) >> 32);
             for (int p = 0; p < 8; p++) {
                 uint32_t cur = ((volatile uint32_t *)k32)[h];
                 if (cur == 0xffffffffu) cur = atomicCAS(&k32[h], 0xffffffffu, kk);
                 if (cur == 0xffffffffu || cur == kk) {
-                    atomicAdd(&c32[h], c);
+                    atomicAdd(&c16w[h >> 1], c << (16 * (h & 1)));
                     return;
                 }
-                h = (h + 1) & (kBHistPacked - 1);
+                h = h + 1 == SL ? 0 : h + 1;
             }
             g_insert(t, (unsigned long long)kk, c, status);
         };
@@ -531,15 +533,15 @@ __device__ void p_hist(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *
         }
         if (run_cnt) add(run_key, run_cnt);
         __syncthreads();
-        for (int i0 = threadIdx.x; i0 < (int)kBHistPacked; i0 += 4 * kBThreads) {
+        for (int i0 = threadIdx.x; i0 < (int)SL; i0 += 4 * kBThreads) {
             unsigned long long k[4];
             uint32_t c[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int i = i0 + j * kBThreads;
-                const uint32_t kk = i < (int)kBHistPacked ? k32[i] : 0xffffffffu;
+                const uint32_t kk = i < (int)SL ? k32[i] : 0xffffffffu;
                 k[j] = kk;
-                c[j] = kk != 0xffffffffu ? c32[i] : 0u;
+                c[j] = kk != 0xffffffffu ? (c16w[i >> 1] >> (16 * (i & 1))) & 0xffffu : 0u;
             }
             g_insert_many<4>(t, k, c, status);
         }

@@ -213,7 +213,7 @@ int32_t gtsc_batch_schedule(gtsc_batch *b);
 typedef struct {
     uint32_t minmax_tile;               /* 1024 .. 16384, a multiple of 256 x the values per thread */
     uint32_t minmax_values_per_thread;  /* consecutive values a thread loads per round: 1, 2, 4, 8, 16 */
-    uint32_t hist_tile;                 /* dict / const histogram: 8192, 16384, 32768 or 65536 */
+    uint32_t hist_tile;                 /* dict / const histogram: a multiple of 256, at most 32768 */
     int32_t schedule_compress;          /* GTSC_SCHEDULE_* */
     int32_t schedule_decompress;
     /* filled by gtsc_batch_autotune: step times (ms) with the default and with the chosen
@@ -230,7 +230,7 @@ gtsc_status gtsc_batch_get_tuning(gtsc_batch *b, gtsc_batch_tuning *tuning);
 /*
  * Times candidate parameters on the batch's own columns and trees with CUDA events: the schedule of
  * each step; then the min/max tile (1K .. 16K) x values per thread (1 .. 16) on the min/max
- * launches; then the histogram tile (8K .. 64K) on the histogram and top-k launches (a rebuild
+ * launches; then the histogram tile (8K .. 32K) on the histogram and top-k launches (a rebuild
  * each); a candidate is kept when it is at least 2 % faster.  The batch keeps the best parameters
  * (its device buffers, the framed output included, may move: call gtsc_batch_output again).
  * Synchronises; a few seconds for hundreds of columns.  *report may be NULL.

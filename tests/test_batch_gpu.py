@@ -263,7 +263,7 @@ TUNINGS = [dict(minmax_tile=1024, minmax_values_per_thread=1),
            dict(minmax_tile=2048, minmax_values_per_thread=2, hist_tile=4096),
            dict(minmax_tile=4096, minmax_values_per_thread=4, hist_tile=8192),
            dict(minmax_tile=16384, minmax_values_per_thread=8, hist_tile=16384),
-           dict(minmax_tile=8192, minmax_values_per_thread=16, hist_tile=65536),
+           dict(minmax_tile=8192, minmax_values_per_thread=16, hist_tile=32768),
            dict(minmax_tile=16384, minmax_values_per_thread=16, persistent_compress=True, persistent_decompress=True)]
 
 
