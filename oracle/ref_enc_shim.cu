@@ -33,6 +33,12 @@
 #include <stdexcept>
 #include <string>
 
+// the reference's exit(1) on a CUDA error (refshim/ref_compat.hpp renames exit to this)
+[[noreturn]] void ref_exit(int status)
+{
+    throw std::runtime_error("the reference stopped on a CUDA error (exit status " + std::to_string(status) + ")");
+}
+
 namespace ddj {
 template <typename T>
 SharedCudaPtr<int> Histogram::CudaHistogram(SharedCudaPtr<T>, int)

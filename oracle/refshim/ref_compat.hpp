@@ -7,7 +7,10 @@
 //    magnitude for char and short, INT_MIN / LONG_MIN for the minimum of int / long;
 //  - util/splitter/splitter.cu:111 calls thrust::count and tree/compression_statistics.cpp:121
 //    uses std::stringstream without including their headers, which the headers here no longer
-//    bring in through the others.
+//    bring in through the others;
+//  - CUDA_ASSERT_RETURN (core/macros.h:8-14) ends the process with exit(1) on any CUDA error; here
+//    exit throws (ref_exit, oracle/ref_enc_shim.cu), so that a failing call of the reference
+//    returns an error to the test that made it instead of ending the test run.
 #pragma once
 #include <cstdlib>
 #include <cmath>
@@ -29,3 +32,7 @@ inline auto abs(T v) -> decltype(+v)
     }
 }
 }  // namespace std
+
+#include <stdlib.h>
+[[noreturn]] void ref_exit(int status);
+#define exit(status) ref_exit(status)
