@@ -137,7 +137,7 @@ __device__ void p_afl_unpack(const BItem &it, uint32_t tile, StreamDesc *S, uint
 
 // ------------------------------------------------------------------------------- delta decode
 template <int ES>
-__device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+__device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, uint8_t *xs)
 {
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
@@ -156,8 +156,19 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     const uint64_t m = n ? n - 1 : 0;
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    const uint64_t wb = base - (uint64_t)(threadIdx.x & 31) * kBVPT;  // the warp's first element
+    constexpr uint64_t WRUN = 32 * kBVPT;
     uint64_t v[kBVPT];
-    load_dview<ES, kBVPT>(dv, base, v);
+    // a plain view whose warp run lies inside it comes in through the warp's tile; packed views are
+    // extracted blocked (a thread's values share packed words, each loaded once)
+    if (wb + WRUN <= dv.n && dv.b == 0 && dv.aligned && ((uintptr_t)dv.p & 15) == 0) {  // warp-uniform
+        load_run_warp<ES, kBVPT>(dv.p, wb, v, xs);
+        const uint64_t c = dv.c0 + dv.c1;
+#pragma unroll
+        for (int j = 0; j < (int)kBVPT; j++) v[j] = wrap_es(v[j] + c, ES);
+    } else {
+        load_dview<ES, kBVPT>(dv, base, v);
+    }
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++)
         if (base + j >= m) v[j] = 0;
@@ -171,7 +182,9 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
         if (threadIdx.x == 0) s_prefix = e;
     }
     __syncthreads();
-    if (base >= n) return;
+    // warp-uniform: the warp's whole run is inside the output and the output is 16-byte aligned
+    const bool wfull = wb + WRUN <= n && ((uintptr_t)out.ptr & 15) == 0;
+    if (!wfull && base >= n) return;
     unsigned long long acc = ld_unaligned<ES>(meta.ptr) + s_prefix + excl;
     uint64_t o[kBVPT];
 #pragma unroll
@@ -179,7 +192,10 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
         o[j] = wrap_es(acc, ES);
         acc += v[j];
     }
-    store_run<ES, kBVPT>(out.ptr, base, n, o);
+    if (wfull)
+        store_run_warp<ES, kBVPT>(out.ptr, wb, o, xs);
+    else
+        store_run<ES, kBVPT>(out.ptr, base, n, o);
 }
 
 // ------------------------------------------------------------------------------- scale add
@@ -196,14 +212,15 @@ __device__ void p_scale_add(const BItem &it, uint32_t tile, StreamDesc *S, uint3
         return;
     }
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
-    if (base >= n) return;
     const uint64_t mn = ld_unaligned<ES>(meta.ptr);
-    uint64_t v[kBVPT];
-    load_dview<ES, kBVPT>(dv, base, v);
-#pragma unroll
-    for (int j = 0; j < (int)kBVPT; j++) v[j] = wrap_es(v[j] + mn, ES);
-    store_run<ES, kBVPT>(out.ptr, base, n, v);
+    // block-striped: the k-th access of a warp covers 32 consecutive elements
+    const uint64_t t0 = (uint64_t)tile * kBTile + threadIdx.x;
+#pragma unroll 4
+    for (int j = 0; j < (int)kBVPT; j++) {
+        const uint64_t i = t0 + (uint64_t)j * kBThreads;
+        if (i >= n) break;
+        st_elem<ES>(out.ptr, i, wrap_es(dview_elem<ES>(dv, i) + mn, ES));
+    }
 }
 
 // ------------------------------------------------------------------------------- merge
@@ -537,7 +554,7 @@ __device__ void p_rle_scan(const BItem &it, uint32_t tile, StreamDesc *S, uint32
 }
 
 template <int ES>
-__device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
+__device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, uint8_t *xs)
 {
     // the tile's run ends relative to its first element, clamped to kBTile (at most kBTile + 1 runs)
     uint16_t *s_end = s_rle_end;
@@ -569,7 +586,10 @@ __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint
     __syncthreads();
     const uint32_t b = threadIdx.x * kBVPT;  // relative to t0
     const uint64_t base = t0 + b;
-    if (base >= n) return;
+    const uint64_t wb = base - (uint64_t)(threadIdx.x & 31) * kBVPT;  // the warp's first element
+    // warp-uniform: the warp's whole run is inside the output and the output is 16-byte aligned
+    const bool wfull = wb + 32 * kBVPT <= n && ((uintptr_t)out.ptr & 15) == 0;
+    if (!wfull && base >= n) return;
     uint32_t lo = 0, hi = m;  // first staged run ending after b
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -591,7 +611,10 @@ __device__ void p_rle_expand(const BItem &it, uint32_t tile, StreamDesc *S, uint
         }
         v[j] = in ? last_v : 0;
     }
-    store_run<ES, kBVPT>(out.ptr, base, n, v);
+    if (wfull)
+        store_run_warp<ES, kBVPT>(out.ptr, wb, v, xs);
+    else
+        store_run<ES, kBVPT>(out.ptr, base, n, v);
     (void)status;
 }
 
@@ -629,26 +652,29 @@ __device__ void p_f2i_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_
         return;
     }
     if (tile == 0 && threadIdx.x == 0) out.len = n * ES;
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
+    // block-striped: the k-th access of a warp covers 32 consecutive elements
+    const uint64_t t0 = (uint64_t)tile * kBTile + threadIdx.x;
     const Order o = (Order)it.order;
-    for (int j = 0; j < (int)kBVPT && base + j < n; j++) {
+    for (int j = 0; j < (int)kBVPT; j++) {
+        const uint64_t i = t0 + (uint64_t)j * kBThreads;
+        if (i >= n) break;
         uint64_t v;
         if (p < 10) {
-            const int k = (int32_t)dview_elem<4>(d, base + j);
+            const int k = (int32_t)dview_elem<4>(d, i);
             if (o == ORD_F32) v = __float_as_uint(__double2float_rn(__ddiv_rn((double)__int2float_rn(k), p10[p])));
             else if (o == ORD_F64) v = (uint64_t)__double_as_longlong(__ddiv_rn((double)k, p10[p]));
             else if (ES == 8) v = (uint64_t)__double2ll_rz(__ddiv_rn((double)k, p10[p]));
             else v = (uint64_t)(long long)__double2int_rz(__ddiv_rn((double)sext((uint64_t)(long long)k, ES), p10[p]));
         } else if (ES == 8) {  // raw bytes: two int32 per element
-            v = dview_elem<4>(d, 2 * (base + j)) | (dview_elem<4>(d, 2 * (base + j) + 1) << 32);
+            v = dview_elem<4>(d, 2 * i) | (dview_elem<4>(d, 2 * i + 1) << 32);
         } else if (ES == 4) {
-            v = dview_elem<4>(d, base + j);
+            v = dview_elem<4>(d, i);
         } else {  // 1- and 2-byte elements inside the int32 words
             constexpr uint64_t emask = ES >= 8 ? ~0ull : ((1ull << (8 * (ES % 8))) - 1);
-            const uint64_t byte = (base + j) * ES;
+            const uint64_t byte = i * ES;
             v = (dview_elem<4>(d, byte / 4) >> (8 * (byte % 4))) & emask;
         }
-        st_elem<ES>(out.ptr, base + j, v);
+        st_elem<ES>(out.ptr, i, v);
     }
 }
 
@@ -885,7 +911,11 @@ k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *cou
        uint32_t total_tiles)
 {
     constexpr bool DYN = OP == B_DELTA_DEC || OP == B_RLE_SCAN;
-    __shared__ __align__(16) unsigned char smem[OP == B_MERGE ? 8 * kBTile : OP == B_GFC_DEC ? kGfcRing * (kBThreads / 32) : 16];
+    constexpr int kSmem = OP == B_MERGE                             ? 8 * kBTile
+                          : OP == B_GFC_DEC                         ? kGfcRing * (kBThreads / 32)
+                          : OP == B_DELTA_DEC || OP == B_RLE_EXPAND ? kXchgBlockBytes  // warp exchange
+                                                                    : 16;
+    __shared__ __align__(16) unsigned char smem[kSmem];
     if (*(volatile uint32_t *)(status + 1)) return;
     if constexpr (!dec_persistent(OP)) {
         uint32_t tile;
@@ -930,12 +960,12 @@ __device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDe
     }
     if constexpr (OP == B_NONE_COPY) p_none_copy(it, tile, S, status);
     else if constexpr (OP == B_AFL_UNPACK) { GTSC_ES_SWITCH(p_afl_unpack<E>(it, tile, S, status)) }
-    else if constexpr (OP == B_DELTA_DEC) { GTSC_ES_SWITCH(p_delta_dec<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_DELTA_DEC) { GTSC_ES_SWITCH(p_delta_dec<E>(it, tile, S, status, smem)) }
     else if constexpr (OP == B_SCALE_ADD) { GTSC_ES_SWITCH(p_scale_add<E>(it, tile, S, status)) }
     else if constexpr (OP == B_MERGE) { GTSC_ES_SWITCH(p_merge<E>(it, tile, S, status, smem)) }
     else if constexpr (OP == B_MERGE_COUNT) { GTSC_ES_SWITCH(p_merge_count<E>(it, tile, S)) }
     else if constexpr (OP == B_RLE_SCAN) p_rle_scan(it, tile, S, status);
-    else if constexpr (OP == B_RLE_EXPAND) { GTSC_ES_SWITCH(p_rle_expand<E>(it, tile, S, status)) }
+    else if constexpr (OP == B_RLE_EXPAND) { GTSC_ES_SWITCH(p_rle_expand<E>(it, tile, S, status, smem)) }
     else if constexpr (OP == B_F2I_DEC) { GTSC_ES_SWITCH(p_f2i_dec<E>(it, tile, S, status)) }
     else if constexpr (OP == B_GFC_SIZES) p_gfc_sizes(it, tile, S, status);
     else if constexpr (OP == B_GFC_DEC) {
@@ -947,7 +977,7 @@ __device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDe
 
 #ifdef GTSC_PERSISTENT_TU
 // ------------------------------------------------------------------------------- persistent step
-constexpr size_t kPersistSmemD = 8 * kBTile > kGfcRing * (kBThreads / 32) ? 8 * kBTile : kGfcRing * (kBThreads / 32);
+constexpr size_t kPersistSmemD = std::max<size_t>({8 * kBTile, kGfcRing * (kBThreads / 32), kXchgBlockBytes});
 
 __device__ __forceinline__ uint32_t persist_extent_d(int op, const BItem &it, const StreamDesc *S)
 {

@@ -69,6 +69,91 @@ __device__ __forceinline__ void store_run(uint8_t *p, uint64_t base, uint64_t n,
     }
 }
 
+// ------------------------------------------------------------------------------- warp exchange
+// A warp's 32 * VPT consecutive elements pass between the blocked arrangement of the scan passes
+// (lane l holds elements [VPT l, VPT l + VPT) of the warp's run) and a striped one (the warp's k-th
+// access covers 32 consecutive 16-byte chunks) through a per-warp shared-memory tile.  A blocked
+// 16-byte access by a warp touches one half of 32 different sectors; the striped access touches
+// whole consecutive sectors, with a quarter of the L2 requests.  The tile holds one row of VPT
+// elements per lane; the 16-byte chunks of row r are permuted by an XOR with (r / G) mod (chunks
+// per row), G = 8 / chunks per row, so that the blocked accesses of eight consecutive lanes (one
+// shared-memory wavefront of 16-byte accesses) fall in eight distinct 16-byte bank groups, while a
+// striped access still covers whole rows.  The warp's lanes all take part; no block barrier is
+// involved.  `xs` is the block's exchange area (16-byte aligned, kXchgBlockBytes), one tile per
+// warp.  Used where it measured faster: the delta decode's plain inputs and its output, and the
+// RLE expansion's output (packed inputs stay blocked, where a thread's values share words).
+constexpr int kXchgWarpBytes = 32 * (int)kBVPT * 8;
+constexpr int kXchgBlockBytes = kBThreads / 32 * kXchgWarpBytes;
+
+template <int ES, int VPT>
+__device__ __forceinline__ uint8_t *xchg_tile(uint8_t *xs)
+{
+    static_assert(32 * VPT * ES <= kXchgWarpBytes, "exchange tile too small");
+    static_assert((VPT * ES) % 16 == 0 && VPT * ES / 16 <= 8, "a lane's row is 1 to 8 whole 16-byte chunks");
+    return xs + (threadIdx.x >> 5) * kXchgWarpBytes;
+}
+
+// byte offset of 16-byte chunk c of row r in a warp's tile
+template <int ES, int VPT>
+__device__ __forceinline__ uint32_t xchg_chunk(uint32_t r, uint32_t c)
+{
+    constexpr uint32_t CPR = VPT * ES / 16, G = 8 / CPR;
+    return (r * CPR + (c ^ ((r / G) & (CPR - 1)))) * 16;
+}
+
+// byte offset of 16-byte chunk q of the warp's run
+template <int ES, int VPT>
+__device__ __forceinline__ uint32_t xchg_chunk_at(uint32_t q)
+{
+    constexpr uint32_t CPR = VPT * ES / 16;
+    return xchg_chunk<ES, VPT>(q / CPR, q % CPR);
+}
+
+// Elements [wb, wb + 32 VPT) of a 16-byte aligned stream (the run lies inside it and wb * ES is a
+// multiple of 16) into the blocked arrangement, loaded as 32 consecutive 16-byte chunks per access.
+template <int ES, int VPT>
+__device__ __forceinline__ void load_run_warp(const uint8_t *p, uint64_t wb, uint64_t (&v)[VPT], uint8_t *xs)
+{
+    constexpr int PER = 16 / ES, CPR = VPT * ES / 16;
+    uint8_t *w = xchg_tile<ES, VPT>(xs);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint4 *src = reinterpret_cast<const uint4 *>(p + wb * ES);
+    __syncwarp();  // earlier reads of the tile by other lanes are done
+#pragma unroll
+    for (int k = 0; k < CPR; k++) {
+        const uint32_t q = 32 * k + lane;
+        *reinterpret_cast<uint4 *>(w + xchg_chunk_at<ES, VPT>(q)) = ldg(src + q);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < CPR; c++) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(w + xchg_chunk<ES, VPT>(lane, c));
+#pragma unroll
+        for (int j = 0; j < PER; j++) v[c * PER + j] = chunk_elem<ES>(q, j);
+    }
+}
+
+// Elements [wb, wb + 32 VPT) of a 16-byte aligned stream (the run lies inside it and wb * ES is a
+// multiple of 16) from the blocked arrangement, stored as 32 consecutive 16-byte chunks per access.
+template <int ES, int VPT>
+__device__ __forceinline__ void store_run_warp(uint8_t *p, uint64_t wb, const uint64_t (&v)[VPT], uint8_t *xs)
+{
+    constexpr int PER = 16 / ES, CPR = VPT * ES / 16;
+    uint8_t *w = xchg_tile<ES, VPT>(xs);
+    const uint32_t lane = threadIdx.x & 31;
+    __syncwarp();  // earlier reads of the tile by other lanes are done
+#pragma unroll
+    for (int c = 0; c < CPR; c++)
+        *reinterpret_cast<uint4 *>(w + xchg_chunk<ES, VPT>(lane, c)) = make_chunk<ES>(v + c * PER);
+    __syncwarp();
+    uint4 *dst = reinterpret_cast<uint4 *>(p + wb * ES);
+#pragma unroll
+    for (int k = 0; k < CPR; k++) {
+        const uint32_t q = 32 * k + lane;
+        dst[q] = *reinterpret_cast<const uint4 *>(w + xchg_chunk_at<ES, VPT>(q));
+    }
+}
+
 __device__ __forceinline__ void set_status(uint32_t *status, gtsc_status code)
 {
     atomicCAS(status, 0u, (uint32_t)(-code));
