@@ -1117,6 +1117,22 @@ __device__ __forceinline__ int f2i_decide(const BItem &it, const uint8_t *col, u
     return p;
 }
 
+// the raw branch (p = 10): the bytes of the tile's elements that fall in the stream's whole 32-bit
+// words (`words`), block-striped; whole words when the input is 4-byte aligned (the output, a node
+// stream, always is), else bytes
+template <int ES>
+__device__ __forceinline__ void f2i_copy_words(uint8_t *out, const uint8_t *in, uint32_t tile, uint64_t words)
+{
+    constexpr uint64_t B = (uint64_t)kBTile * ES;  // bytes of one tile
+    const uint64_t b0 = (uint64_t)tile * B, b1 = b0 + B < 4 * words ? b0 + B : 4 * words;
+    if (((uintptr_t)in & 3) == 0) {
+        for (uint64_t w = b0 / 4 + threadIdx.x; w < b1 / 4; w += kBThreads)
+            ((uint32_t *)out)[w] = ldg((const uint32_t *)in + w);
+    } else {
+        for (uint64_t b = b0 + threadIdx.x; b < b1; b += kBThreads) out[b] = ldg(in + b);
+    }
+}
+
 template <int ES>
 __device__ void p_f2i_enc(const BItem &it, uint32_t tile, StreamDesc *S)
 {
@@ -1135,23 +1151,25 @@ __device__ void p_f2i_enc(const BItem &it, uint32_t tile, StreamDesc *S)
             S[it.out[1]].len = 0;
         }
     }
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
-    if (base >= n) return;
+    // block-striped: the k-th access of a warp covers 32 consecutive elements (or words)
+    const uint64_t t0 = (uint64_t)tile * kBTile;
+    if (t0 >= n) return;
     uint8_t *out = S[it.out[1]].ptr;
     if (transform) {
         const Order o = (Order)it.order;
         const uint64_t wm = ES == 8 ? ~0ull : ((1ull << (8 * ES)) - 1);
         bool bad = false;
-        for (int j = 0; j < (int)kBVPT && base + j < n; j++) {
-            const uint64_t u = ld_elem<ES>(in.ptr, base + j);
+        for (int j = 0; j < (int)kBVPT; j++) {
+            const uint64_t i = t0 + (uint64_t)j * kBThreads + threadIdx.x;
+            if (i >= n) break;
+            const uint64_t u = ld_elem<ES>(in.ptr, i);
             const int k = (int)(long long)__double2ll_rn(__dmul_rn(as_double<ES>(u, o), p10[p]));
-            ((int32_t *)out)[base + j] = k;
+            ((int32_t *)out)[i] = k;
             if (((f2i_dec_one<ES>(k, p, o, p10) ^ u) & wm) != 0) bad = true;
         }
         if (bad) atomicExch((unsigned int *)(it.scratch + 64), 1u);
     } else {
-        const uint64_t bytes = (n * ES) / 4 * 4;
-        for (uint64_t b = base * ES; b < (base + kBVPT) * ES && b < bytes; b++) out[b] = in.ptr[b];
+        f2i_copy_words<ES>(out, in.ptr, tile, (n * ES) / 4);
     }
 }
 
@@ -1167,9 +1185,7 @@ __device__ void p_f2i_raw(const BItem &it, uint32_t tile, StreamDesc *S)
         *(int32_t *)S[it.out[0]].ptr = 10;
         S[it.out[1]].len = bytes;
     }
-    const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
-    uint8_t *out = S[it.out[1]].ptr;
-    for (uint64_t b = base * ES; b < (base + kBVPT) * ES && b < bytes; b++) out[b] = in.ptr[b];
+    f2i_copy_words<ES>(S[it.out[1]].ptr, in.ptr, tile, bytes / 4);
 }
 
 // ------------------------------------------------------------------------------- GFC
