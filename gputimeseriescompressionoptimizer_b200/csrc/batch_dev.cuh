@@ -80,8 +80,9 @@ __device__ __forceinline__ void store_run(uint8_t *p, uint64_t base, uint64_t n,
 // shared-memory wavefront of 16-byte accesses) fall in eight distinct 16-byte bank groups, while a
 // striped access still covers whole rows.  The warp's lanes all take part; no block barrier is
 // involved.  `xs` is the block's exchange area (16-byte aligned, kXchgBlockBytes), one tile per
-// warp.  Used where it measured faster: the delta decode's plain inputs and its output, and the
-// RLE expansion's output (packed inputs stay blocked, where a thread's values share words).
+// warp.  Used where it measured faster: the delta decode's plain inputs and its output, the RLE
+// expansion's output, and the split's and RLE heads' source runs (packed inputs stay blocked, where
+// a thread's values share words).
 constexpr int kXchgWarpBytes = 32 * (int)kBVPT * 8;
 constexpr int kXchgBlockBytes = kBThreads / 32 * kXchgWarpBytes;
 
@@ -357,6 +358,45 @@ __device__ __forceinline__ void load_view(const BItem &it, const ViewCtx &vc, co
     uint64_t x[VPT + kMaxViewOps];
     uint64_t head[VPT];
     load_run<ES, VPT>(src, base, vc.n_src, head);
+#pragma unroll
+    for (int j = 0; j < VPT; j++) x[j] = head[j];
+#pragma unroll
+    for (int j = 0; j < kMaxViewOps; j++)
+        x[VPT + j] = j < vc.nd && base + VPT + j < vc.n_src ? ld_elem<ES>(src, base + VPT + j) : 0;
+#pragma unroll
+    for (int k = 0; k < kMaxViewOps; k++) {
+        if (it.vop[k] == V_DELTA) {
+#pragma unroll
+            for (int j = 0; j + 1 < VPT + kMaxViewOps; j++) x[j] = wrap_es(x[j + 1] - x[j], ES);
+        } else if (it.vop[k] == V_SCALE) {
+#pragma unroll
+            for (int j = 0; j < VPT + kMaxViewOps; j++) x[j] = wrap_es(x[j] - vc.c[k], ES);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < VPT; j++) v[j] = x[j];
+}
+
+// load_view for passes whose block has `xs` (kXchgBlockBytes of shared memory, free at this point):
+// a warp whose source run lies wholly inside the source and starts 16-byte aligned loads it through
+// the warp exchange, as whole consecutive sectors; other warps load blocked.  Every lane of the
+// block calls it.
+template <int ES, int VPT>
+__device__ __forceinline__ void load_view_x(const BItem &it, const ViewCtx &vc, const uint8_t *src, uint64_t base,
+                                            uint64_t (&v)[VPT], uint8_t *xs)
+{
+    const uint64_t wb = base - (uint64_t)(threadIdx.x & 31) * VPT;
+    if (!(wb + 32 * VPT <= vc.n_src && ((uintptr_t)src & 15) == 0)) {  // warp-uniform
+        load_view<ES, VPT>(it, vc, src, base, v);
+        return;
+    }
+    if (vc.plain) {
+        load_run_warp<ES, VPT>(src, wb, v, xs);
+        return;
+    }
+    uint64_t x[VPT + kMaxViewOps];
+    uint64_t head[VPT];
+    load_run_warp<ES, VPT>(src, wb, head, xs);
 #pragma unroll
     for (int j = 0; j < VPT; j++) x[j] = head[j];
 #pragma unroll

@@ -789,7 +789,7 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
     if (tile > 0 && (uint64_t)tile * kBTile >= n) return;
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     uint64_t v[kBVPT];
-    load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+    load_view_x<ES, kBVPT>(it, vc, in.ptr, base, v, sm);  // sm is free until the staging below
     uint32_t bits = 0, codes = 0;
     if (mode == SPLIT_LOWER && outside) {
         // OutsideOperator (stencil_operators.hpp:14-25): false when x > high or x < low
@@ -936,7 +936,7 @@ __device__ void p_split(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t 
 
 // ------------------------------------------------------------------------------- RLE
 template <int ES>
-__device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
+__device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S, uint8_t *xs)
 {
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
@@ -958,7 +958,7 @@ __device__ void p_rle_heads(const BItem &it, uint32_t tile, StreamDesc *S)
     if ((uint64_t)tile * kBTile >= n) return;  // past the input: no successor needs this tile
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
     uint64_t v[kBVPT];
-    load_view<ES, kBVPT>(it, vc, in.ptr, base, v);
+    load_view_x<ES, kBVPT>(it, vc, in.ptr, base, v, xs);
     const uint64_t prev = base > 0 && base - 1 < n ? view_elem<ES>(it, vc, in.ptr, base - 1) : 0;
     uint32_t heads = 0;
 #pragma unroll
@@ -1408,10 +1408,12 @@ constexpr size_t stage_smem(int op)
     return op == B_AFL_PACK ? 8 * (kBTile + kBTile / 16 + 8)
          : op == B_HIST     ? 8 * kBHistPacked + 8 * 4 * (kBThreads / 32)
          : op == B_TOPK     ? sizeof(Cand) * kBThreads * 4
-         : op == B_SPLIT    ? 8 * (kBTile + kBTile / 16)
+         : op == B_SPLIT    ? 8 * (kBTile + kBTile / 16)  // >= kXchgBlockBytes (its loads)
+         : op == B_RLE_HEADS ? kXchgBlockBytes
          : op == B_GFC_COMPRESS ? kGfcStage * (kBThreads / 32)
                             : 16;
 }
+static_assert(stage_smem(B_SPLIT) >= kXchgBlockBytes, "the split loads through the warp exchange");
 
 // Tiles of an item that do work in a pass (the grid is sized for worst-case capacities; the real
 // stream lengths are only known on the device).  Tile 0 of a pass that writes metadata always
@@ -1522,7 +1524,7 @@ __device__ __forceinline__ void run_stage(const BItem &it, uint32_t tile, Stream
     else if constexpr (OP == B_TOPK) { GTSC_ES_SWITCH(p_topk<E>(it, tile, S, smem)) }
     else if constexpr (OP == B_VMETA) { GTSC_ES_SWITCH(p_vmeta<E>(it, S)) }
     else if constexpr (OP == B_SPLIT) { GTSC_ES_SWITCH(p_split<E>(it, tile, S, status, smem)) }
-    else if constexpr (OP == B_RLE_HEADS) { GTSC_ES_SWITCH(p_rle_heads<E>(it, tile, S)) }
+    else if constexpr (OP == B_RLE_HEADS) { GTSC_ES_SWITCH(p_rle_heads<E>(it, tile, S, smem)) }
     else if constexpr (OP == B_RLE_LENGTHS) { p_rle_lengths(it, tile, S); }
     else if constexpr (OP == B_F2I_STATS) { GTSC_ES_SWITCH(p_f2i_stats<E>(it, tile, S)) }
     else if constexpr (OP == B_F2I_ENC) { GTSC_ES_SWITCH(p_f2i_enc<E>(it, tile, S)) }
