@@ -137,7 +137,7 @@ __device__ void p_afl_unpack(const BItem &it, uint32_t tile, StreamDesc *S, uint
 
 // ------------------------------------------------------------------------------- delta decode
 template <int ES>
-__device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status, uint8_t *xs)
+__device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint32_t *status)
 {
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long s_prefix;
@@ -156,19 +156,8 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
     Lookback lb = lookback_at(it.scratch + it.p[0], it.tiles);
     const uint64_t m = n ? n - 1 : 0;
     const uint64_t base = (uint64_t)tile * kBTile + (uint64_t)threadIdx.x * kBVPT;
-    const uint64_t wb = base - (uint64_t)(threadIdx.x & 31) * kBVPT;  // the warp's first element
-    constexpr uint64_t WRUN = 32 * kBVPT;
     uint64_t v[kBVPT];
-    // a plain view whose warp run lies inside it comes in through the warp's tile; packed views are
-    // extracted blocked (a thread's values share packed words, each loaded once)
-    if (wb + WRUN <= dv.n && dv.b == 0 && dv.aligned && ((uintptr_t)dv.p & 15) == 0) {  // warp-uniform
-        load_run_warp<ES, kBVPT>(dv.p, wb, v, xs);
-        const uint64_t c = dv.c0 + dv.c1;
-#pragma unroll
-        for (int j = 0; j < (int)kBVPT; j++) v[j] = wrap_es(v[j] + c, ES);
-    } else {
-        load_dview<ES, kBVPT>(dv, base, v);
-    }
+    load_dview<ES, kBVPT>(dv, base, v);
 #pragma unroll
     for (int j = 0; j < (int)kBVPT; j++)
         if (base + j >= m) v[j] = 0;
@@ -182,9 +171,7 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
         if (threadIdx.x == 0) s_prefix = e;
     }
     __syncthreads();
-    // warp-uniform: the warp's whole run is inside the output and the output is 16-byte aligned
-    const bool wfull = wb + WRUN <= n && ((uintptr_t)out.ptr & 15) == 0;
-    if (!wfull && base >= n) return;
+    if (base >= n) return;
     unsigned long long acc = ld_unaligned<ES>(meta.ptr) + s_prefix + excl;
     uint64_t o[kBVPT];
 #pragma unroll
@@ -192,10 +179,7 @@ __device__ void p_delta_dec(const BItem &it, uint32_t tile, StreamDesc *S, uint3
         o[j] = wrap_es(acc, ES);
         acc += v[j];
     }
-    if (wfull)
-        store_run_warp<ES, kBVPT>(out.ptr, wb, o, xs);
-    else
-        store_run<ES, kBVPT>(out.ptr, base, n, o);
+    store_run<ES, kBVPT>(out.ptr, base, n, o);
 }
 
 // ------------------------------------------------------------------------------- scale add
@@ -913,7 +897,7 @@ k_bdec(const BItem *items, const uint32_t *item_of, StreamDesc *S, uint32_t *cou
     constexpr bool DYN = OP == B_DELTA_DEC || OP == B_RLE_SCAN;
     constexpr int kSmem = OP == B_MERGE                             ? 8 * kBTile
                           : OP == B_GFC_DEC                         ? kGfcRing * (kBThreads / 32)
-                          : OP == B_DELTA_DEC || OP == B_RLE_EXPAND ? kXchgBlockBytes  // warp exchange
+                          : OP == B_RLE_EXPAND                      ? kXchgBlockBytes  // warp exchange
                                                                     : 16;
     __shared__ __align__(16) unsigned char smem[kSmem];
     if (*(volatile uint32_t *)(status + 1)) return;
@@ -960,7 +944,7 @@ __device__ __forceinline__ void run_dec(const BItem &it, uint32_t tile, StreamDe
     }
     if constexpr (OP == B_NONE_COPY) p_none_copy(it, tile, S, status);
     else if constexpr (OP == B_AFL_UNPACK) { GTSC_ES_SWITCH(p_afl_unpack<E>(it, tile, S, status)) }
-    else if constexpr (OP == B_DELTA_DEC) { GTSC_ES_SWITCH(p_delta_dec<E>(it, tile, S, status, smem)) }
+    else if constexpr (OP == B_DELTA_DEC) { GTSC_ES_SWITCH(p_delta_dec<E>(it, tile, S, status)) }
     else if constexpr (OP == B_SCALE_ADD) { GTSC_ES_SWITCH(p_scale_add<E>(it, tile, S, status)) }
     else if constexpr (OP == B_MERGE) { GTSC_ES_SWITCH(p_merge<E>(it, tile, S, status, smem)) }
     else if constexpr (OP == B_MERGE_COUNT) { GTSC_ES_SWITCH(p_merge_count<E>(it, tile, S)) }

@@ -80,9 +80,10 @@ __device__ __forceinline__ void store_run(uint8_t *p, uint64_t base, uint64_t n,
 // shared-memory wavefront of 16-byte accesses) fall in eight distinct 16-byte bank groups, while a
 // striped access still covers whole rows.  The warp's lanes all take part; no block barrier is
 // involved.  `xs` is the block's exchange area (16-byte aligned, kXchgBlockBytes), one tile per
-// warp.  Used where it measured faster: the delta decode's plain inputs and its output, the RLE
-// expansion's output, and the split's and RLE heads' source runs (packed inputs stay blocked, where
-// a thread's values share words).
+// warp.  Used where it measured faster: the RLE expansion's output and the split's and RLE heads'
+// source runs.  Not in the delta decode: there it sped up the many-column step but slowed one long
+// column's decode by a quarter (its stores leave the block later, and one column's tiles form a
+// single look-back chain).
 constexpr int kXchgWarpBytes = 32 * (int)kBVPT * 8;
 constexpr int kXchgBlockBytes = kBThreads / 32 * kXchgWarpBytes;
 
